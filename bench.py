@@ -1,0 +1,354 @@
+"""Benchmark of the B200 batched dense linear-solve path.
+
+Workload (default, one step): the uneven FP64 batch — 8192 systems, order n
+log-uniform in [4, 512], nrhs uniform from {1, 8, 32}, A = N(0,1) + n I, b =
+N(0,1) from default_rng (PCG64, the reference's generator); solve and slogdet
+for every system, inverse for a seeded 10%. One step = one replay of the plan
+(one persistent launch per size class, one CUDA graph) over the whole batch
+with inputs already resident in HBM (1.8 GB of matrices: larger than L2, so
+no flush is needed between steps).
+
+Arms:
+  python bench.py [--gpus N --steps K --warmup W]      this path (one rank per GPU)
+  python bench.py --impl reference ...                  the reference's own CPU path
+                                                        (oracle/_ref) on the host cores
+
+Prints one JSON line (rank 0). Under torchrun every rank runs its own batch
+(seed + rank): weak scaling, no collective on the data path; the step time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "batched solves/s at ≤1e-10 backward err, refined mixed vs FP64 LU; p50/p99 ms"
+WORKLOAD = ("uneven FP64 batch: 8192 systems, n log-uniform [4,512], nrhs {1,8,32}, A=N(0,1)+nI, "
+            "solve+slogdet all, inv 10%")
+SEED = 2025
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--count", type=int, default=8192)
+    p.add_argument("--cpu-sample", type=int, default=512, help="systems in the bounded CPU sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except OSError:
+        return {}
+
+
+def fp64_peak_tflops(torch, dev):
+    """cuBLAS DGEMM 8192^3 (best of 5) as the measured FP64 tensor-pipe peak."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_reference_sample(sys, sample: int, threads: int, seed: int = 1):
+    """Time the reference's CPU path (oracle/_ref) on a bounded random sample of the
+    same workload; returns (solves/s, kind, cores, description)."""
+    from numpp_b200 import workloads
+    from oracle import load_oracle, load_ref, ref_available
+
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(len(sys["n"]), min(sample, len(sys["n"])), replace=False))
+    sub = workloads.take(sys, idx)
+    if ref_available():
+        r = load_ref()
+        t0 = time.perf_counter()
+        r.solve_grouped(sub, threads=threads)
+        dt = time.perf_counter() - t0
+        kind, cores = "reference", threads
+    else:
+        o = load_oracle()
+        t0 = time.perf_counter()
+        o.solve_grouped(sub)
+        dt = time.perf_counter() - t0
+        kind, cores = "port", 1
+    desc = (f"{len(idx)} of {len(sys['n'])} systems drawn uniformly (seed {seed}), "
+            f"numpp::linalg::solve + slogdet + inv per system, {cores} thread(s)")
+    return len(idx) / dt, kind, cores, desc, dt
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from numpp_b200 import workloads
+    sys_ = workloads.uneven_batch(seed=SEED, count=args.count)
+    threads = os.cpu_count() or 1
+    rates = []
+    for i in range(args.warmup + args.steps):
+        rate, kind, cores, desc, dt = cpu_reference_sample(sys_, args.cpu_sample, threads, seed=100 + i)
+        if i >= args.warmup:
+            rates.append(rate)
+    value = float(np.mean(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (PCG64 default_rng, seed %d)" % SEED,
+        "config": {"workload": WORKLOAD, "count": args.count, "sample_per_step": args.cpu_sample},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind, "sample": desc},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args):
+    import torch
+    import torch.distributed as dist
+
+    from numpp_b200 import _lib, workloads
+    from numpp_b200.grouped import Plan
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    L = _lib.load()
+    assert L.nppb_device_available() == 1, _lib.last_error()
+
+    sys_ = workloads.uneven_batch(seed=SEED + rank, count=args.count)
+    flags = _lib.WANT_SOLVE | _lib.WANT_SLOGDET | _lib.WANT_INV
+    plan = Plan(sys_, flags)
+    cnt = len(sys_["n"])
+    dA = torch.from_numpy(sys_["A"]).to(dev)
+    dB = torch.from_numpy(sys_["B"]).to(dev)
+    dX = torch.zeros_like(dB)
+    dInv = torch.zeros(max(plan.inv_elems, 1), dtype=torch.float64, device=dev)
+    dDet = torch.zeros(cnt, dtype=torch.float64, device=dev)
+    dSign = torch.zeros_like(dDet)
+    dLog = torch.zeros_like(dDet)
+    dInfo = torch.zeros(cnt, dtype=torch.int32, device=dev)
+    bufs = (dA, dB, dX, dInv, dDet, dSign, dLog, dInfo)
+    stream = torch.cuda.Stream()
+    nclass = len(plan.classes())
+
+    def step():
+        plan.execute(*bufs, stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    stream.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        with torch.cuda.stream(stream):
+            ev[0].record(stream)
+            for i in range(args.steps):
+                step()
+                ev[i + 1].record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    per_step = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ms_step = total_ms / args.steps
+    value = world * cnt / (ms_step * 1e-3)
+
+    # correctness gate on what was just timed: normwise backward error on a sample
+    info = dInfo.cpu().numpy()
+    X = dX.cpu().numpy()
+    rng = np.random.default_rng(rank)
+    worst = 0.0
+    for i in rng.choice(cnt, 64, replace=False):
+        n, k = int(sys_["n"][i]), int(sys_["nrhs"][i])
+        A = sys_["A"][sys_["a_off"][i]:sys_["a_off"][i] + n * n].reshape(n, n)
+        B = sys_["B"][sys_["b_off"][i]:sys_["b_off"][i] + n * k].reshape(n, k)
+        x = X[sys_["b_off"][i]:sys_["b_off"][i] + n * k].reshape(n, k)
+        eta = np.abs(B - A @ x).max() / (np.abs(A).sum(1).max() * np.abs(x).max() + np.abs(B).max())
+        worst = max(worst, float(eta))
+    assert not info.any() and worst <= 1e-10, (int(info.astype(bool).sum()), worst)
+
+    # per-class kernel time (CUDA events on the launching stream) -> roofline of the top class
+    cls = plan.classes()
+    cls_ms = plan.time_classes(*bufs, stream=stream, reps=3)
+    top = int(np.argmax(cls_ms))
+    flops_top = cls[top][3]
+    peak64 = fp64_peak_tflops(torch, dev)
+    achieved = flops_top / (cls_ms[top] * 1e-3) / 1e12
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "lu_cta_uneven8192_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("bytes_per_launch")
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
+    hA, hB = pin(sys_["A"]), pin(sys_["B"])
+    hX = pin(np.zeros_like(sys_["B"]))
+    hInv = pin(np.zeros(max(plan.inv_elems, 1)))
+    hDet, hSign, hLog = pin(np.zeros(cnt)), pin(np.zeros(cnt)), pin(np.zeros(cnt))
+    hInfo = pin(np.zeros(cnt, np.int32))
+    for _ in range(max(1, args.warmup)):
+        plan.execute_host(hA, hB, hX, hInv, hDet, hSign, hLog, hInfo)
+    if world > 1:
+        dist.barrier()
+    e2e_ms = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        plan.execute_host(hA, hB, hX, hInv, hDet, hSign, hLog, hInfo)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = float(np.mean(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_step], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    h2d = 8 * (plan.a_elems + plan.b_elems)
+    d2h = 8 * (plan.b_elems + plan.inv_elems + 3 * cnt) + 4 * cnt
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, desc, _ = cpu_reference_sample(sys_, args.cpu_sample, os.cpu_count() or 1)
+        cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind, "sample": desc}
+
+    flops_step = workloads.uneven_flops(sys_)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (PCG64 default_rng, seed %d + rank)" % SEED,
+            "config": {"workload": WORKLOAD, "count": cnt, "parallelism": f"replicas{world}",
+                       "l2": "inputs (%.2f GB of A) larger than L2; no flush" % (8 * plan.a_elems / 1e9),
+                       "graph": True, "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls]},
+            "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
+            "gflops": flops_step * world / (ms_step * 1e-3) / 1e9,
+            "max_backward_error_sample": worst,
+            "roofline": {"bound": "tensor", "kernel": f"k_lu_cta (class n<={cls[top][1]})",
+                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                         "peak_source": "measured cuBLAS FP64 GEMM 8192^3 on this GPU (burst)",
+                         "traffic": traffic, "launch_ms": cls_ms[top], "flops_per_launch": flops_top},
+            "class_ms": {f"{c[0]}<={c[1]}": round(m, 4) for c, m in zip(cls, cls_ms)},
+            "e2e": {"value": world * cnt / (e2e_step * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
+                    "path": "nppb_plan_execute_host (C ABI), pinned host buffers"},
+            "gpu_launches": args.steps * nclass,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+            "hbm_peak_gbs": measured_peaks().get("hbm_gbs"),
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,171 @@
+/*
+ * numpp_b200.h — C ABI of the B200-native (sm_100a) batched dense linear-solve
+ * path for NumPP: numpp::linalg::solve / inv / det / slogdet on stacked
+ * (..., n, n) float64 arrays, and the matmul they rest on.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, and is
+ * thread-safe. Arrays are C-contiguous (row-major). Host-buffer entry points
+ * copy in, compute on the GPU and copy out before returning, exactly like a
+ * NumPP GpuVTable slot (the caller owns every buffer; nothing is retained).
+ * Device-buffer entry points (prefix nppb_d_) take device pointers and a CUDA
+ * stream (cudaStream_t passed as void*; NULL = the legacy default stream) and
+ * only enqueue work.
+ *
+ * Status codes: NPPB_OK (0) on success; NPPB_DECLINED (1) when the request is
+ * outside what the GPU path serves (dtype, op), so a NumPP dispatcher falls
+ * back to its portable CPU kernel; negative values are errors, described by
+ * nppb_last_error() on the calling thread. A singular matrix is not an error:
+ * the per-system info[] entry is set to k+1 for the first exactly-zero pivot
+ * k (0-based), mirroring where the reference stops.
+ *
+ * Pivots (ipiv) are LAPACK-style swap lists, 0-based: at step k rows k and
+ * ipiv[k] were exchanged. The reference's permutation vector piv
+ * (src/linalg/linalg.cpp:52,60 in NumPP) is the identity with those swaps
+ * applied in order.
+ */
+#ifndef NUMPP_B200_H
+#define NUMPP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NPPB_ABI_VERSION 1
+
+enum {
+  NPPB_OK = 0,
+  NPPB_DECLINED = 1,
+  NPPB_E_ARG = -1,      /* invalid argument (shape, null pointer, size)      */
+  NPPB_E_NODEV = -2,    /* no usable sm_100 device                           */
+  NPPB_E_CUDA = -3,     /* a CUDA runtime call failed                        */
+  NPPB_E_NOMEM = -4,    /* device allocation failed or budget exceeded      */
+  NPPB_E_RANGE = -5     /* size outside what this entry point supports      */
+};
+
+/* numpp::DTypeId values (include/numpp/core/dtype.hpp:16-22 in NumPP). */
+enum { NPPB_DT_FLOAT32 = 10, NPPB_DT_FLOAT64 = 11 };
+
+/* ---- library ---------------------------------------------------------- */
+int nppb_abi_version(void);
+/* 1 when a compute-capability 10.x device is present (numpp gpu_vtable() is
+ * non-null exactly then: src/backend/cuda_backend.cu:120-123,320). */
+int nppb_device_available(void);
+/* Message for the last failing call on this thread ("" if none). */
+const char* nppb_last_error(void);
+/* Largest order served by the batched entry points. */
+int32_t nppb_max_order(void);
+/* The numpp::GpuVTable this library provides (numpp::gpu_vtable(), see
+ * include/numpp/backend/gpu_vtable.hpp), for hosts that cannot name the C++
+ * symbol; NULL when no compute-capability 10.x device is present. */
+const void* nppb_gpu_vtable(void);
+
+/* ---- GpuVTable slots (include/numpp/backend/gpu_vtable.hpp:17-26) ------ */
+/* The elementwise/reduce slots are called by NumPP's ufunc layer without a
+ * null check (src/umath/ufunc.cpp:528-531,539-541,611-613); this backend
+ * declines them (returns NPPB_DECLINED) so the portable kernels run. */
+int nppb_elementwise_binary(int op, int dtype, int64_t n, const void* a, const void* b, void* out);
+int nppb_elementwise_unary(int op, int dtype, int64_t n, const void* a, void* out);
+int nppb_reduce(int op, int dtype, int64_t n, const void* a, void* out);
+/* GpuVTable::gemm (gpu_vtable.hpp:22-26; the CUDA backend's gemm_impl at
+ * src/backend/cuda_backend.cu:288-293): row-major C[m,n] = A[m,k] B[k,n],
+ * float32 or float64, host buffers. */
+int nppb_gemm(int dtype, int64_t m, int64_t n, int64_t k, const void* A, const void* B, void* C);
+/* Same on device buffers (FP64 runs on DMMA). */
+int nppb_d_gemm(int dtype, int64_t m, int64_t n, int64_t k, const void* dA, const void* dB,
+                void* dC, void* stream);
+
+/* ---- uniform batches: count systems of order n (host buffers) ----------- */
+/* getrf: LU with partial pivoting in place (src/linalg/linalg.cpp:48-71),
+ * A (count,n,n) overwritten by the unit-lower L and U in pivoted row order. */
+int nppb_getrf_batched(int64_t count, int32_t n, double* A, int32_t* ipiv, int32_t* info);
+/* getrs: B (count,n,nrhs) overwritten by the solution (linalg.cpp:73-90). */
+int nppb_getrs_batched(int64_t count, int32_t n, int32_t nrhs, const double* LU,
+                       const int32_t* ipiv, double* B);
+/* numpp::linalg::solve on a (count,n,n) stack with a (count,n,nrhs) right-hand
+ * side (linalg.cpp:368-385, src/linalg/batched.cpp:90-100). */
+int nppb_solve_batched(int64_t count, int32_t n, int32_t nrhs, const double* A, const double* B,
+                       double* X, int32_t* info);
+/* numpp::linalg::inv (linalg.cpp:386-392, 105-115; batched.cpp:75). */
+int nppb_inv_batched(int64_t count, int32_t n, const double* A, double* Ainv, int32_t* info);
+/* numpp::linalg::det (linalg.cpp:393-407; batched.cpp:76). Singular -> 0. */
+int nppb_det_batched(int64_t count, int32_t n, const double* A, double* det);
+/* numpp::linalg::slogdet (linalg.cpp:408-439; batched.cpp:102-108).
+ * Singular -> sign 0, logabsdet -inf. */
+int nppb_slogdet_batched(int64_t count, int32_t n, const double* A, double* sign,
+                         double* logabsdet);
+/* solve and det from one factorisation (the reference factors twice). */
+int nppb_solve_det_batched(int64_t count, int32_t n, int32_t nrhs, const double* A,
+                           const double* B, double* X, double* det, int32_t* info);
+
+/* ---- uniform batches on device buffers --------------------------------- */
+/* `flags` selects outputs: NPPB_WANT_* below. Null output pointers are
+ * allowed for outputs not selected. dLU/dipiv are the factor workspace
+ * (count*n*n doubles, count*n int32); pass NULL to let the library allocate
+ * it stream-ordered for the call. With NPPB_WANT_LU the factors stay there. */
+enum {
+  NPPB_WANT_LU = 1,
+  NPPB_WANT_SOLVE = 2,
+  NPPB_WANT_DET = 4,
+  NPPB_WANT_SLOGDET = 8,
+  NPPB_WANT_INV = 16
+};
+int nppb_d_linalg_batched(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA,
+                          const double* dB, double* dX, double* dInv, double* dDet,
+                          double* dSign, double* dLogabs, double* dLU, int32_t* dipiv,
+                          int32_t* dinfo, void* stream);
+/* getrs from factors left by nppb_d_linalg_batched(NPPB_WANT_LU): dB -> dX
+ * (dX may equal dB). */
+int nppb_d_getrs_batched(int64_t count, int32_t n, int32_t nrhs, const double* dLU,
+                         const int32_t* dipiv, const double* dB, double* dX, void* stream);
+
+/* ---- uneven batches ------------------------------------------------------ */
+/* A plan packs `count` systems of different orders n[i] and right-hand-side
+ * counts nrhs[i] into size classes, one persistent launch per class, and
+ * replays them as one CUDA graph. System i's matrix starts at element
+ * a_off[i] of the packed A array, its right-hand side / solution at b_off[i]
+ * of B / X, and its inverse (when inv_off[i] >= 0) at inv_off[i] of Inv.
+ * Per-system outputs (sign, logabsdet, det, info) are indexed by i.
+ * `flags` is a NPPB_WANT_* mask (NPPB_WANT_LU is ignored). */
+typedef struct nppb_plan nppb_plan;
+int nppb_plan_create(nppb_plan** plan, int64_t count, const int32_t* n, const int32_t* nrhs,
+                     const int64_t* a_off, const int64_t* b_off, const int64_t* inv_off,
+                     int flags);
+/* Sizes (elements) the packed arrays must have. */
+int nppb_plan_sizes(const nppb_plan* plan, int64_t* a_elems, int64_t* b_elems,
+                    int64_t* inv_elems);
+/* Device buffers; enqueues on `stream`. */
+int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, double* dX,
+                      double* dInv, double* dDet, double* dSign, double* dLogabs,
+                      int32_t* dinfo, void* stream);
+/* Host buffers: copies in, runs, copies out, synchronises. Inputs in pinned
+ * memory take the fast DMA path. */
+int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X,
+                           double* Inv, double* Det, double* Sign, double* Logabs,
+                           int32_t* info);
+int nppb_plan_destroy(nppb_plan* plan);
+/* Introspection for measurement: the plan's size classes, each with its kernel
+ * (1 = warp-per-system, 0 = CTA-per-system), order bound, system count and the
+ * algorithmic flops / minimum bytes of what it computes (LAPACK counts:
+ * getrf 2/3n^3-1/2n^2+5/6n, getrs 2n^2k-nk, inverse +4/3n^3). */
+int nppb_plan_num_classes(const nppb_plan* plan);
+int nppb_plan_class_info(const nppb_plan* plan, int cls, int* is_warp, int* bound,
+                         int64_t* systems, double* flops, double* bytes);
+/* Runs every class alone on `stream`, `reps` launches each between two CUDA
+ * events on that stream; ms_out[cls] = mean milliseconds of one launch. */
+int nppb_plan_time_classes(nppb_plan* plan, const double* dA, const double* dB, double* dX,
+                           double* dInv, double* dDet, double* dSign, double* dLogabs,
+                           int32_t* dinfo, void* stream, int reps, float* ms_out);
+
+/* One-shot uneven batch on host buffers (plan + execute + destroy). */
+int nppb_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
+                       const int64_t* b_off, const int64_t* inv_off, int flags, const double* A,
+                       const double* B, double* X, double* Inv, double* Det, double* Sign,
+                       double* Logabs, int32_t* info);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif /* NUMPP_B200_H */

@@ -1,0 +1,27 @@
+// FP64 tensor-core (DMMA) and warp helpers for sm_100a.
+#pragma once
+
+#include <climits>
+
+namespace nppb {
+
+// D(8x8) += A(8x4) * B(4x8), FP64, one warp. Lane l = 4*g + t holds
+// A[g][t], B[t][g] and D[g][2t], D[g][2t+1].
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Warp-wide argmax of (v, i): the largest v wins, ties go to the smaller i.
+// Every lane ends with the same pair.
+__device__ __forceinline__ void warp_argmax(double& v, int& i) {
+#pragma unroll
+  for (int off = 16; off; off >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+    const int oi = __shfl_xor_sync(0xffffffffu, i, off);
+    if (ov > v || (ov == v && oi < i)) { v = ov; i = oi; }
+  }
+}
+
+}  // namespace nppb

@@ -1,0 +1,120 @@
+// Host runtime: device probe, errors, per-thread streams, allocations, and the
+// order -> kernel choice for uniform batches. C++20.
+#include "runtime.hpp"
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/numpp_b200.h"
+
+namespace nppb {
+namespace {
+
+thread_local std::string t_error;
+
+struct DeviceTable {
+  std::mutex mu;
+  std::vector<Device> devs;      // by ordinal; id == -1 until probed
+  std::vector<int> probed;       // 0 unprobed, 1 ok, -1 not sm_100
+};
+DeviceTable& table() {
+  static DeviceTable t;
+  return t;
+}
+
+}  // namespace
+
+void set_error(std::string msg) { t_error = std::move(msg); }
+const char* last_error() { return t_error.c_str(); }
+void clear_error() { t_error.clear(); }
+
+int cuda_status(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? NPPB_E_NOMEM : NPPB_E_CUDA;
+}
+
+const Device* device() {
+  int cur = 0;
+  if (cudaGetDevice(&cur) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return nullptr;
+  }
+  DeviceTable& t = table();
+  std::lock_guard<std::mutex> lk(t.mu);
+  if ((int)t.devs.size() <= cur) {
+    t.devs.resize(cur + 1);
+    t.probed.resize(cur + 1, 0);
+  }
+  if (t.probed[cur] == 0) {
+    cudaDeviceProp p{};
+    if (cudaGetDeviceProperties(&p, cur) != cudaSuccess) {
+      cudaGetLastError();
+      t.probed[cur] = -1;
+    } else if (p.major != 10) {
+      t.probed[cur] = -1;
+    } else {
+      Device& d = t.devs[cur];
+      d.id = cur;
+      d.sms = p.multiProcessorCount;
+      d.cc_major = p.major;
+      d.cc_minor = p.minor;
+      t.probed[cur] = prepare_kernels() == cudaSuccess ? 1 : -1;
+    }
+  }
+  if (t.probed[cur] != 1) {
+    set_error("device is not an sm_100 (B200-class) GPU or kernel setup failed");
+    return nullptr;
+  }
+  return &t.devs[cur];
+}
+
+cudaStream_t thread_stream() {
+  struct Holder {
+    cudaStream_t s = nullptr;
+    int dev = -1;
+    ~Holder() {
+      if (s) cudaStreamDestroy(s);
+    }
+  };
+  thread_local Holder h;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (!h.s || h.dev != cur) {
+    if (h.s) cudaStreamDestroy(h.s);
+    cudaStreamCreateWithFlags(&h.s, cudaStreamNonBlocking);
+    h.dev = cur;
+  }
+  return h.s;
+}
+
+cudaError_t DevMem::alloc(size_t bytes, cudaStream_t st) {
+  release();
+  st_ = st;
+  if (bytes == 0) return cudaSuccess;
+  return cudaMallocAsync(&p_, bytes, st);
+}
+
+void DevMem::release() {
+  if (p_) cudaFreeAsync(p_, st_);
+  p_ = nullptr;
+}
+
+cudaError_t prepare_kernels() { return lu_cta_prepare(); }
+
+int lu_cta_grid(int nsys, int nmax, int num_sms) {
+  const int g = lu_cta_blocks_per_sm(nmax) * num_sms;
+  return nsys < g ? nsys : g;
+}
+
+cudaError_t run_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
+  const Device* d = device();
+  if (!d) return cudaErrorNoDevice;
+  const int c = static_cast<int>(count);
+  if (n <= 32) return launch_lu_warp(bt, nullptr, c, n <= 8 ? 8 : (n <= 16 ? 16 : 32), st);
+  if (n <= kCtaMaxN) return launch_lu_cta(bt, nullptr, c, n, lu_cta_grid(c, n, d->sms), st);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace nppb

@@ -1,0 +1,64 @@
+// Host runtime shared by the C ABI entry points: device probe, per-thread
+// streams and error text, stream-ordered device allocations. C++20.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "nppb_internal.hpp"
+
+namespace nppb {
+
+struct Device {
+  int id = -1;
+  int sms = 0;
+  int cc_major = 0, cc_minor = 0;
+};
+
+// The current CUDA device if it is compute capability 10.x, else nullptr
+// (message in last_error()). Probed once per device, thread-safe.
+const Device* device();
+
+void set_error(std::string msg);
+const char* last_error();
+void clear_error();
+
+// Maps a CUDA failure to a status code and records the message.
+int cuda_status(cudaError_t e, const char* what);
+
+// A non-blocking stream owned by the calling thread (host-buffer entry points).
+cudaStream_t thread_stream();
+
+// Stream-ordered device allocation, freed on the same stream on destruction.
+class DevMem {
+ public:
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+  cudaError_t alloc(size_t bytes, cudaStream_t st);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p_); }
+  bool empty() const { return p_ == nullptr; }
+
+ private:
+  void* p_ = nullptr;
+  cudaStream_t st_ = nullptr;
+};
+
+// Fills on the device (k_util.cu).
+cudaError_t launch_fill_f64(double* p, int64_t n, double v, cudaStream_t st);
+cudaError_t launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t st);
+
+// Picks the kernel for a uniform batch of order n and launches it.
+cudaError_t run_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st);
+
+// One-time kernel attribute setup (dynamic shared memory opt-in), done before
+// any stream capture.
+cudaError_t prepare_kernels();
+int lu_cta_grid(int nsys, int nmax, int num_sms);
+
+}  // namespace nppb

@@ -1,0 +1,235 @@
+"""numpp::linalg front-end on the B200 path (host-side mirror of NumPP's interface).
+
+Same names, argument meaning and error behaviour as NumPP's
+include/numpp/linalg/linalg.hpp:29-32 and src/backend/backend.cpp:121-177,
+on numpy arrays:
+
+* ``solve(a, b)``  -- linalg.cpp:368-385; stacked a (ndim > 2) follows
+  batched.cpp:90-100: b is a stack of vectors when b.ndim == a.ndim - 1
+  (NumPP keeps NumPy 1.x's rule), else a stack of (n, k) matrices.
+* ``inv(a)``, ``det(a)``, ``slogdet(a)`` -- linalg.cpp:386-439, batched.cpp:75-108.
+* ``matmul(a, b)`` -- backend.cpp:121-177 with the GPU forced (2-D only).
+
+dtype policy (``la_kind``, linalg.cpp:20-26): the computation is float64;
+float32 results come back as float32, every other real dtype as float64.
+Complex inputs are not served by this path (NumPP's portable CPU kernel keeps
+them), so they raise ``Declined``.
+
+Errors: ``LinAlgError("Last 2 dimensions of the array must be square")`` and
+``LinAlgError("Singular matrix")`` as numpp::linalg_error (linalg.cpp:30-33,
+100, 110); a singular matrix makes det 0 and slogdet (0, -inf) (:402, :418-423).
+Like the reference loop, one singular matrix in a stack fails the whole solve /
+inv call. Unlike the reference, an empty stack returns an empty result (the
+reference indexes its first output there) and mismatched right-hand-side shapes
+raise ``ValueError`` before any device work.
+
+All GPU work goes through the C ABI (``_lib``); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+class LinAlgError(Exception):
+    """numpp::linalg_error (include/numpp/core/error.hpp:43-46)."""
+
+
+class Declined(NotImplementedError):
+    """The request is outside the B200 path (the GpuVTable slot would return false)."""
+
+
+class DeviceError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"numpp_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _check(rc: int) -> None:
+    if rc == _lib.OK:
+        return
+    if rc == _lib.DECLINED:
+        raise Declined(_lib.last_error() or "declined")
+    raise DeviceError(rc, _lib.last_error())
+
+
+class NativeBackend:
+    """The C ABI on host buffers: (count, n, n) float64 stacks in, numpy out."""
+
+    def __init__(self):
+        self.L = _lib.load()
+
+    def solve(self, A, B):
+        cnt, n = A.shape[0], A.shape[-1]
+        k = B.shape[-1]
+        X = np.empty_like(B)
+        info = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_solve_batched(cnt, n, k, _lib.ptr(A), _lib.ptr(B), _lib.ptr(X),
+                                         _lib.ptr(info)))
+        return X, info
+
+    def inv(self, A):
+        cnt, n = A.shape[0], A.shape[-1]
+        out = np.empty_like(A)
+        info = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_inv_batched(cnt, n, _lib.ptr(A), _lib.ptr(out), _lib.ptr(info)))
+        return out, info
+
+    def det(self, A):
+        cnt, n = A.shape[0], A.shape[-1]
+        out = np.empty(cnt)
+        _check(self.L.nppb_det_batched(cnt, n, _lib.ptr(A), _lib.ptr(out)))
+        return out
+
+    def slogdet(self, A):
+        cnt, n = A.shape[0], A.shape[-1]
+        s = np.empty(cnt)
+        la = np.empty(cnt)
+        _check(self.L.nppb_slogdet_batched(cnt, n, _lib.ptr(A), _lib.ptr(s), _lib.ptr(la)))
+        return s, la
+
+    def gemm(self, A, B):
+        m, k = A.shape
+        n = B.shape[1]
+        Cm = np.empty((m, n), A.dtype)
+        dt = _lib.DT_FLOAT64 if A.dtype == np.float64 else _lib.DT_FLOAT32
+        _check(self.L.nppb_gemm(dt, m, n, k, _lib.ptr(A), _lib.ptr(B), _lib.ptr(Cm)))
+        return Cm
+
+
+_default = None
+
+
+def default_backend():
+    global _default
+    if _default is None:
+        _default = NativeBackend()
+    return _default
+
+
+def _la_out(dt) -> np.dtype:
+    dt = np.dtype(dt)
+    if dt.kind == "c":
+        raise Declined("complex dtypes are served by NumPP's portable CPU path, not the B200 path")
+    if dt.kind not in "biuf":
+        raise TypeError(f"unsupported dtype {dt}")
+    return np.dtype(np.float32) if dt == np.float32 else np.dtype(np.float64)
+
+
+def _require_square(a) -> None:
+    if a.ndim != 2 or a.shape[0] != a.shape[1]:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+
+
+def _stack(a):
+    """(lead shape, count, n, (count, n, n) float64 contiguous) of a stack."""
+    if a.shape[-1] != a.shape[-2]:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+    lead = a.shape[:-2]
+    n = a.shape[-1]
+    cnt = int(np.prod(lead)) if lead else 1
+    A3 = np.ascontiguousarray(a, dtype=np.float64).reshape(cnt, n, n)
+    return lead, cnt, n, A3
+
+
+def solve(a, b, backend=None):
+    be = backend or default_backend()
+    a = np.asarray(a)
+    b = np.asarray(b)
+    out_dt = _la_out(np.result_type(a.dtype, b.dtype))
+    if a.ndim > 2:
+        lead, cnt, n, A3 = _stack(a)
+        bvec = b.ndim == a.ndim - 1
+        k = 1 if bvec else b.shape[-1]
+        if b.size != cnt * n * k or b.shape[-2 if not bvec else -1] != n:
+            raise ValueError(f"solve: b of shape {b.shape} does not match a of shape {a.shape}")
+        B3 = np.ascontiguousarray(b, dtype=np.float64).reshape(cnt, n, k)
+        out_shape = lead + ((n,) if bvec else (n, k))
+    else:
+        _require_square(a)
+        n = a.shape[0]
+        bvec = b.ndim == 1
+        if b.ndim not in (1, 2) or b.shape[0] != n:
+            raise ValueError(f"solve: b of shape {b.shape} does not match a of shape {a.shape}")
+        k = 1 if bvec else b.shape[1]
+        A3 = np.ascontiguousarray(a, dtype=np.float64).reshape(1, n, n)
+        B3 = np.ascontiguousarray(b, dtype=np.float64).reshape(1, n, k)
+        cnt = 1
+        out_shape = b.shape
+    if cnt == 0 or n == 0 or k == 0:
+        return np.zeros(out_shape, out_dt)
+    X, info = be.solve(A3, B3)
+    if np.any(info):
+        raise LinAlgError("Singular matrix")
+    return X.reshape(out_shape).astype(out_dt, copy=False)
+
+
+def inv(a, backend=None):
+    be = backend or default_backend()
+    a = np.asarray(a)
+    out_dt = _la_out(a.dtype)
+    if a.ndim > 2:
+        lead, cnt, n, A3 = _stack(a)
+    else:
+        _require_square(a)
+        lead, cnt, n = (), 1, a.shape[0]
+        A3 = np.ascontiguousarray(a, dtype=np.float64).reshape(1, n, n)
+    if cnt == 0 or n == 0:
+        return np.zeros(lead + (n, n), out_dt)
+    out, info = be.inv(A3)
+    if np.any(info):
+        raise LinAlgError("Singular matrix")
+    return out.reshape(lead + (n, n)).astype(out_dt, copy=False)
+
+
+def det(a, backend=None):
+    be = backend or default_backend()
+    a = np.asarray(a)
+    out_dt = _la_out(a.dtype)
+    if a.ndim > 2:
+        lead, cnt, n, A3 = _stack(a)
+    else:
+        _require_square(a)
+        lead, cnt, n = (), 1, a.shape[0]
+        A3 = np.ascontiguousarray(a, dtype=np.float64).reshape(1, n, n)
+    if cnt == 0:
+        return np.zeros(lead, out_dt)
+    return be.det(A3).reshape(lead).astype(out_dt, copy=False)
+
+
+def slogdet(a, backend=None):
+    """(sign, logabsdet), numpp::linalg::SignLogDet (linalg.hpp:22)."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    out_dt = _la_out(a.dtype)
+    if a.ndim > 2:
+        lead, cnt, n, A3 = _stack(a)
+    else:
+        _require_square(a)
+        lead, cnt, n = (), 1, a.shape[0]
+        A3 = np.ascontiguousarray(a, dtype=np.float64).reshape(1, n, n)
+    if cnt == 0:
+        return np.zeros(lead, out_dt), np.zeros(lead, out_dt)
+    s, la = be.slogdet(A3)
+    return (s.reshape(lead).astype(out_dt, copy=False),
+            la.reshape(lead).astype(out_dt, copy=False))
+
+
+def matmul(a, b, backend=None):
+    """numpp::matmul(a, b, Backend::Cuda) for float32 / float64 2-D operands."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.ndim != 2 or b.ndim != 2:
+        raise ValueError("matmul requires 2-D arrays")
+    if a.shape[1] != b.shape[0]:
+        raise ValueError("matmul: shape mismatch")
+    dt = np.result_type(a.dtype, b.dtype)
+    if dt not in (np.float32, np.float64):
+        raise Declined(f"the B200 gemm serves float32 and float64, not {dt}")
+    if a.shape[0] == 0 or b.shape[1] == 0:
+        return np.zeros((a.shape[0], b.shape[1]), dt)
+    return be.gemm(np.ascontiguousarray(a, dt), np.ascontiguousarray(b, dt))

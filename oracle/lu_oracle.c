@@ -1,0 +1,228 @@
+/*
+ * CPU ORACLE — TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of NumPP's portable dense linear-solve path, used by
+ * tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py as the
+ * checker. Nothing in the product (numpp_b200/) links, loads or calls it.
+ *
+ * Each function names the reference code it restates (paths are inside the
+ * CyberdyneCorp/NumPP tree). The arithmetic is the same sequence of IEEE
+ * double operations as the reference's templates compiled without FMA
+ * contraction (x86-64 baseline, no -mfma), so results are bit-identical to the
+ * reference build (checked against oracle/_ref and tests/golden/).
+ *
+ * Row-major everywhere. Status codes: 1 = ok, 0 = singular (exact zero pivot).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* src/linalg/linalg.cpp:48-71 (lu_decompose<T>): unblocked right-looking LU
+ * with partial pivoting. Column-k argmax of |A[i,k]| scanning i = k+1.. with a
+ * strict '>' so the first maximum wins; full-row swap; piv is the permutation
+ * vector (piv[i] = original row now at position i); permsign flips per swap.
+ * Returns 0 as soon as the best pivot is exactly 0.0 (A is then partly
+ * factored, as in the reference). */
+int oracle_lu_decompose(double* A, int n, int* piv, double* permsign) {
+  for (int i = 0; i < n; ++i) piv[i] = i;
+  *permsign = 1.0;
+  for (int k = 0; k < n; ++k) {
+    int pr = k;
+    double best = fabs(A[(int64_t)k * n + k]);
+    for (int i = k + 1; i < n; ++i) {
+      double v = fabs(A[(int64_t)i * n + k]);
+      if (v > best) { best = v; pr = i; }
+    }
+    if (best == 0.0) return 0;
+    if (pr != k) {
+      for (int j = 0; j < n; ++j) {
+        double t = A[(int64_t)k * n + j];
+        A[(int64_t)k * n + j] = A[(int64_t)pr * n + j];
+        A[(int64_t)pr * n + j] = t;
+      }
+      int t = piv[k]; piv[k] = piv[pr]; piv[pr] = t;
+      *permsign = -*permsign;
+    }
+    const double akk = A[(int64_t)k * n + k];
+    for (int i = k + 1; i < n; ++i) {
+      double f = A[(int64_t)i * n + k] / akk;
+      A[(int64_t)i * n + k] = f;
+      double* ri = A + (int64_t)i * n;
+      const double* rk = A + (int64_t)k * n;
+      for (int j = k + 1; j < n; ++j) {
+        double p = f * rk[j]; /* separate multiply and subtract: no FMA */
+        ri[j] = ri[j] - p;
+      }
+    }
+  }
+  return 1;
+}
+
+/* src/linalg/linalg.cpp:73-90 (lu_solve<T>): X[i,:] = B[piv[i],:], forward
+ * substitution with the unit lower factor, back substitution with the upper
+ * factor, dividing by the diagonal last. B is n x m row-major, overwritten. */
+void oracle_lu_solve(const double* LU, int n, const int* piv, double* B, int m) {
+  size_t sz = (size_t)n * (size_t)m;
+  double* X = (double*)malloc(sz ? sz * sizeof(double) : 1);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < m; ++j) X[(int64_t)i * m + j] = B[(int64_t)piv[i] * m + j];
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < i; ++k) {
+      double l = LU[(int64_t)i * n + k];
+      for (int j = 0; j < m; ++j) {
+        double p = l * X[(int64_t)k * m + j];
+        X[(int64_t)i * m + j] = X[(int64_t)i * m + j] - p;
+      }
+    }
+  for (int i = n - 1; i >= 0; --i) {
+    for (int k = i + 1; k < n; ++k) {
+      double u = LU[(int64_t)i * n + k];
+      for (int j = 0; j < m; ++j) {
+        double p = u * X[(int64_t)k * m + j];
+        X[(int64_t)i * m + j] = X[(int64_t)i * m + j] - p;
+      }
+    }
+    double d = LU[(int64_t)i * n + i];
+    for (int j = 0; j < m; ++j) X[(int64_t)i * m + j] /= d;
+  }
+  if (sz) memcpy(B, X, sz * sizeof(double));
+  free(X);
+}
+
+/* src/linalg/linalg.cpp:92-103 (solve_impl): LU of a copy of A, then lu_solve.
+ * Returns 0 (the reference throws linalg_error("Singular matrix")). */
+int oracle_solve(const double* A, const double* B, double* X, int n, int m) {
+  size_t nn = (size_t)n * n;
+  double* W = (double*)malloc(nn ? nn * sizeof(double) : 1);
+  int* piv = (int*)malloc(n ? n * sizeof(int) : 1);
+  double sgn;
+  if (nn) memcpy(W, A, nn * sizeof(double));
+  int ok = oracle_lu_decompose(W, n, piv, &sgn);
+  if (ok) {
+    if (n && m) memcpy(X, B, (size_t)n * m * sizeof(double));
+    oracle_lu_solve(W, n, piv, X, m);
+  }
+  free(W); free(piv);
+  return ok;
+}
+
+/* src/linalg/linalg.cpp:105-115 (inv_impl): LU, then lu_solve against I. */
+int oracle_inv(const double* A, double* Ainv, int n) {
+  size_t nn = (size_t)n * n;
+  double* W = (double*)malloc(nn ? nn * sizeof(double) : 1);
+  int* piv = (int*)malloc(n ? n * sizeof(int) : 1);
+  double sgn;
+  if (nn) memcpy(W, A, nn * sizeof(double));
+  int ok = oracle_lu_decompose(W, n, piv, &sgn);
+  if (ok) {
+    for (size_t i = 0; i < nn; ++i) Ainv[i] = 0.0;
+    for (int i = 0; i < n; ++i) Ainv[(int64_t)i * n + i] = 1.0;
+    oracle_lu_solve(W, n, piv, Ainv, n);
+  }
+  free(W); free(piv);
+  return ok;
+}
+
+/* src/linalg/linalg.cpp:393-407 (det): permsign * prod U[i,i] multiplied in
+ * order i = 0..n-1; a singular matrix gives 0.0 (no exception). n = 0 gives 1. */
+double oracle_det(const double* A, int n) {
+  size_t nn = (size_t)n * n;
+  double* W = (double*)malloc(nn ? nn * sizeof(double) : 1);
+  int* piv = (int*)malloc(n ? n * sizeof(int) : 1);
+  double sgn, d;
+  if (nn) memcpy(W, A, nn * sizeof(double));
+  if (!oracle_lu_decompose(W, n, piv, &sgn)) d = 0.0;
+  else { d = sgn; for (int i = 0; i < n; ++i) d *= W[(int64_t)i * n + i]; }
+  free(W); free(piv);
+  return d;
+}
+
+/* src/linalg/linalg.cpp:408-439 (slogdet): logabsdet = sum log|d_i| and
+ * sign *= d_i/|d_i| in order; singular gives (0, -inf). */
+void oracle_slogdet(const double* A, int n, double* sign, double* logabsdet) {
+  size_t nn = (size_t)n * n;
+  double* W = (double*)malloc(nn ? nn * sizeof(double) : 1);
+  int* piv = (int*)malloc(n ? n * sizeof(int) : 1);
+  double sgn;
+  if (nn) memcpy(W, A, nn * sizeof(double));
+  if (!oracle_lu_decompose(W, n, piv, &sgn)) {
+    *sign = 0.0;
+    *logabsdet = -INFINITY;
+  } else {
+    double logabs = 0.0, s = sgn;
+    for (int i = 0; i < n; ++i) {
+      double d = W[(int64_t)i * n + i];
+      double m = fabs(d);
+      logabs += log(m);
+      s *= d / m;
+    }
+    *sign = s;
+    *logabsdet = logabs;
+  }
+  free(W); free(piv);
+}
+
+/* src/backend/backend.cpp:55-84 (cpu_matmul): C[m,n] = A[m,k] B[k,n] with the
+ * i-p-j loop order, accumulated in p order. */
+void oracle_matmul(int64_t m, int64_t n, int64_t k, const double* A, const double* B, double* C) {
+  for (int64_t i = 0; i < m; ++i) {
+    for (int64_t j = 0; j < n; ++j) C[i * n + j] = 0.0;
+    for (int64_t p = 0; p < k; ++p) {
+      const double aip = A[i * k + p];
+      const double* brow = B + p * n;
+      double* crow = C + i * n;
+      for (int64_t j = 0; j < n; ++j) {
+        double t = aip * brow[j];
+        crow[j] = crow[j] + t;
+      }
+    }
+  }
+}
+
+/* ---- stacked forms: src/linalg/batched.cpp:51-108 loop the 2-D routine over
+ * a contiguous (count, n, n) view. The reference aborts the whole call on the
+ * first singular matrix; here each matrix reports its own status in ok[] so a
+ * test can check both behaviours. ---- */
+
+void oracle_lu_batched(int64_t count, int n, double* A, int* piv, double* permsign, int* ok) {
+  for (int64_t b = 0; b < count; ++b)
+    ok[b] = oracle_lu_decompose(A + b * (int64_t)n * n, n, piv + b * n, permsign + b);
+}
+
+void oracle_solve_batched(int64_t count, int n, int m, const double* A, const double* B,
+                          double* X, int* ok) {
+  for (int64_t b = 0; b < count; ++b)
+    ok[b] = oracle_solve(A + b * (int64_t)n * n, B + b * (int64_t)n * m,
+                         X + b * (int64_t)n * m, n, m);
+}
+
+void oracle_inv_batched(int64_t count, int n, const double* A, double* Ainv, int* ok) {
+  for (int64_t b = 0; b < count; ++b)
+    ok[b] = oracle_inv(A + b * (int64_t)n * n, Ainv + b * (int64_t)n * n, n);
+}
+
+void oracle_det_batched(int64_t count, int n, const double* A, double* det) {
+  for (int64_t b = 0; b < count; ++b) det[b] = oracle_det(A + b * (int64_t)n * n, n);
+}
+
+void oracle_slogdet_batched(int64_t count, int n, const double* A, double* sign, double* logabsdet) {
+  for (int64_t b = 0; b < count; ++b)
+    oracle_slogdet(A + b * (int64_t)n * n, n, sign + b, logabsdet + b);
+}
+
+/* Uneven batch: system i has order n[i] and nrhs[i], its matrix at a_off[i]
+ * and its right-hand side / solution at b_off[i] (element offsets). Each system
+ * is the 2-D reference call (linalg.cpp:368-385, 393-439, 386-392). inv_off[i]
+ * < 0 means no inverse for that system. */
+void oracle_solve_grouped(int64_t count, const int* n, const int* nrhs, const int64_t* a_off,
+                          const int64_t* b_off, const int64_t* inv_off, const double* A,
+                          const double* B, double* X, double* sign, double* logabsdet,
+                          double* inv, int* ok) {
+  for (int64_t i = 0; i < count; ++i) {
+    const double* Ai = A + a_off[i];
+    ok[i] = oracle_solve(Ai, B + b_off[i], X + b_off[i], n[i], nrhs[i]);
+    if (sign) oracle_slogdet(Ai, n[i], sign + i, logabsdet + i);
+    if (inv && inv_off[i] >= 0) oracle_inv(Ai, inv + inv_off[i], n[i]);
+  }
+}

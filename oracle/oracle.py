@@ -1,0 +1,262 @@
+"""ctypes loaders for the two CPU checkers (test infrastructure only)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORACLE_SO = os.path.join(_HERE, "liboracle.so")
+_REF_SO = os.path.join(_HERE, "_ref", "libnumpp_ref.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_i32p = C.POINTER(C.c_int32)
+_i64p = C.POINTER(C.c_int64)
+
+F64 = 11  # numpp::DTypeId::Float64
+F32 = 10  # numpp::DTypeId::Float32
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def build_oracle() -> None:
+    """Compile liboracle.so (and the reference library when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    if os.path.isdir(os.environ.get("NUMPP_REF_SRC", "/root/reference")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+
+
+class Oracle:
+    """The C restatement of the reference's portable LU path."""
+
+    def __init__(self, path: str = _ORACLE_SO):
+        if not os.path.exists(path):
+            build_oracle()
+        L = C.CDLL(path)
+        L.oracle_lu_decompose.argtypes = [_dp, C.c_int, _ip, _dp]
+        L.oracle_solve.argtypes = [_dp, _dp, _dp, C.c_int, C.c_int]
+        L.oracle_inv.argtypes = [_dp, _dp, C.c_int]
+        L.oracle_det.argtypes = [_dp, C.c_int]
+        L.oracle_det.restype = C.c_double
+        L.oracle_slogdet.argtypes = [_dp, C.c_int, _dp, _dp]
+        L.oracle_matmul.argtypes = [C.c_int64, C.c_int64, C.c_int64, _dp, _dp, _dp]
+        L.oracle_lu_batched.argtypes = [C.c_int64, C.c_int, _dp, _ip, _dp, _ip]
+        L.oracle_solve_batched.argtypes = [C.c_int64, C.c_int, C.c_int, _dp, _dp, _dp, _ip]
+        L.oracle_inv_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _ip]
+        L.oracle_det_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp]
+        L.oracle_slogdet_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _dp]
+        L.oracle_solve_grouped.argtypes = [C.c_int64, _ip, _ip, _i64p, _i64p, _i64p,
+                                           _dp, _dp, _dp, _dp, _dp, _dp, _ip]
+        self.L = L
+
+    # -- stacked (count, n, n) helpers; every array is float64 C-contiguous --
+    def lu(self, A):
+        A = np.array(A, dtype=np.float64, order="C", copy=True)
+        cnt, n = A.shape[0], A.shape[-1]
+        piv = np.zeros((cnt, n), np.intc)
+        sgn = np.zeros(cnt)
+        ok = np.zeros(cnt, np.intc)
+        self.L.oracle_lu_batched(cnt, n, _ptr(A), _ptr(piv, _ip), _ptr(sgn), _ptr(ok, _ip))
+        return A, piv, sgn, ok
+
+    def solve(self, A, B):
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.ascontiguousarray(B, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        m = B.shape[-1] if B.ndim == 3 else 1
+        X = np.zeros_like(B)
+        ok = np.zeros(cnt, np.intc)
+        self.L.oracle_solve_batched(cnt, n, m, _ptr(A), _ptr(B), _ptr(X), _ptr(ok, _ip))
+        return X, ok
+
+    def inv(self, A):
+        A = np.ascontiguousarray(A, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        out = np.zeros_like(A)
+        ok = np.zeros(cnt, np.intc)
+        self.L.oracle_inv_batched(cnt, n, _ptr(A), _ptr(out), _ptr(ok, _ip))
+        return out, ok
+
+    def det(self, A):
+        A = np.ascontiguousarray(A, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        out = np.zeros(cnt)
+        self.L.oracle_det_batched(cnt, n, _ptr(A), _ptr(out))
+        return out
+
+    def slogdet(self, A):
+        A = np.ascontiguousarray(A, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        s = np.zeros(cnt)
+        la = np.zeros(cnt)
+        self.L.oracle_slogdet_batched(cnt, n, _ptr(A), _ptr(s), _ptr(la))
+        return s, la
+
+    def matmul(self, A, B):
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.ascontiguousarray(B, np.float64)
+        m, k = A.shape
+        n = B.shape[1]
+        Cm = np.zeros((m, n))
+        self.L.oracle_matmul(m, n, k, _ptr(A), _ptr(B), _ptr(Cm))
+        return Cm
+
+    def solve_grouped(self, sys, want_slogdet=True, want_inv=True):
+        """sys: a packed uneven batch (numpp_b200 grouped layout as a dict of arrays)."""
+        cnt = len(sys["n"])
+        n = np.ascontiguousarray(sys["n"], np.intc)
+        k = np.ascontiguousarray(sys["nrhs"], np.intc)
+        X = np.zeros_like(sys["B"])
+        s = np.zeros(cnt) if want_slogdet else None
+        la = np.zeros(cnt) if want_slogdet else None
+        inv = np.zeros(max(int(sys["inv_size"]), 1)) if want_inv else None
+        ok = np.zeros(cnt, np.intc)
+        self.L.oracle_solve_grouped(cnt, _ptr(n, _ip), _ptr(k, _ip), _ptr(sys["a_off"], _i64p),
+                                    _ptr(sys["b_off"], _i64p), _ptr(sys["inv_off"], _i64p),
+                                    _ptr(sys["A"]), _ptr(sys["B"]), _ptr(X), _ptr(s), _ptr(la),
+                                    _ptr(inv), _ptr(ok, _ip))
+        return X, s, la, inv, ok
+
+
+class RefError(Exception):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class RefLib:
+    """The reference's own public API (numpp::linalg / numpp::matmul)."""
+
+    def __init__(self, path: str = _REF_SO):
+        L = C.CDLL(path)
+        vp = C.c_void_p
+        cp = C.c_char_p
+        L.ref_solve.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int, _i64p, C.c_int, vp, vp,
+                                _ip, _i64p, cp, C.c_int]
+        L.ref_inv.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
+        L.ref_det.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
+        L.ref_slogdet.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, vp, _ip, _i64p, cp, C.c_int]
+        L.ref_matmul_cpu.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int, vp, vp, vp, cp, C.c_int]
+        L.ref_solve_grouped.argtypes = [C.c_int64, _i32p, _i32p, _i64p, _i64p, _i64p, _dp, _dp,
+                                        _dp, _dp, _dp, _dp, _i32p, C.c_int]
+        L.ref_standard_normal2.argtypes = [C.c_uint64, C.c_int64, _dp, C.c_int64, _dp]
+        L.ref_uniform.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_int64, _dp]
+        self.L = L
+
+    @staticmethod
+    def _dt(a):
+        if a.dtype == np.float64:
+            return F64
+        if a.dtype == np.float32:
+            return F32
+        raise TypeError(a.dtype)
+
+    @staticmethod
+    def _np(dt):
+        return np.float64 if dt == F64 else np.float32
+
+    def _call(self, fn, *args):
+        err = C.create_string_buffer(256)
+        rc = fn(*args, err, 256)
+        if rc:
+            raise RefError(rc, err.value.decode())
+
+    def solve(self, A, B):
+        A = np.ascontiguousarray(A)
+        B = np.ascontiguousarray(B)
+        sa = np.array(A.shape, np.int64)
+        sb = np.array(B.shape, np.int64)
+        out = np.zeros(B.size, np.float64)  # large enough for either dtype
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(self.L.ref_solve, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data, B.ndim,
+                   _ptr(sb, _i64p), self._dt(B), B.ctypes.data, out.ctypes.data, C.byref(dt),
+                   C.byref(sz))
+        return np.frombuffer(out.tobytes(), self._np(dt.value), sz.value).reshape(B.shape)
+
+    def _unary(self, fn, A, out_shape):
+        A = np.ascontiguousarray(A)
+        sa = np.array(A.shape, np.int64)
+        out = np.zeros(max(int(np.prod(out_shape)), 1), np.float64)
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(fn, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data, out.ctypes.data,
+                   C.byref(dt), C.byref(sz))
+        return np.frombuffer(out.tobytes(), self._np(dt.value), sz.value).reshape(out_shape)
+
+    def inv(self, A):
+        return self._unary(self.L.ref_inv, A, A.shape)
+
+    def det(self, A):
+        return self._unary(self.L.ref_det, A, A.shape[:-2])
+
+    def slogdet(self, A):
+        A = np.ascontiguousarray(A)
+        sa = np.array(A.shape, np.int64)
+        shp = A.shape[:-2]
+        cnt = max(int(np.prod(shp)), 1)
+        s = np.zeros(cnt)
+        la = np.zeros(cnt)
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(self.L.ref_slogdet, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data,
+                   s.ctypes.data, la.ctypes.data, C.byref(dt), C.byref(sz))
+        if dt.value == F32:
+            s = np.frombuffer(s.tobytes(), np.float32, sz.value)
+            la = np.frombuffer(la.tobytes(), np.float32, sz.value)
+        return s[: sz.value].reshape(shp), la[: sz.value].reshape(shp)
+
+    def matmul(self, A, B):
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.ascontiguousarray(B, np.float64)
+        Cm = np.zeros((A.shape[0], B.shape[1]))
+        self._call(self.L.ref_matmul_cpu, A.shape[0], B.shape[1], A.shape[1], F64, A.ctypes.data,
+                   B.ctypes.data, Cm.ctypes.data)
+        return Cm
+
+    def standard_normal2(self, seed, n1, n2):
+        a = np.zeros(n1)
+        b = np.zeros(n2)
+        rc = self.L.ref_standard_normal2(seed, n1, _ptr(a), n2, _ptr(b))
+        if rc:
+            raise RefError(rc, "standard_normal failed")
+        return a, b
+
+    def uniform(self, seed, low, high, n):
+        out = np.zeros(n)
+        rc = self.L.ref_uniform(seed, low, high, n, _ptr(out))
+        if rc:
+            raise RefError(rc, "uniform failed")
+        return out
+
+    def solve_grouped(self, sys, want_slogdet=True, want_inv=True, threads=1):
+        cnt = len(sys["n"])
+        n = np.ascontiguousarray(sys["n"], np.int32)
+        k = np.ascontiguousarray(sys["nrhs"], np.int32)
+        X = np.zeros_like(sys["B"])
+        s = np.zeros(cnt) if want_slogdet else None
+        la = np.zeros(cnt) if want_slogdet else None
+        inv = np.zeros(max(int(sys["inv_size"]), 1)) if want_inv else None
+        ok = np.zeros(cnt, np.int32)
+        self.L.ref_solve_grouped(cnt, _ptr(n, _i32p), _ptr(k, _i32p), _ptr(sys["a_off"], _i64p),
+                                 _ptr(sys["b_off"], _i64p), _ptr(sys["inv_off"], _i64p),
+                                 _ptr(sys["A"]), _ptr(sys["B"]), _ptr(X), _ptr(s), _ptr(la),
+                                 _ptr(inv), _ptr(ok, _i32p), threads)
+        return X, s, la, inv, ok
+
+
+def load_oracle() -> Oracle:
+    return Oracle()
+
+
+def ref_available() -> bool:
+    return os.path.exists(_REF_SO)
+
+
+def load_ref() -> RefLib:
+    return RefLib()
