@@ -334,7 +334,8 @@ k_lu_cta(Batch bt, const int32_t* __restrict__ order, int nsys, int nmax) {
       if (tid == 0) {
         for (int i = 0; i < n; ++i) s.perm[i] = i;
         for (int k = 0; k < n; ++k) {
-          const int p = v.ipiv[k];
+          int p = v.ipiv[k];
+          if (p < k || p >= n) p = k;  // a swap list only names rows >= k; ignore anything else
           const int t = s.perm[k]; s.perm[k] = s.perm[p]; s.perm[p] = t;
         }
       }

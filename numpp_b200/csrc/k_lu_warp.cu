@@ -100,7 +100,8 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
     if (lane == 0) {
       for (int i = 0; i < n; ++i) s_lane_of_pos[wib][i] = i;
       for (int k = 0; k < n; ++k) {
-        const int p = v.ipiv[k];
+        int p = v.ipiv[k];
+        if (p < k || p >= n) p = k;  // a swap list only names rows >= k; ignore anything else
         const int t = s_lane_of_pos[wib][k];
         s_lane_of_pos[wib][k] = s_lane_of_pos[wib][p];
         s_lane_of_pos[wib][p] = t;
