@@ -8,6 +8,7 @@
 #include <string>
 
 #include "../../include/numpp_b200.h"
+#include "plan.hpp"
 #include "runtime.hpp"
 
 using namespace nppb;
@@ -40,8 +41,8 @@ int check_shape(int64_t count, int32_t n, int32_t nrhs) {
     set_error("batch count above 2^31-1");
     return NPPB_E_RANGE;
   }
-  if (n > kCtaMaxN) {
-    set_error("order above " + std::to_string(kCtaMaxN) + " is not served by the batched path");
+  if (n > kStepMaxN) {
+    set_error("order above " + std::to_string(kStepMaxN) + " is not served by the batched path");
     return NPPB_E_RANGE;
   }
   return NPPB_OK;
@@ -97,6 +98,20 @@ int d_linalg(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA
   if ((flags & NPPB_WANT_SLOGDET) && (!dSign || !dLogabs)) return arg_error("slogdet needs Sign and Logabs");
   if ((flags & NPPB_WANT_LU) && nn && (!dLU || !dipiv)) return arg_error("keeping factors needs LU and ipiv");
   if (!device()) return NPPB_E_NODEV;
+  if (n > 32) {
+    // step-wise path through a cached uniform plan
+    int rc = NPPB_OK;
+    const bool own_lu = dLU == nullptr;
+    auto pl = uniform_plan(count, n, nrhs, flags, false, own_lu, &rc);
+    if (!pl) return rc;
+    Plan::Ptrs p{};
+    p.A = (dLU && dA == dLU) ? nullptr : dA;
+    p.B = dB; p.X = dX; p.Inv = dInv; p.Det = dDet; p.Sign = dSign; p.Logabs = dLogabs;
+    p.info = dinfo;
+    p.LU = own_lu ? pl->d_lu : dLU;
+    p.ipiv = dipiv ? dipiv : pl->d_piv;
+    return pl->execute(p, st);
+  }
   DevMem lu_m, piv_m;
   double* LU = dLU;
   int32_t* piv = dipiv;
@@ -114,7 +129,7 @@ int d_linalg(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA
   bt.det = dDet; bt.sign = dSign; bt.logabs = dLogabs; bt.info = dinfo;
   bt.desc = nullptr; bt.n = n; bt.nrhs = nrhs;
   bt.flags = flags | (dA == LU ? kInPlace : 0);
-  NPPB_CUDA(run_uniform(bt, count, n, st), "batched LU launch");
+  NPPB_CUDA(run_warp_uniform(bt, count, n, st), "batched LU launch");
   return NPPB_OK;
 }
 
@@ -124,11 +139,31 @@ int d_getrs(int64_t count, int32_t n, int32_t nrhs, const double* dLU, const int
   if (count == 0 || n == 0 || nrhs == 0) return NPPB_OK;
   if (!dLU || !dipiv || !dB || !dX) return arg_error("getrs needs LU, ipiv, B and X");
   if (!device()) return NPPB_E_NODEV;
+  if (n > 32) {
+    int rc = NPPB_OK;
+    auto pl = uniform_plan(count, n, nrhs, NPPB_WANT_SOLVE, true, false, &rc);
+    if (!pl) return rc;
+    DevMem tmp;
+    double* X = dX;
+    if (dX == dB) {  // the row gather needs a separate output
+      NPPB_RC(scratch<double>(tmp, (size_t)count * n * nrhs, st));
+      X = tmp.as<double>();
+    }
+    Plan::Ptrs p{};
+    p.B = dB; p.X = X;
+    p.LU = const_cast<double*>(dLU);
+    p.ipiv = const_cast<int32_t*>(dipiv);
+    NPPB_RC(pl->execute(p, st));
+    if (X != dX)
+      NPPB_CUDA(cudaMemcpyAsync(dX, X, sizeof(double) * count * n * nrhs, cudaMemcpyDeviceToDevice, st),
+                "device copy");
+    return NPPB_OK;
+  }
   Batch bt{};
   bt.A = dLU; bt.LU = const_cast<double*>(dLU); bt.ipiv = const_cast<int32_t*>(dipiv);
   bt.B = dB; bt.X = dX; bt.n = n; bt.nrhs = nrhs;
   bt.flags = kSolveOnly | kWantSolve | kInPlace;
-  NPPB_CUDA(run_uniform(bt, count, n, st), "getrs launch");
+  NPPB_CUDA(run_warp_uniform(bt, count, n, st), "getrs launch");
   return NPPB_OK;
 }
 
@@ -187,7 +222,7 @@ int nppb_device_available(void) {
 
 const char* nppb_last_error(void) { return last_error(); }
 
-int32_t nppb_max_order(void) { return kCtaMaxN; }
+int32_t nppb_max_order(void) { return kStepMaxN; }
 
 int nppb_elementwise_binary(int, int, int64_t, const void*, const void*, void*) { return NPPB_DECLINED; }
 int nppb_elementwise_unary(int, int, int64_t, const void*, void*) { return NPPB_DECLINED; }

@@ -166,6 +166,7 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
         }
         x[c] = b;
       }
+      __syncwarp();  // every lane has read its right-hand side before any lane writes X (getrs in place)
       // forward: unit lower, position order
 #pragma unroll 64
       for (int k = 0; k < NP; ++k) {

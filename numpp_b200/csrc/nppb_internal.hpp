@@ -96,15 +96,6 @@ __device__ __forceinline__ SysView sys_view(const Batch& bt, int s) {
 cudaError_t launch_lu_warp(const Batch& bt, const int32_t* order, int nsys, int np,
                            cudaStream_t st);
 
-// Orders up to kCtaMaxN: one CTA per system, blocked right-looking LU with FP64
-// DMMA trailing updates, then getrs / inverse in shared-memory chunks.
-// The grid is persistent: CTAs stride over the `nsys` systems in `order`.
-constexpr int kCtaMaxN = 512;
-cudaError_t lu_cta_prepare();                 // opt in to the dynamic shared memory
-int lu_cta_blocks_per_sm(int nmax);           // occupancy for a class of order <= nmax
-cudaError_t launch_lu_cta(const Batch& bt, const int32_t* order, int nsys, int nmax, int grid,
-                          cudaStream_t st);
-
 // Row-major C[m,n] = A[m,k] B[k,n] in FP64 on DMMA (device pointers).
 cudaError_t launch_gemm_f64(int64_t m, int64_t n, int64_t k, const double* A, int64_t lda,
                             const double* B, int64_t ldb, double* C, int64_t ldc,

@@ -1,0 +1,68 @@
+// Step-wise batched LU (orders > 32): shared types of k_step.cu and plan.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "nppb_internal.hpp"
+
+namespace nppb {
+
+constexpr int kStepNB = 32;     // panel width
+constexpr int kStepMaxN = 512;  // largest order the register panel holds (2 rows x 256 threads)
+
+// Per-system state carried from one step to the next (one slot per system,
+// SysDesc::pad_ is the slot index).
+struct StepScratch {
+  double linv[kStepNB * kStepNB];  // L11^-1 of the current panel, row-major
+  int top_src[kStepNB];            // panel-relative source row of each top position
+  int disp_dst[kStepNB];           // displaced old top rows: their new positions
+  int disp_src[kStepNB];           //   ... and their old positions
+  int ndisp;
+  int info;                        // 0, or first zero pivot + 1 (later launches skip)
+  int nswap;
+  int pad_;
+  double det, logabs, sign;        // running det / log|det| / sign
+};
+
+// Strip kinds.
+enum : int16_t { kSegMatrix = 0, kSegRhs = 1, kSegInv = 2, kSegLeft = 3 };
+
+// One CTA of k_update / k_back / k_forward: a 64-column strip of one system.
+struct StepItem {
+  int32_t sys;    // index into desc
+  int16_t kind;
+  int16_t width;  // columns in this strip (<= 64)
+  int32_t c0;     // first column
+  int32_t pad_;
+};
+
+struct StepArgs {
+  const SysDesc* desc;
+  StepScratch* scratch;
+  const double* A;   // step-0 source of the matrices (nullptr: factor LU in place)
+  double* LU;
+  int32_t* ipiv;
+  const double* B;
+  double* X;
+  double* inv;
+  double* det;
+  double* sign;
+  double* logabs;
+  int32_t* info;
+  int solve_only;    // getrs from stored factors: no factorisation state to consult
+};
+
+cudaError_t step_prepare();
+// Panel of every listed system at column k0; mmax = largest n - k0 among them.
+cudaError_t launch_panel(const StepArgs& sa, const int32_t* list, int nsys, int mmax, int k0,
+                         cudaStream_t st);
+// Row moves + U12 + trailing update for each strip item of step k0 (nmax >= n of any item).
+cudaError_t launch_update(const StepArgs& sa, const StepItem* items, int nitems, int nmax, int k0,
+                          cudaStream_t st);
+cudaError_t launch_back(const StepArgs& sa, const StepItem* items, int nitems, cudaStream_t st);
+cudaError_t launch_forward(const StepArgs& sa, const StepItem* items, int nitems, int nmax,
+                           cudaStream_t st);
+
+}  // namespace nppb

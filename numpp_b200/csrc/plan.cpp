@@ -1,68 +1,68 @@
-// Uneven batches: size-class packing, one persistent launch per class, the
-// classes replayed together as one CUDA graph. C++20.
+// Batched execution plans: size classes, step schedules, CUDA graphs. C++20.
 //
 // The reference loops the 2-D routine over every matrix of a stack
 // (src/linalg/batched.cpp:51-108); systems of different orders are separate
-// calls there. Here a plan sorts the systems into classes by order
-// (<=8, <=16, <=32 on the warp kernel; <=64, <=128, <=256, <=512 on the CTA
-// kernel), longest first inside a class so the persistent CTAs finish
-// together, uploads the descriptors once, and on execute launches every class
-// on its own stream branch of a captured graph so classes share the GPU.
-#include <cuda_runtime.h>
+// calls there. A plan takes a whole (possibly uneven) batch at once:
+//  * orders <= 32 go to the warp-per-system kernel, one launch per padded order
+//    class (8 / 16 / 32);
+//  * orders 33..512 go to the step-wise path: systems sorted by order, step s
+//    (columns 32s..32s+31) is one panel launch per panel-height class plus one
+//    update launch over every (system, 64-column strip) still active, then one
+//    back-substitution launch.
+// Descriptors, work lists and workspaces are built and uploaded once; execute
+// replays everything as one CUDA graph whose branches (warp classes, step
+// chain) overlap on the GPU.
+#include "plan.hpp"
 
 #include <algorithm>
-#include <array>
 #include <cstdlib>
 #include <cstring>
+#include <list>
 #include <mutex>
 #include <new>
 #include <string>
-#include <vector>
+#include <tuple>
 
 #include "../../include/numpp_b200.h"
-#include "runtime.hpp"
 
-using namespace nppb;
+namespace nppb {
+namespace {
 
-struct nppb_plan {
-  struct Class {
-    bool warp;      // warp kernel (np) or CTA kernel (nmax)
-    int bound;      // np or nmax
-    int64_t first;  // slice of h_order
-    int64_t num;
-    int grid;       // CTA kernel only
-    double flops;   // algorithmic (LAPACK counts) of the outputs asked for
-    double bytes;   // algorithmic minimum traffic
-  };
-  int dev = -1;
-  int64_t count = 0;
-  int flags = 0;
-  int64_t a_elems = 0, b_elems = 0, inv_elems = 0, lu_elems = 0, piv_elems = 0;
-  std::vector<Class> classes;
-  SysDesc* d_desc = nullptr;
-  int32_t* d_order = nullptr;
-  double* d_lu = nullptr;
-  int32_t* d_piv = nullptr;
+int arg_error(const std::string& m) {
+  set_error(m);
+  return NPPB_E_ARG;
+}
 
-  std::mutex mu;
-  bool use_graph = true;
-  std::array<const void*, 8> key{};
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaStream_t cap = nullptr;
-  std::vector<cudaStream_t> side;
-  cudaEvent_t fork = nullptr;
-  std::vector<cudaEvent_t> join;
+#define NPPB_CUDA(call, what)                            \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return nppb::cuda_status(e_, what); \
+  } while (0)
 
-  // device staging for execute_host, allocated on first use
-  double *hA = nullptr, *hB = nullptr, *hX = nullptr, *hInv = nullptr, *hDet = nullptr,
-         *hSign = nullptr, *hLog = nullptr;
-  int32_t* hInfo = nullptr;
+template <class T>
+int upload(T** d, const std::vector<T>& h) {
+  if (h.empty()) return NPPB_OK;
+  NPPB_CUDA(cudaMalloc(d, sizeof(T) * h.size()), "plan allocation");
+  NPPB_CUDA(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "plan upload");
+  return NPPB_OK;
+}
 
-  ~nppb_plan();
-};
+int panel_class(int m) { return m <= 64 ? 0 : m <= 128 ? 1 : m <= 256 ? 2 : 3; }
 
-nppb_plan::~nppb_plan() {
+void add_strips(std::vector<StepItem>& out, int32_t sys, int16_t kind, int c0, int c1) {
+  for (int c = c0; c < c1; c += 64) {
+    StepItem it{};
+    it.sys = sys;
+    it.kind = kind;
+    it.width = (int16_t)std::min(64, c1 - c);
+    it.c0 = c;
+    out.push_back(it);
+  }
+}
+
+}  // namespace
+
+Plan::~Plan() {
   int prev = -1;
   cudaGetDevice(&prev);
   if (dev >= 0) cudaSetDevice(dev);
@@ -71,78 +71,43 @@ nppb_plan::~nppb_plan() {
   for (auto s : side) cudaStreamDestroy(s);
   for (auto e : join) cudaEventDestroy(e);
   if (fork) cudaEventDestroy(fork);
+  if (done) cudaEventDestroy(done);
   if (cap) cudaStreamDestroy(cap);
-  for (void* p : {(void*)d_desc, (void*)d_order, (void*)d_lu, (void*)d_piv, (void*)hA, (void*)hB,
-                  (void*)hX, (void*)hInv, (void*)hDet, (void*)hSign, (void*)hLog, (void*)hInfo})
+  for (void* p : {(void*)d_desc, (void*)d_order, (void*)d_lu, (void*)d_piv, (void*)d_scratch,
+                  (void*)d_step_list, (void*)d_items, (void*)d_back, (void*)hA, (void*)hB, (void*)hX,
+                  (void*)hInv, (void*)hDet, (void*)hSign, (void*)hLog, (void*)hInfo})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
-namespace {
-
-// p: A, B, X, Inv, Det, Sign, Logabs, info
-Batch plan_batch(const nppb_plan& pl, const void* const* p) {
-  Batch bt{};
-  bt.A = (const double*)p[0];
-  bt.B = (const double*)p[1];
-  bt.X = (double*)p[2];
-  bt.inv = (pl.flags & NPPB_WANT_INV) ? (double*)p[3] : nullptr;
-  bt.det = (double*)p[4];
-  bt.sign = (double*)p[5];
-  bt.logabs = (double*)p[6];
-  bt.info = (int32_t*)p[7];
-  bt.LU = pl.d_lu;
-  bt.ipiv = pl.d_piv;
-  bt.desc = pl.d_desc;
-  bt.flags = pl.flags & ~NPPB_WANT_LU;
-  return bt;
-}
-
-cudaError_t launch_class(const nppb_plan& pl, const nppb_plan::Class& c, const Batch& bt,
-                         cudaStream_t st) {
-  const int32_t* order = pl.d_order + c.first;
-  if (c.warp) return launch_lu_warp(bt, order, (int)c.num, c.bound, st);
-  return launch_lu_cta(bt, order, (int)c.num, c.bound, c.grid, st);
-}
-
-#define NPPB_CUDA(call, what)                            \
-  do {                                                   \
-    cudaError_t e_ = (call);                             \
-    if (e_ != cudaSuccess) return cuda_status(e_, what); \
-  } while (0)
-
-int arg_error(const std::string& m) {
-  set_error(m);
-  return NPPB_E_ARG;
-}
-
-int build(nppb_plan& pl, int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
-          const int64_t* b_off, const int64_t* inv_off, int flags) {
-  if (count < 0 || count > INT32_MAX) return arg_error("bad system count");
-  if (flags & ~(NPPB_WANT_LU | NPPB_WANT_SOLVE | NPPB_WANT_DET | NPPB_WANT_SLOGDET | NPPB_WANT_INV))
+int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
+                const int64_t* b_off, const int64_t* inv_off, int fl, bool solve_only_, bool own_lu) {
+  if (cnt < 0 || cnt > INT32_MAX) return arg_error("bad system count");
+  if (fl & ~(NPPB_WANT_LU | NPPB_WANT_SOLVE | NPPB_WANT_DET | NPPB_WANT_SLOGDET | NPPB_WANT_INV))
     return arg_error("unknown flag bits");
-  if (count && (!n || !a_off)) return arg_error("n and a_off are required");
-  const bool solve = flags & NPPB_WANT_SOLVE, inv = flags & NPPB_WANT_INV;
-  if (solve && count && (!nrhs || !b_off)) return arg_error("solve needs nrhs and b_off");
-  if (inv && count && !inv_off) return arg_error("inverse needs inv_off");
+  if (cnt && (!n || !a_off)) return arg_error("n and a_off are required");
+  const bool solve = fl & NPPB_WANT_SOLVE, want_inv = fl & NPPB_WANT_INV;
+  if (solve && cnt && (!nrhs || !b_off)) return arg_error("solve needs nrhs and b_off");
+  if (want_inv && cnt && !inv_off) return arg_error("inverse needs inv_off");
   const Device* d = device();
   if (!d) return NPPB_E_NODEV;
-  pl.dev = d->id;
-  pl.count = count;
-  pl.flags = flags;
-  if (const char* e = std::getenv("NPPB_NO_GRAPH")) pl.use_graph = !(e[0] == '1');
+  dev = d->id;
+  count = cnt;
+  flags = fl;
+  solve_only = solve_only_;
+  if (const char* e = std::getenv("NPPB_NO_GRAPH")) use_graph = !(e[0] == '1');
 
-  std::vector<SysDesc> desc(count);
-  // class index: 0..2 warp (8/16/32), 3..6 CTA (64/128/256/512)
-  static constexpr int kBounds[7] = {8, 16, 32, 64, 128, 256, 512};
-  std::vector<std::vector<int32_t>> members(7);
+  std::vector<SysDesc> desc(cnt);
+  static constexpr int kWarpBounds[3] = {8, 16, 32};
+  std::vector<std::vector<int32_t>> warp_members(3);
+  std::vector<int32_t> step_members;
   int64_t lu = 0, piv = 0;
-  for (int64_t i = 0; i < count; ++i) {
+  for (int64_t i = 0; i < cnt; ++i) {
     const int ni = n[i];
     const int ki = solve ? nrhs[i] : 0;
-    if (ni < 0 || ni > kCtaMaxN) {
+    if (ni < 0 || ni > kStepMaxN) {
       set_error("system " + std::to_string(i) + ": order " + std::to_string(ni) + " outside [0, " +
-                std::to_string(kCtaMaxN) + "]");
+                std::to_string(kStepMaxN) + "]");
       return ni < 0 ? NPPB_E_ARG : NPPB_E_RANGE;
     }
     if (ki < 0) return arg_error("negative nrhs");
@@ -151,141 +116,341 @@ int build(nppb_plan& pl, int64_t count, const int32_t* n, const int32_t* nrhs, c
     s.n = ni;
     s.nrhs = ki;
     s.idx = (int32_t)i;
-    s.pad_ = 0;
+    s.pad_ = -1;
     s.a_off = a_off[i];
-    s.lu_off = lu;
+    s.lu_off = own_lu ? lu : a_off[i];
     s.b_off = solve ? b_off[i] : 0;
-    s.inv_off = (inv && inv_off[i] >= 0) ? inv_off[i] : -1;
+    s.inv_off = (want_inv && inv_off[i] >= 0) ? inv_off[i] : -1;
     s.piv_off = piv;
     lu += (int64_t)ni * ni;
     piv += ni;
-    pl.a_elems = std::max(pl.a_elems, a_off[i] + (int64_t)ni * ni);
-    if (solve) pl.b_elems = std::max(pl.b_elems, b_off[i] + (int64_t)ni * ki);
-    if (s.inv_off >= 0) pl.inv_elems = std::max(pl.inv_elems, s.inv_off + (int64_t)ni * ni);
-    int c = 0;
-    while (ni > kBounds[c]) ++c;
-    members[c].push_back((int32_t)i);
+    a_elems = std::max(a_elems, a_off[i] + (int64_t)ni * ni);
+    if (solve) b_elems = std::max(b_elems, b_off[i] + (int64_t)ni * ki);
+    if (s.inv_off >= 0) inv_elems = std::max(inv_elems, s.inv_off + (int64_t)ni * ni);
+    if (ni <= 32) {
+      int c = 0;
+      while (ni > kWarpBounds[c]) ++c;
+      warp_members[c].push_back((int32_t)i);
+    } else {
+      step_members.push_back((int32_t)i);
+    }
   }
-  pl.lu_elems = lu;
-  pl.piv_elems = piv;
+  lu_elems = own_lu ? lu : 0;
+  piv_elems = piv;
+
+  // warp classes: longest first
   std::vector<int32_t> order;
-  order.reserve(count);
-  for (int c = 0; c < 7; ++c) {
-    auto& m = members[c];
-    if (m.empty()) continue;
-    std::stable_sort(m.begin(), m.end(), [&](int32_t x, int32_t y) {
+  order.reserve(cnt);
+  for (int c = 0; c < 3; ++c) {
+    auto& mb = warp_members[c];
+    if (mb.empty()) continue;
+    std::stable_sort(mb.begin(), mb.end(), [&](int32_t x, int32_t y) {
       if (desc[x].n != desc[y].n) return desc[x].n > desc[y].n;
       return desc[x].nrhs > desc[y].nrhs;
     });
-    nppb_plan::Class cl;
-    cl.flops = 0.0;
-    cl.bytes = 0.0;
-    for (int32_t i : m) {
-      const double nd = desc[i].n, kd = desc[i].nrhs;
-      cl.flops += 2.0 / 3.0 * nd * nd * nd - 0.5 * nd * nd + 5.0 / 6.0 * nd;  // getrf
-      cl.bytes += 8.0 * nd * nd + 4.0 * 5;                                       // A, per-system outputs
-      if (solve) {
-        cl.flops += 2.0 * nd * nd * kd - nd * kd;                                // getrs
-        cl.bytes += 16.0 * nd * kd;                                              // B in, X out
-      }
-      if (desc[i].inv_off >= 0) {
-        cl.flops += 4.0 / 3.0 * nd * nd * nd;                                    // getri-equivalent
-        cl.bytes += 8.0 * nd * nd;
+    WarpClass wc;
+    wc.bound = kWarpBounds[c];
+    wc.first = (int64_t)order.size();
+    wc.num = (int64_t)mb.size();
+    wc.flops = wc.bytes = 0.0;
+    for (int32_t i : mb) add_cost(desc[i], wc.flops, wc.bytes);
+    warp_classes.push_back(wc);
+    order.insert(order.end(), mb.begin(), mb.end());
+  }
+
+  // step-wise set: descending order, slot = rank
+  std::stable_sort(step_members.begin(), step_members.end(),
+                   [&](int32_t x, int32_t y) { return desc[x].n > desc[y].n; });
+  for (size_t r = 0; r < step_members.size(); ++r) desc[step_members[r]].pad_ = (int32_t)r;
+  nstep_sys = (int64_t)step_members.size();
+  std::vector<StepItem> items, back;
+  step_flops = step_bytes = 0.0;
+  for (int32_t i : step_members) add_cost(desc[i], step_flops, step_bytes);
+  if (nstep_sys) {
+    const int nbig = desc[step_members[0]].n;
+    if (!solve_only) {
+      for (int k0 = 0; k0 < nbig; k0 += kStepNB) {
+        Step st;
+        st.k0 = k0;
+        int64_t act = 0;
+        while (act < nstep_sys && desc[step_members[act]].n > k0) ++act;
+        // panel launches: contiguous runs with the same panel-height class
+        int64_t b = 0;
+        while (b < act) {
+          const int pc = panel_class(desc[step_members[b]].n - k0);
+          int64_t e = b;
+          while (e < act && panel_class(desc[step_members[e]].n - k0) == pc) ++e;
+          st.panels.push_back({b, e - b, desc[step_members[b]].n - k0});
+          b = e;
+        }
+        st.item_first = (int64_t)items.size();
+        st.nmax = nbig;
+        for (int64_t r = 0; r < act; ++r) {
+          const SysDesc& s = desc[step_members[r]];
+          const int32_t si = step_members[r];
+          add_strips(items, si, kSegMatrix, k0 + kStepNB, s.n);
+          if (solve && s.nrhs) add_strips(items, si, kSegRhs, 0, s.nrhs);
+          if (s.inv_off >= 0) add_strips(items, si, kSegInv, 0, s.n);
+          if ((fl & NPPB_WANT_LU) && k0 > 0) add_strips(items, si, kSegLeft, 0, k0);
+        }
+        st.item_count = (int64_t)items.size() - st.item_first;
+        steps.push_back(st);
       }
     }
-    cl.warp = c < 3;
-    cl.bound = kBounds[c];
-    cl.first = (int64_t)order.size();
-    cl.num = (int64_t)m.size();
-    cl.grid = cl.warp ? 0 : lu_cta_grid((int)cl.num, cl.bound, d->sms);
-    pl.classes.push_back(cl);
-    order.insert(order.end(), m.begin(), m.end());
+    for (int32_t si : step_members) {
+      const SysDesc& s = desc[si];
+      if (solve && s.nrhs) add_strips(back, si, kSegRhs, 0, s.nrhs);
+      if (s.inv_off >= 0 && !solve_only) add_strips(back, si, kSegInv, 0, s.n);
+    }
+    step_nmax = nbig;
   }
-  if (count) {
-    NPPB_CUDA(cudaMalloc(&pl.d_desc, sizeof(SysDesc) * count), "plan descriptors");
-    NPPB_CUDA(cudaMalloc(&pl.d_order, sizeof(int32_t) * count), "plan order");
-    NPPB_CUDA(cudaMemcpy(pl.d_desc, desc.data(), sizeof(SysDesc) * count, cudaMemcpyHostToDevice),
-              "plan upload");
-    NPPB_CUDA(cudaMemcpy(pl.d_order, order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice),
-              "plan upload");
-  }
-  if (lu) NPPB_CUDA(cudaMalloc(&pl.d_lu, sizeof(double) * lu), "plan LU workspace");
-  if (piv) NPPB_CUDA(cudaMalloc(&pl.d_piv, sizeof(int32_t) * piv), "plan pivot workspace");
+  nback = (int64_t)back.size();
+
+  int rc = upload(&d_desc, desc);
+  if (rc == NPPB_OK) rc = upload(&d_order, order);
+  if (rc == NPPB_OK) rc = upload(&d_step_list, step_members);
+  if (rc == NPPB_OK) rc = upload(&d_items, items);
+  if (rc == NPPB_OK) rc = upload(&d_back, back);
+  if (rc != NPPB_OK) return rc;
+  if (nstep_sys) NPPB_CUDA(cudaMalloc(&d_scratch, sizeof(StepScratch) * nstep_sys), "plan scratch");
+  if (lu_elems) NPPB_CUDA(cudaMalloc(&d_lu, sizeof(double) * lu_elems), "plan LU workspace");
+  if (piv) NPPB_CUDA(cudaMalloc(&d_piv, sizeof(int32_t) * piv), "plan pivot workspace");
   return NPPB_OK;
 }
 
-int execute(nppb_plan& pl, const void* const* ptrs, cudaStream_t st) {
-  if (pl.classes.empty()) return NPPB_OK;
-  if (pl.a_elems && !ptrs[0]) return arg_error("A is null");
-  if ((pl.flags & NPPB_WANT_SOLVE) && pl.b_elems && (!ptrs[1] || !ptrs[2]))
-    return arg_error("solve needs B and X");
-  if ((pl.flags & NPPB_WANT_INV) && pl.inv_elems && !ptrs[3]) return arg_error("inverse needs Inv");
-  if ((pl.flags & NPPB_WANT_DET) && !ptrs[4]) return arg_error("det needs Det");
-  if ((pl.flags & NPPB_WANT_SLOGDET) && (!ptrs[5] || !ptrs[6])) return arg_error("slogdet needs Sign, Logabs");
+void Plan::add_cost(const SysDesc& s, double& fl, double& by) const {
+  const double nd = s.n, kd = s.nrhs;
+  if (!solve_only) {
+    fl += 2.0 / 3.0 * nd * nd * nd - 0.5 * nd * nd + 5.0 / 6.0 * nd;  // getrf
+    by += 8.0 * nd * nd + 20.0;                                        // A, per-system outputs
+  } else {
+    by += 8.0 * nd * nd;                                               // reads L and U
+  }
+  if (flags & NPPB_WANT_SOLVE) {
+    fl += 2.0 * nd * nd * kd - nd * kd;                                // getrs
+    by += 16.0 * nd * kd;
+  }
+  if (s.inv_off >= 0) {
+    fl += 4.0 / 3.0 * nd * nd * nd;                                    // getri-equivalent
+    by += 8.0 * nd * nd;
+  }
+}
+
+Batch Plan::warp_batch(const Ptrs& p) const {
+  Batch bt{};
+  bt.A = p.A ? p.A : p.LU;
+  bt.B = p.B;
+  bt.X = p.X;
+  bt.inv = (flags & NPPB_WANT_INV) ? p.Inv : nullptr;
+  bt.det = p.Det;
+  bt.sign = p.Sign;
+  bt.logabs = p.Logabs;
+  bt.info = p.info;
+  bt.LU = p.LU;
+  bt.ipiv = p.ipiv;
+  bt.desc = d_desc;
+  bt.flags = flags | (solve_only ? (kSolveOnly | kWantSolve) : 0) | (p.A ? 0 : kInPlace);
+  return bt;
+}
+
+StepArgs Plan::step_args(const Ptrs& p) const {
+  StepArgs sa{};
+  sa.desc = d_desc;
+  sa.scratch = d_scratch;
+  sa.A = p.A;
+  sa.LU = p.LU;
+  sa.ipiv = p.ipiv;
+  sa.B = p.B;
+  sa.X = p.X;
+  sa.inv = (flags & NPPB_WANT_INV) ? p.Inv : nullptr;
+  sa.det = p.Det;
+  sa.sign = p.Sign;
+  sa.logabs = p.Logabs;
+  sa.info = p.info;
+  sa.solve_only = solve_only ? 1 : 0;
+  return sa;
+}
+
+cudaError_t Plan::launch_warp(const Ptrs& p, int cls, cudaStream_t st) const {
+  const WarpClass& c = warp_classes[cls];
+  return launch_lu_warp(warp_batch(p), d_order + c.first, (int)c.num, c.bound, st);
+}
+
+cudaError_t Plan::launch_steps(const Ptrs& p, cudaStream_t st) const {
+  if (!nstep_sys) return cudaSuccess;
+  const StepArgs sa = step_args(p);
+  if (solve_only) {
+    cudaError_t e = launch_forward(sa, d_back, (int)nback, step_nmax, st);
+    if (e != cudaSuccess) return e;
+    return launch_back(sa, d_back, (int)nback, st);
+  }
+  for (const Step& s : steps) {
+    for (const auto& pr : s.panels) {
+      cudaError_t e = launch_panel(sa, d_step_list + pr.first, (int)pr.num, pr.mmax, s.k0, st);
+      if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st);
+    if (e != cudaSuccess) return e;
+  }
+  return launch_back(sa, d_back, (int)nback, st);
+}
+
+int Plan::execute(const Ptrs& p, cudaStream_t st) {
+  if (count == 0) return NPPB_OK;
+  if (a_elems && !p.A && !p.LU) return arg_error("A is null");
+  if ((flags & NPPB_WANT_SOLVE) && b_elems && (!p.B || !p.X)) return arg_error("solve needs B and X");
+  if ((flags & NPPB_WANT_INV) && inv_elems && !p.Inv) return arg_error("inverse needs Inv");
+  if ((flags & NPPB_WANT_DET) && !p.Det) return arg_error("det needs Det");
+  if ((flags & NPPB_WANT_SLOGDET) && (!p.Sign || !p.Logabs)) return arg_error("slogdet needs Sign, Logabs");
+  if ((lu_elems || !p.A) && !p.LU) return arg_error("plan workspace missing");
+  if (piv_elems && !p.ipiv) return arg_error("plan pivot workspace missing");
   int cur = -1;
   cudaGetDevice(&cur);
-  if (cur != pl.dev) return arg_error("plan used on a different device than it was created on");
-  const Batch bt = plan_batch(pl, ptrs);
-  std::lock_guard<std::mutex> lk(pl.mu);
-  if (!pl.use_graph) {
-    for (const auto& c : pl.classes) NPPB_CUDA(launch_class(pl, c, bt, st), "class launch");
+  if (cur != dev) return arg_error("plan used on a different device than it was created on");
+  std::lock_guard<std::mutex> lk(mu);
+  const int branches = num_kernel_groups();
+  // executions share the plan's workspace: each one starts after the previous
+  if (!done) NPPB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "event");
+  else NPPB_CUDA(cudaStreamWaitEvent(st, done, 0), "stream wait");
+  if (!use_graph) {
+    for (size_t c = 0; c < warp_classes.size(); ++c) NPPB_CUDA(launch_warp(p, (int)c, st), "warp class launch");
+    NPPB_CUDA(launch_steps(p, st), "step launch");
+    NPPB_CUDA(cudaEventRecord(done, st), "event record");
     return NPPB_OK;
   }
-  std::array<const void*, 8> key;
-  std::copy(ptrs, ptrs + 8, key.begin());
-  if (!pl.exec || key != pl.key) {
-    if (!pl.cap) {
-      NPPB_CUDA(cudaStreamCreateWithFlags(&pl.cap, cudaStreamNonBlocking), "stream");
-      NPPB_CUDA(cudaEventCreateWithFlags(&pl.fork, cudaEventDisableTiming), "event");
-      for (size_t i = 0; i < pl.classes.size(); ++i) {
+  if (!exec || std::memcmp(&p, &key, sizeof(Ptrs)) != 0) {
+    if (!cap) {
+      NPPB_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking), "stream");
+      NPPB_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "event");
+      for (int i = 0; i < branches; ++i) {
         cudaStream_t s;
         cudaEvent_t e;
         NPPB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
         NPPB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-        pl.side.push_back(s);
-        pl.join.push_back(e);
+        side.push_back(s);
+        join.push_back(e);
       }
     }
-    if (pl.exec) { cudaGraphExecDestroy(pl.exec); pl.exec = nullptr; }
-    if (pl.graph) { cudaGraphDestroy(pl.graph); pl.graph = nullptr; }
-    NPPB_CUDA(cudaStreamBeginCapture(pl.cap, cudaStreamCaptureModeThreadLocal), "begin capture");
-    cudaError_t err = cudaEventRecord(pl.fork, pl.cap);
-    for (size_t i = 0; i < pl.classes.size() && err == cudaSuccess; ++i) {
-      err = cudaStreamWaitEvent(pl.side[i], pl.fork, 0);
-      if (err == cudaSuccess) err = launch_class(pl, pl.classes[i], bt, pl.side[i]);
-      if (err == cudaSuccess) err = cudaEventRecord(pl.join[i], pl.side[i]);
-      if (err == cudaSuccess) err = cudaStreamWaitEvent(pl.cap, pl.join[i], 0);
+    if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+    if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    NPPB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t err = cudaEventRecord(fork, cap);
+    // the step chain is the long pole: start it first
+    for (int b = 0; b < branches && err == cudaSuccess; ++b) {
+      const int i = (b + branches - 1) % branches;
+      err = cudaStreamWaitEvent(side[i], fork, 0);
+      if (err == cudaSuccess)
+        err = (i < (int)warp_classes.size()) ? launch_warp(p, i, side[i]) : launch_steps(p, side[i]);
+      if (err == cudaSuccess) err = cudaEventRecord(join[i], side[i]);
+      if (err == cudaSuccess) err = cudaStreamWaitEvent(cap, join[i], 0);
     }
     cudaGraph_t g = nullptr;
-    const cudaError_t end = cudaStreamEndCapture(pl.cap, &g);
+    const cudaError_t end = cudaStreamEndCapture(cap, &g);
     if (err == cudaSuccess) err = end;
     if (err != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
       return cuda_status(err, "graph capture");
     }
-    pl.graph = g;
-    NPPB_CUDA(cudaGraphInstantiate(&pl.exec, pl.graph, 0), "graph instantiate");
-    pl.key = key;
+    graph = g;
+    NPPB_CUDA(cudaGraphInstantiate(&exec, graph, 0), "graph instantiate");
+    key = p;
   }
-  NPPB_CUDA(cudaGraphLaunch(pl.exec, st), "graph launch");
+  NPPB_CUDA(cudaGraphLaunch(exec, st), "graph launch");
+  NPPB_CUDA(cudaEventRecord(done, st), "event record");
   return NPPB_OK;
 }
+
+int Plan::num_kernel_groups() const { return (int)warp_classes.size() + (nstep_sys ? 1 : 0); }
+
+int Plan::launches_per_execute() const {
+  int l = (int)warp_classes.size();
+  if (nstep_sys) {
+    if (solve_only) return l + 2;
+    for (const Step& s : steps) l += (int)s.panels.size() + 1;
+    l += 1;
+  }
+  return l;
+}
+
+std::shared_ptr<Plan> uniform_plan(int64_t count, int32_t n, int32_t nrhs, int flags, bool solve_only,
+                                   bool own_lu, int* rc) {
+  using Key = std::tuple<int, int64_t, int32_t, int32_t, int, bool, bool>;
+  static std::mutex mu;
+  static std::list<std::pair<Key, std::shared_ptr<Plan>>> cache;
+  int dev = -1;
+  cudaGetDevice(&dev);
+  const Key k{dev, count, n, nrhs, flags, solve_only, own_lu};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto it = cache.begin(); it != cache.end(); ++it) {
+      if (it->first == k) {
+        cache.splice(cache.begin(), cache, it);
+        *rc = NPPB_OK;
+        return cache.front().second;
+      }
+    }
+  }
+  std::vector<int32_t> nv(count, n), kv(count, nrhs);
+  std::vector<int64_t> ao(count), bo(count), io(count);
+  for (int64_t i = 0; i < count; ++i) {
+    ao[i] = i * (int64_t)n * n;
+    bo[i] = i * (int64_t)n * nrhs;
+    io[i] = i * (int64_t)n * n;
+  }
+  auto p = std::make_shared<Plan>();
+  p->use_graph = false;  // pointers change from call to call
+  *rc = p->build(count, nv.data(), kv.data(), ao.data(), bo.data(), io.data(), flags, solve_only, own_lu);
+  if (*rc != NPPB_OK) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  cache.emplace_front(k, p);
+  if (cache.size() > 8) cache.pop_back();
+  return p;
+}
+
+}  // namespace nppb
+
+// ---------------------------------------------------------------------------
+// C ABI
+using nppb::Plan;
+
+struct nppb_plan {
+  Plan p;
+};
+
+namespace {
 
 template <class F>
 int guarded(F&& f) {
   try {
-    clear_error();
+    nppb::clear_error();
     return f();
   } catch (const std::bad_alloc&) {
-    set_error("host allocation failed");
+    nppb::set_error("host allocation failed");
     return NPPB_E_NOMEM;
   }
 }
 
 int ensure(void** p, size_t bytes) {
   if (*p || bytes == 0) return NPPB_OK;
-  NPPB_CUDA(cudaMalloc(p, bytes), "plan staging");
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return nppb::cuda_status(e, "plan staging");
   return NPPB_OK;
+}
+
+Plan::Ptrs dev_ptrs(const Plan& pl, const double* dA, const double* dB, double* dX, double* dInv,
+                    double* dDet, double* dSign, double* dLogabs, int32_t* dinfo) {
+  Plan::Ptrs p{};
+  p.A = dA;
+  p.B = dB;
+  p.X = dX;
+  p.Inv = dInv;
+  p.Det = dDet;
+  p.Sign = dSign;
+  p.Logabs = dLogabs;
+  p.info = dinfo;
+  p.LU = pl.d_lu;
+  p.ipiv = pl.d_piv;
+  return p;
 }
 
 }  // namespace
@@ -295,10 +460,13 @@ extern "C" {
 int nppb_plan_create(nppb_plan** plan, int64_t count, const int32_t* n, const int32_t* nrhs,
                      const int64_t* a_off, const int64_t* b_off, const int64_t* inv_off, int flags) {
   return guarded([&]() -> int {
-    if (!plan) return arg_error("plan is null");
+    if (!plan) {
+      nppb::set_error("plan is null");
+      return NPPB_E_ARG;
+    }
     *plan = nullptr;
     auto* pl = new nppb_plan();
-    const int rc = build(*pl, count, n, nrhs, a_off, b_off, inv_off, flags);
+    const int rc = pl->p.build(count, n, nrhs, a_off, b_off, inv_off, flags & ~NPPB_WANT_LU, false, true);
     if (rc != NPPB_OK) {
       delete pl;
       return rc;
@@ -309,27 +477,40 @@ int nppb_plan_create(nppb_plan** plan, int64_t count, const int32_t* n, const in
 }
 
 int nppb_plan_sizes(const nppb_plan* plan, int64_t* a_elems, int64_t* b_elems, int64_t* inv_elems) {
-  if (!plan) return arg_error("plan is null");
-  if (a_elems) *a_elems = plan->a_elems;
-  if (b_elems) *b_elems = plan->b_elems;
-  if (inv_elems) *inv_elems = plan->inv_elems;
+  if (!plan) {
+    nppb::set_error("plan is null");
+    return NPPB_E_ARG;
+  }
+  if (a_elems) *a_elems = plan->p.a_elems;
+  if (b_elems) *b_elems = plan->p.b_elems;
+  if (inv_elems) *inv_elems = plan->p.inv_elems;
   return NPPB_OK;
 }
 
 int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,
                       double* dDet, double* dSign, double* dLogabs, int32_t* dinfo, void* stream) {
   return guarded([&]() -> int {
-    if (!plan) return arg_error("plan is null");
-    const void* ptrs[8] = {dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo};
-    return execute(*plan, ptrs, static_cast<cudaStream_t>(stream));
+    if (!plan) {
+      nppb::set_error("plan is null");
+      return NPPB_E_ARG;
+    }
+    if (plan->p.a_elems && !dA) {
+      nppb::set_error("A is null");
+      return NPPB_E_ARG;
+    }
+    return plan->p.execute(dev_ptrs(plan->p, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo),
+                           static_cast<cudaStream_t>(stream));
   });
 }
 
 int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X, double* Inv,
                            double* Det, double* Sign, double* Logabs, int32_t* info) {
   return guarded([&]() -> int {
-    if (!plan) return arg_error("plan is null");
-    nppb_plan& pl = *plan;
+    if (!plan) {
+      nppb::set_error("plan is null");
+      return NPPB_E_ARG;
+    }
+    Plan& pl = plan->p;
     const int f = pl.flags;
     const size_t c = (size_t)pl.count;
     int rc = ensure((void**)&pl.hA, sizeof(double) * pl.a_elems);
@@ -341,21 +522,24 @@ int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, do
     if (rc == NPPB_OK && (f & NPPB_WANT_SLOGDET)) rc = ensure((void**)&pl.hLog, sizeof(double) * c);
     if (rc == NPPB_OK) rc = ensure((void**)&pl.hInfo, sizeof(int32_t) * c);
     if (rc != NPPB_OK) return rc;
-    cudaStream_t st = thread_stream();
+    if (pl.a_elems && !A) {
+      nppb::set_error("A is null");
+      return NPPB_E_ARG;
+    }
+    if ((f & NPPB_WANT_SOLVE) && pl.b_elems && (!B || !X)) {
+      nppb::set_error("solve needs B and X");
+      return NPPB_E_ARG;
+    }
+    cudaStream_t st = nppb::thread_stream();
     auto h2d = [&](void* d, const void* h, size_t bytes) {
       return bytes ? cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, st) : cudaSuccess;
     };
     auto d2h = [&](void* h, const void* d, size_t bytes) {
       return (bytes && h) ? cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, st) : cudaSuccess;
     };
-    if (pl.a_elems && !A) return arg_error("A is null");
     NPPB_CUDA(h2d(pl.hA, A, sizeof(double) * pl.a_elems), "host to device copy");
-    if (f & NPPB_WANT_SOLVE) {
-      if (pl.b_elems && (!B || !X)) return arg_error("solve needs B and X");
-      NPPB_CUDA(h2d(pl.hB, B, sizeof(double) * pl.b_elems), "host to device copy");
-    }
-    const void* ptrs[8] = {pl.hA, pl.hB, pl.hX, pl.hInv, pl.hDet, pl.hSign, pl.hLog, pl.hInfo};
-    rc = execute(pl, ptrs, st);
+    if (f & NPPB_WANT_SOLVE) NPPB_CUDA(h2d(pl.hB, B, sizeof(double) * pl.b_elems), "host to device copy");
+    rc = pl.execute(dev_ptrs(pl, pl.hA, pl.hB, pl.hX, pl.hInv, pl.hDet, pl.hSign, pl.hLog, pl.hInfo), st);
     if (rc != NPPB_OK) return rc;
     if (f & NPPB_WANT_SOLVE) NPPB_CUDA(d2h(X, pl.hX, sizeof(double) * pl.b_elems), "device to host copy");
     if (f & NPPB_WANT_INV) NPPB_CUDA(d2h(Inv, pl.hInv, sizeof(double) * pl.inv_elems), "device to host copy");
@@ -370,53 +554,68 @@ int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, do
   });
 }
 
-int nppb_plan_num_classes(const nppb_plan* plan) {
-  return plan ? (int)plan->classes.size() : 0;
+int nppb_plan_destroy(nppb_plan* plan) {
+  delete plan;
+  return NPPB_OK;
 }
+
+int nppb_plan_num_classes(const nppb_plan* plan) { return plan ? plan->p.num_kernel_groups() : 0; }
 
 int nppb_plan_class_info(const nppb_plan* plan, int c, int* is_warp, int* bound, int64_t* systems,
                          double* flops, double* bytes) {
-  if (!plan || c < 0 || c >= (int)plan->classes.size()) return arg_error("bad plan or class index");
-  const auto& cl = plan->classes[c];
-  if (is_warp) *is_warp = cl.warp ? 1 : 0;
-  if (bound) *bound = cl.bound;
-  if (systems) *systems = cl.num;
-  if (flops) *flops = cl.flops;
-  if (bytes) *bytes = cl.bytes;
+  if (!plan || c < 0 || c >= plan->p.num_kernel_groups()) {
+    nppb::set_error("bad plan or class index");
+    return NPPB_E_ARG;
+  }
+  const Plan& pl = plan->p;
+  if (c < (int)pl.warp_classes.size()) {
+    const auto& w = pl.warp_classes[c];
+    if (is_warp) *is_warp = 1;
+    if (bound) *bound = w.bound;
+    if (systems) *systems = w.num;
+    if (flops) *flops = w.flops;
+    if (bytes) *bytes = w.bytes;
+  } else {
+    if (is_warp) *is_warp = 0;
+    if (bound) *bound = pl.step_nmax;
+    if (systems) *systems = pl.nstep_sys;
+    if (flops) *flops = pl.step_flops;
+    if (bytes) *bytes = pl.step_bytes;
+  }
   return NPPB_OK;
 }
 
 int nppb_plan_time_classes(nppb_plan* plan, const double* dA, const double* dB, double* dX,
-                           double* dInv, double* dDet, double* dSign, double* dLogabs,
-                           int32_t* dinfo, void* stream, int reps, float* ms_out) {
+                           double* dInv, double* dDet, double* dSign, double* dLogabs, int32_t* dinfo,
+                           void* stream, int reps, float* ms_out) {
   return guarded([&]() -> int {
-    if (!plan || reps < 1 || !ms_out) return arg_error("bad plan, reps or ms_out");
-    const void* ptrs[8] = {dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo};
-    const Batch bt = plan_batch(*plan, ptrs);
+    if (!plan || reps < 1 || !ms_out) {
+      nppb::set_error("bad plan, reps or ms_out");
+      return NPPB_E_ARG;
+    }
+    Plan& pl = plan->p;
+    const Plan::Ptrs p = dev_ptrs(pl, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaEvent_t e0, e1;
     NPPB_CUDA(cudaEventCreate(&e0), "event");
     NPPB_CUDA(cudaEventCreate(&e1), "event");
     int rc = NPPB_OK;
-    for (size_t c = 0; c < plan->classes.size() && rc == NPPB_OK; ++c) {
+    const int groups = pl.num_kernel_groups();
+    for (int c = 0; c < groups && rc == NPPB_OK; ++c) {
       cudaError_t e = cudaEventRecord(e0, st);
-      for (int r = 0; r < reps && e == cudaSuccess; ++r) e = launch_class(*plan, plan->classes[c], bt, st);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r)
+        e = (c < (int)pl.warp_classes.size()) ? pl.launch_warp(p, c, st) : pl.launch_steps(p, st);
       if (e == cudaSuccess) e = cudaEventRecord(e1, st);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
       float ms = 0.f;
       if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-      if (e != cudaSuccess) rc = cuda_status(e, "class timing");
+      if (e != cudaSuccess) rc = nppb::cuda_status(e, "class timing");
       ms_out[c] = ms / reps;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;
   });
-}
-
-int nppb_plan_destroy(nppb_plan* plan) {
-  delete plan;
-  return NPPB_OK;
 }
 
 int nppb_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
@@ -426,7 +625,7 @@ int nppb_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, con
   nppb_plan* pl = nullptr;
   int rc = nppb_plan_create(&pl, count, n, nrhs, a_off, b_off, inv_off, flags);
   if (rc != NPPB_OK) return rc;
-  pl->use_graph = false;  // a one-shot call gains nothing from capture
+  pl->p.use_graph = false;  // a one-shot call gains nothing from capture
   rc = nppb_plan_execute_host(pl, A, B, X, Inv, Det, Sign, Logabs, info);
   nppb_plan_destroy(pl);
   return rc;

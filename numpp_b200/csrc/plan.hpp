@@ -1,0 +1,110 @@
+// Batched execution plan (host side). C++20.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "nppb_internal.hpp"
+#include "nppb_step.hpp"
+#include "runtime.hpp"
+
+namespace nppb {
+
+class Plan {
+ public:
+  // Device pointers of one execution (A may be null: factor LU in place).
+  struct Ptrs {
+    const double* A;
+    const double* B;
+    double* X;
+    double* Inv;
+    double* Det;
+    double* Sign;
+    double* Logabs;
+    int32_t* info;
+    double* LU;
+    int32_t* ipiv;
+  };
+  struct WarpClass {
+    int bound;
+    int64_t first, num;
+    double flops, bytes;
+  };
+  struct PanelRange {
+    int64_t first, num;
+    int mmax;
+  };
+  struct Step {
+    int k0 = 0;
+    std::vector<PanelRange> panels;
+    int64_t item_first = 0, item_count = 0;
+    int nmax = 0;
+  };
+
+  Plan() = default;
+  Plan(const Plan&) = delete;
+  Plan& operator=(const Plan&) = delete;
+  ~Plan();
+
+  // own_lu: allocate an LU workspace (else the factors go where A is: in place).
+  // solve_only: getrs from factors already in LU / ipiv.
+  int build(int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
+            const int64_t* b_off, const int64_t* inv_off, int flags, bool solve_only, bool own_lu);
+  int execute(const Ptrs& p, cudaStream_t st);
+  cudaError_t launch_warp(const Ptrs& p, int cls, cudaStream_t st) const;
+  cudaError_t launch_steps(const Ptrs& p, cudaStream_t st) const;
+  int num_kernel_groups() const;
+  int launches_per_execute() const;
+
+  int dev = -1;
+  int64_t count = 0;
+  int flags = 0;
+  bool solve_only = false;
+  bool use_graph = true;
+  int64_t a_elems = 0, b_elems = 0, inv_elems = 0, lu_elems = 0, piv_elems = 0;
+  std::vector<WarpClass> warp_classes;
+  std::vector<Step> steps;
+  int64_t nstep_sys = 0, nback = 0;
+  int step_nmax = 0;
+  double step_flops = 0.0, step_bytes = 0.0;
+
+  SysDesc* d_desc = nullptr;
+  int32_t* d_order = nullptr;
+  int32_t* d_step_list = nullptr;
+  StepItem* d_items = nullptr;
+  StepItem* d_back = nullptr;
+  StepScratch* d_scratch = nullptr;
+  double* d_lu = nullptr;
+  int32_t* d_piv = nullptr;
+
+  // device staging for host-buffer execution, allocated on first use
+  double *hA = nullptr, *hB = nullptr, *hX = nullptr, *hInv = nullptr, *hDet = nullptr,
+         *hSign = nullptr, *hLog = nullptr;
+  int32_t* hInfo = nullptr;
+
+ private:
+  void add_cost(const SysDesc& s, double& fl, double& by) const;
+  Batch warp_batch(const Ptrs& p) const;
+  StepArgs step_args(const Ptrs& p) const;
+
+  std::mutex mu;
+  Ptrs key{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t cap = nullptr;
+  std::vector<cudaStream_t> side;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t done = nullptr;  // end of the last execution: the next one waits for it
+};
+
+// A cached plan for `count` systems of order n (uniform layout), for the
+// uniform-batch entry points.
+std::shared_ptr<Plan> uniform_plan(int64_t count, int32_t n, int32_t nrhs, int flags, bool solve_only,
+                                   bool own_lu, int* rc);
+
+}  // namespace nppb

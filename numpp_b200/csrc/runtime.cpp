@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/numpp_b200.h"
+#include "nppb_step.hpp"
 
 namespace nppb {
 namespace {
@@ -101,20 +102,11 @@ void DevMem::release() {
   p_ = nullptr;
 }
 
-cudaError_t prepare_kernels() { return lu_cta_prepare(); }
+cudaError_t prepare_kernels() { return step_prepare(); }
 
-int lu_cta_grid(int nsys, int nmax, int num_sms) {
-  const int g = lu_cta_blocks_per_sm(nmax) * num_sms;
-  return nsys < g ? nsys : g;
-}
-
-cudaError_t run_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
-  const Device* d = device();
-  if (!d) return cudaErrorNoDevice;
-  const int c = static_cast<int>(count);
-  if (n <= 32) return launch_lu_warp(bt, nullptr, c, n <= 8 ? 8 : (n <= 16 ? 16 : 32), st);
-  if (n <= kCtaMaxN) return launch_lu_cta(bt, nullptr, c, n, lu_cta_grid(c, n, d->sms), st);
-  return cudaErrorInvalidValue;
+cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
+  if (n > 32) return cudaErrorInvalidValue;
+  return launch_lu_warp(bt, nullptr, static_cast<int>(count), n <= 8 ? 8 : (n <= 16 ? 16 : 32), st);
 }
 
 }  // namespace nppb

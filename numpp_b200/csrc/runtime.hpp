@@ -53,12 +53,11 @@ class DevMem {
 cudaError_t launch_fill_f64(double* p, int64_t n, double v, cudaStream_t st);
 cudaError_t launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t st);
 
-// Picks the kernel for a uniform batch of order n and launches it.
-cudaError_t run_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st);
+// Uniform batch of order n <= 32 on the warp-per-system kernel.
+cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st);
 
 // One-time kernel attribute setup (dynamic shared memory opt-in), done before
 // any stream capture.
 cudaError_t prepare_kernels();
-int lu_cta_grid(int nsys, int nmax, int num_sms);
 
 }  // namespace nppb
