@@ -37,6 +37,7 @@ METRIC = "batched solves/s at ≤1e-10 backward err, refined mixed vs FP64 LU; p
 WORKLOAD = ("uneven FP64 batch: 8192 systems, n log-uniform [4,512], nrhs {1,8,32}, A=N(0,1)+nI, "
             "solve+slogdet all, inv 10%")
 SEED = 2025
+KERNEL_NAMES = {"warp_lu": "k_lu_warp", "panel": "k_panel", "update": "k_update", "back": "k_back"}
 
 
 def parse():
@@ -222,7 +223,7 @@ def run_b200(args):
     dInfo = torch.zeros(cnt, dtype=torch.int32, device=dev)
     bufs = (dA, dB, dX, dInv, dDet, dSign, dLog, dInfo)
     stream = torch.cuda.Stream()
-    nclass = len(plan.classes())
+    nlaunch = plan.launches()
 
     def step():
         plan.execute(*bufs, stream=stream)
@@ -267,15 +268,15 @@ def run_b200(args):
         worst = max(worst, float(eta))
     assert not info.any() and worst <= 1e-10, (int(info.astype(bool).sum()), worst)
 
-    # per-class kernel time (CUDA events on the launching stream) -> roofline of the top class
+    # per-kernel time (CUDA events around every launch, on the launching stream)
     cls = plan.classes()
-    cls_ms = plan.time_classes(*bufs, stream=stream, reps=3)
-    top = int(np.argmax(cls_ms))
-    flops_top = cls[top][3]
+    kern = plan.time_kernels(*bufs, stream=stream)
+    top = max(kern, key=lambda k: kern[k][0])
+    top_ms, flops_top = kern[top]
     peak64 = fp64_peak_tflops(torch, dev)
-    achieved = flops_top / (cls_ms[top] * 1e-3) / 1e12
+    achieved = flops_top / (top_ms * 1e-3) / 1e12
     traffic = None
-    tfile = os.path.join(ROOT, "profiles", "lu_cta_uneven8192_traffic.json")
+    tfile = os.path.join(ROOT, "profiles", "k_update_uneven8192_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             traffic = json.load(f).get("bytes_per_launch")
@@ -322,15 +323,17 @@ def run_b200(args):
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "gflops": flops_step * world / (ms_step * 1e-3) / 1e9,
             "max_backward_error_sample": worst,
-            "roofline": {"bound": "tensor", "kernel": f"k_lu_cta (class n<={cls[top][1]})",
+            "roofline": {"bound": "tensor", "kernel": KERNEL_NAMES[top],
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
                          "peak_source": "measured cuBLAS FP64 GEMM 8192^3 on this GPU (burst)",
-                         "traffic": traffic, "launch_ms": cls_ms[top], "flops_per_launch": flops_top},
-            "class_ms": {f"{c[0]}<={c[1]}": round(m, 4) for c, m in zip(cls, cls_ms)},
+                         "traffic": traffic, "ms_per_step": top_ms, "flops_per_step": flops_top,
+                         "note": "summed over the kernel's launches in one step, each timed alone"},
+            "kernels": {KERNEL_NAMES[k]: {"ms": round(v[0], 4), "tflops": v[1] / max(v[0], 1e-9) / 1e9}
+                        for k, v in kern.items()},
             "e2e": {"value": world * cnt / (e2e_step * 1e-3), "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": e2e_step,
                     "path": "nppb_plan_execute_host (C ABI), pinned host buffers"},
-            "gpu_launches": args.steps * nclass,
+            "gpu_launches": args.steps * nlaunch,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "hbm_peak_gbs": measured_peaks().get("hbm_gbs"),

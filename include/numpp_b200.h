@@ -150,6 +150,8 @@ int nppb_plan_destroy(nppb_plan* plan);
  * algorithmic flops / minimum bytes of what it computes (LAPACK counts:
  * getrf 2/3n^3-1/2n^2+5/6n, getrs 2n^2k-nk, inverse +4/3n^3). */
 int nppb_plan_num_classes(const nppb_plan* plan);
+/* Kernel launches one execution makes (graph nodes). */
+int nppb_plan_num_launches(const nppb_plan* plan);
 int nppb_plan_class_info(const nppb_plan* plan, int cls, int* is_warp, int* bound,
                          int64_t* systems, double* flops, double* bytes);
 /* Runs every class alone on `stream`, `reps` launches each between two CUDA
@@ -157,6 +159,14 @@ int nppb_plan_class_info(const nppb_plan* plan, int cls, int* is_warp, int* boun
 int nppb_plan_time_classes(nppb_plan* plan, const double* dA, const double* dB, double* dX,
                            double* dInv, double* dDet, double* dSign, double* dLogabs,
                            int32_t* dinfo, void* stream, int reps, float* ms_out);
+/* Every launch of one execution, one after another on `stream`, each between
+ * two CUDA events: ms_out[k] = summed milliseconds and flops_out[k] = the
+ * arithmetic done, per kernel kind k: 0 warp-per-system LU (orders <= 32),
+ * 1 panel factorisation, 2 strip update (row moves, U12, trailing update on
+ * DMMA), 3 back substitution (and, for getrs plans, forward substitution). */
+int nppb_plan_time_kernels(nppb_plan* plan, const double* dA, const double* dB, double* dX,
+                           double* dInv, double* dDet, double* dSign, double* dLogabs,
+                           int32_t* dinfo, void* stream, double* ms_out, double* flops_out);
 
 /* One-shot uneven batch on host buffers (plan + execute + destroy). */
 int nppb_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,

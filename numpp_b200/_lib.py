@@ -48,9 +48,11 @@ SIGNATURES = {
     "nppb_plan_execute_host": (_int, [_vp] * 9),
     "nppb_plan_destroy": (_int, [_vp]),
     "nppb_plan_num_classes": (_int, [_vp]),
+    "nppb_plan_num_launches": (_int, [_vp]),
     "nppb_plan_class_info": (_int, [_vp, _int, C.POINTER(_int), C.POINTER(_int), C.POINTER(_i64),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_plan_time_classes": (_int, [_vp] * 10 + [_int, C.POINTER(C.c_float)]),
+    "nppb_plan_time_kernels": (_int, [_vp] * 10 + [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_solve_grouped": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _int] + [_vp] * 8),
 }
 

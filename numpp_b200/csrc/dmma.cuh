@@ -24,4 +24,19 @@ __device__ __forceinline__ void warp_argmax(double& v, int& i) {
   }
 }
 
+// Warp-wide argmax for magnitudes (v >= 0; v < 0 marks "no candidate"): the
+// largest v wins, ties go to the smaller key. IEEE bit patterns of non-negative
+// doubles order like the values, so three redux instructions replace the
+// shuffle butterfly. Every lane ends with the same pair.
+__device__ __forceinline__ void warp_argmax_abs(double& v, int& key) {
+  const unsigned long long bits = v > 0.0 ? (unsigned long long)__double_as_longlong(v) : 0ull;
+  const unsigned hi = (unsigned)(bits >> 32), lo = (unsigned)bits;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool top = hi == mhi && lo == mlo;
+  const int k = __reduce_min_sync(0xffffffffu, top ? key : INT_MAX);
+  v = __longlong_as_double((long long)(((unsigned long long)mhi << 32) | mlo));
+  key = k;
+}
+
 }  // namespace nppb

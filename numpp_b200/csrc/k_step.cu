@@ -41,7 +41,7 @@ constexpr int WS = 64 + 1;   // 65: stride of 64-wide shared tiles
 // ---------------------------------------------------------------------------
 // k_panel
 template <int NT, int RPT>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
 k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   constexpr int NW = NT / 32;
   __shared__ double cand_row[2][NW][NB];
@@ -95,7 +95,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
           if (v > best || (v == best && pos[q] < key)) { best = v; key = pos[q]; }
         }
       }
-      warp_argmax(best, key);
+      warp_argmax_abs(best, key);
       const int par = j & 1;
       if (lane == 0) { cand_v[par][warp] = best; cand_k[par][warp] = key; }
 #pragma unroll
@@ -226,6 +226,14 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
 
 // ---------------------------------------------------------------------------
 // Shared helpers for the 64-column strip kernels.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(pred ? 8 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 struct Seg {
   double* dst;         // where the strip lives
   const double* src;   // where it is read from (== dst after step 0)
@@ -316,8 +324,8 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
   extern __shared__ __align__(16) double smem[];
   double* Us = smem;                 // 32 x WS   U12 strip
   double* D = Us + NB * WS;          // 32 x WS   displaced rows
-  double* T = D + NB * WS;           // 32 x WS   A12 (permuted), then reused
-  double* As = T + NB * WS;          // 64 x LS   L21 tile / L11^-1
+  double* T = D + NB * WS;           // 64 x LS   A12 (permuted, 32 x WS), then L21 buffer 1
+  double* As = T + 64 * LS;          // 64 x LS   L11^-1, then L21 buffer 0
   int* tsrc = reinterpret_cast<int*>(As + 64 * LS);
   int* ddst = tsrc + NB;
   int* dsrc = ddst + NB;
@@ -396,22 +404,91 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
   }
   __syncthreads();
   if (kb < NB) return;  // last panel: nothing below it
-  // A22 strip -= L21 U12, 64-row tiles
+  // A22 strip -= L21 U12 in 64-row tiles, software-pipelined: while the tensor
+  // pipe works on tile t, tile t+1's L21 rows stream into shared memory
+  // (cp.async) and its accumulator inputs into registers.
   const double* L = sa.LU + d.lu_off;
-  for (int r0 = k0 + NB; r0 < n; r0 += 64) {
+  const int g = lane >> 2, tq = lane & 3;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+  // L21 buffers: As (L11^-1 is consumed) and T (A12 is consumed once U12 is in Us)
+  auto prefetch_a = [&](int buf, int r0) {
+    double* dstb = buf ? T : As;
+#pragma unroll 4
     for (int idx = tid; idx < 64 * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
-      As[i * LS + q] = (r0 + i < n) ? L[(int64_t)(r0 + i) * n + k0 + q] : 0.0;
+      const bool ok = r0 + i < n;
+      cp_async8(dstb + i * LS + q, ok ? L + (int64_t)(r0 + i) * n + k0 + q : L, ok);
+    }
+    cp_async_commit();
+  };
+  auto load_c = [&](double (&c)[4][4][2], int r0) {
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const int r = r0 + wm + mi * 8 + g;
+      const int dm = r < n ? dmap[r - k0 - kb] : -1;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int cc = wn + ni * 8 + 2 * tq + e;
+          double v = 0.0;
+          if (r < n && cc < w) v = dm >= 0 ? D[dm * WS + cc] : seg_load(s, r, c0 + cc);
+          c[mi][ni][e] = v;
+        }
+      }
+    }
+  };
+  const int r_first = k0 + NB;
+  double cur[4][4][2], nxt[4][4][2];
+  prefetch_a(0, r_first);
+  load_c(cur, r_first);
+  int buf = 0;
+  for (int r0 = r_first; r0 < n; r0 += 64) {
+    const bool more = r0 + 64 < n;
+    if (more) {
+      prefetch_a(buf ^ 1, r0 + 64);
+      load_c(nxt, r0 + 64);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
-    tile_update(
-        As, Us, r0, n, w,
-        [&](int r, int cc) {
-          const int dm = dmap[r - k0 - kb];
-          return dm >= 0 ? D[dm * WS + cc] : seg_load(s, r, c0 + cc);
-        },
-        [&](int r, int cc, double v) { s.dst[(int64_t)r * s.ld + c0 + cc] = v; });
-    __syncthreads();
+    const double* Ab = buf ? T : As;
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) af[mi] = -Ab[(wm + mi * 8 + g) * LS + kk + tq];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Us[(kk + tq) * WS + wn + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma884(cur[mi][ni], af[mi], bf[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi) {
+      const int r = r0 + wm + mi * 8 + g;
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int cc = wn + ni * 8 + 2 * tq + e;
+          if (r < n && cc < w) s.dst[(int64_t)r * s.ld + c0 + cc] = cur[mi][ni][e];
+        }
+      }
+    }
+    if (more) {
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          cur[mi][ni][0] = nxt[mi][ni][0];
+          cur[mi][ni][1] = nxt[mi][ni][1];
+        }
+    }
+    buf ^= 1;
+    __syncthreads();  // buffer `buf` is refilled by the next iteration's prefetch
   }
 }
 
@@ -537,7 +614,7 @@ k_forward(StepArgs sa, const StepItem* __restrict__ items) {
 }
 
 size_t update_smem(int nmax) {
-  return sizeof(double) * (3 * NB * WS + 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
+  return sizeof(double) * (2 * NB * WS + 2 * 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
 }
 size_t forward_smem(int nmax) {
   return sizeof(double) * (NB * LS + NB * WS + 64 * LS) + sizeof(int) * (size_t)nmax;

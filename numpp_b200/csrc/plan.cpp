@@ -154,6 +154,7 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
     wc.num = (int64_t)mb.size();
     wc.flops = wc.bytes = 0.0;
     for (int32_t i : mb) add_cost(desc[i], wc.flops, wc.bytes);
+    kind_flops[kKindWarp] += wc.flops;
     warp_classes.push_back(wc);
     order.insert(order.end(), mb.begin(), mb.end());
   }
@@ -166,43 +167,71 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
   std::vector<StepItem> items, back;
   step_flops = step_bytes = 0.0;
   for (int32_t i : step_members) add_cost(desc[i], step_flops, step_bytes);
+  if (const char* e = std::getenv("NPPB_CHAINS")) nchains = std::max(1, std::atoi(e));
   if (nstep_sys) {
-    const int nbig = desc[step_members[0]].n;
-    if (!solve_only) {
-      for (int k0 = 0; k0 < nbig; k0 += kStepNB) {
-        Step st;
-        st.k0 = k0;
-        int64_t act = 0;
-        while (act < nstep_sys && desc[step_members[act]].n > k0) ++act;
-        // panel launches: contiguous runs with the same panel-height class
-        int64_t b = 0;
-        while (b < act) {
-          const int pc = panel_class(desc[step_members[b]].n - k0);
-          int64_t e = b;
-          while (e < act && panel_class(desc[step_members[e]].n - k0) == pc) ++e;
-          st.panels.push_back({b, e - b, desc[step_members[b]].n - k0});
-          b = e;
+    step_nmax = desc[step_members[0]].n;
+    const int G = (int)std::min<int64_t>(nchains, nstep_sys);
+    // chain g takes every G-th system of the sorted list: similar order mixes
+    std::vector<int32_t> list;
+    list.reserve(nstep_sys);
+    std::vector<int64_t> chain_first(G);
+    for (int g = 0; g < G; ++g) {
+      chain_first[g] = (int64_t)list.size();
+      for (int64_t r = g; r < nstep_sys; r += G) list.push_back(step_members[r]);
+    }
+    for (int g = 0; g < G; ++g) {
+      const int64_t first = chain_first[g];
+      const int64_t num = (g + 1 < G ? chain_first[g + 1] : (int64_t)list.size()) - first;
+      Chain ch;
+      ch.nmax = desc[list[first]].n;
+      if (!solve_only) {
+        for (int k0 = 0; k0 < ch.nmax; k0 += kStepNB) {
+          Step st;
+          st.k0 = k0;
+          int64_t act = 0;
+          while (act < num && desc[list[first + act]].n > k0) ++act;
+          // panel launches: contiguous runs with the same panel-height class
+          int64_t b = 0;
+          while (b < act) {
+            const int pc = panel_class(desc[list[first + b]].n - k0);
+            int64_t e = b;
+            while (e < act && panel_class(desc[list[first + e]].n - k0) == pc) ++e;
+            st.panels.push_back({first + b, e - b, desc[list[first + b]].n - k0});
+            b = e;
+          }
+          st.item_first = (int64_t)items.size();
+          st.nmax = ch.nmax;
+          for (int64_t r = 0; r < act; ++r) {
+            const int32_t si = list[first + r];
+            const SysDesc& s = desc[si];
+            {
+              const double m = s.n - k0, kb = std::min(32.0, m);
+              const double w = (s.n - k0 - kb) + (solve ? s.nrhs : 0) + (s.inv_off >= 0 ? s.n : 0);
+              for (int j = 0; j < (int)kb; ++j) kind_flops[kKindPanel] += (m - j - 1) * (1.0 + 2.0 * (kb - j - 1));
+              kind_flops[kKindUpdate] += kb * kb * w + 2.0 * (m - kb) * kb * w;
+            }
+            add_strips(items, si, kSegMatrix, k0 + kStepNB, s.n);
+            if (solve && s.nrhs) add_strips(items, si, kSegRhs, 0, s.nrhs);
+            if (s.inv_off >= 0) add_strips(items, si, kSegInv, 0, s.n);
+            if ((fl & NPPB_WANT_LU) && k0 > 0) add_strips(items, si, kSegLeft, 0, k0);
+          }
+          st.item_count = (int64_t)items.size() - st.item_first;
+          ch.steps.push_back(st);
         }
-        st.item_first = (int64_t)items.size();
-        st.nmax = nbig;
-        for (int64_t r = 0; r < act; ++r) {
-          const SysDesc& s = desc[step_members[r]];
-          const int32_t si = step_members[r];
-          add_strips(items, si, kSegMatrix, k0 + kStepNB, s.n);
-          if (solve && s.nrhs) add_strips(items, si, kSegRhs, 0, s.nrhs);
-          if (s.inv_off >= 0) add_strips(items, si, kSegInv, 0, s.n);
-          if ((fl & NPPB_WANT_LU) && k0 > 0) add_strips(items, si, kSegLeft, 0, k0);
-        }
-        st.item_count = (int64_t)items.size() - st.item_first;
-        steps.push_back(st);
       }
+      ch.back_first = (int64_t)back.size();
+      for (int64_t r = 0; r < num; ++r) {
+        const int32_t si = list[first + r];
+        const SysDesc& s = desc[si];
+        const double cols = (solve ? s.nrhs : 0) + ((s.inv_off >= 0 && !solve_only) ? s.n : 0);
+        kind_flops[kKindBack] += (double)s.n * s.n * cols * (solve_only ? 2.0 : 1.0);
+        if (solve && s.nrhs) add_strips(back, si, kSegRhs, 0, s.nrhs);
+        if (s.inv_off >= 0 && !solve_only) add_strips(back, si, kSegInv, 0, s.n);
+      }
+      ch.back_count = (int64_t)back.size() - ch.back_first;
+      chains.push_back(ch);
     }
-    for (int32_t si : step_members) {
-      const SysDesc& s = desc[si];
-      if (solve && s.nrhs) add_strips(back, si, kSegRhs, 0, s.nrhs);
-      if (s.inv_off >= 0 && !solve_only) add_strips(back, si, kSegInv, 0, s.n);
-    }
-    step_nmax = nbig;
+    step_members.swap(list);
   }
   nback = (int64_t)back.size();
 
@@ -276,15 +305,16 @@ cudaError_t Plan::launch_warp(const Ptrs& p, int cls, cudaStream_t st) const {
   return launch_lu_warp(warp_batch(p), d_order + c.first, (int)c.num, c.bound, st);
 }
 
-cudaError_t Plan::launch_steps(const Ptrs& p, cudaStream_t st) const {
-  if (!nstep_sys) return cudaSuccess;
+cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
   const StepArgs sa = step_args(p);
+  const Chain& ch = chains[c];
+  const StepItem* back = d_back + ch.back_first;
   if (solve_only) {
-    cudaError_t e = launch_forward(sa, d_back, (int)nback, step_nmax, st);
+    cudaError_t e = launch_forward(sa, back, (int)ch.back_count, ch.nmax, st);
     if (e != cudaSuccess) return e;
-    return launch_back(sa, d_back, (int)nback, st);
+    return launch_back(sa, back, (int)ch.back_count, st);
   }
-  for (const Step& s : steps) {
+  for (const Step& s : ch.steps) {
     for (const auto& pr : s.panels) {
       cudaError_t e = launch_panel(sa, d_step_list + pr.first, (int)pr.num, pr.mmax, s.k0, st);
       if (e != cudaSuccess) return e;
@@ -292,7 +322,52 @@ cudaError_t Plan::launch_steps(const Ptrs& p, cudaStream_t st) const {
     cudaError_t e = launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st);
     if (e != cudaSuccess) return e;
   }
-  return launch_back(sa, d_back, (int)nback, st);
+  return launch_back(sa, back, (int)ch.back_count, st);
+}
+
+int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
+  for (int k = 0; k < kKinds; ++k) ms[k] = 0.0;
+  cudaEvent_t e0, e1;
+  NPPB_CUDA(cudaEventCreate(&e0), "event");
+  NPPB_CUDA(cudaEventCreate(&e1), "event");
+  cudaError_t err = cudaSuccess;
+  auto timed = [&](int kind, auto&& launch) {
+    if (err != cudaSuccess) return;
+    err = cudaEventRecord(e0, st);
+    if (err == cudaSuccess) err = launch();
+    if (err == cudaSuccess) err = cudaEventRecord(e1, st);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float t = 0.f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&t, e0, e1);
+    ms[kind] += t;
+  };
+  for (int c = 0; c < (int)warp_classes.size(); ++c) timed(kKindWarp, [&] { return launch_warp(p, c, st); });
+  const StepArgs sa = step_args(p);
+  for (const Chain& ch : chains) {
+    const StepItem* back = d_back + ch.back_first;
+    if (solve_only) {
+      timed(kKindBack, [&] { return launch_forward(sa, back, (int)ch.back_count, ch.nmax, st); });
+    } else {
+      for (const Step& s : ch.steps) {
+        for (const auto& pr : s.panels)
+          timed(kKindPanel, [&] { return launch_panel(sa, d_step_list + pr.first, (int)pr.num, pr.mmax, s.k0, st); });
+        timed(kKindUpdate, [&] { return launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st); });
+      }
+    }
+    timed(kKindBack, [&] { return launch_back(sa, back, (int)ch.back_count, st); });
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return cuda_status(err, "kernel timing");
+  return NPPB_OK;
+}
+
+cudaError_t Plan::launch_steps(const Ptrs& p, cudaStream_t st) const {
+  for (int c = 0; c < (int)chains.size(); ++c) {
+    cudaError_t e = launch_chain(p, c, st);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 int Plan::execute(const Ptrs& p, cudaStream_t st) {
@@ -308,7 +383,8 @@ int Plan::execute(const Ptrs& p, cudaStream_t st) {
   cudaGetDevice(&cur);
   if (cur != dev) return arg_error("plan used on a different device than it was created on");
   std::lock_guard<std::mutex> lk(mu);
-  const int branches = num_kernel_groups();
+  const int nwarp = (int)warp_classes.size();
+  const int branches = nwarp + (int)chains.size();
   // executions share the plan's workspace: each one starts after the previous
   if (!done) NPPB_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming), "event");
   else NPPB_CUDA(cudaStreamWaitEvent(st, done, 0), "stream wait");
@@ -335,12 +411,12 @@ int Plan::execute(const Ptrs& p, cudaStream_t st) {
     if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
     NPPB_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
     cudaError_t err = cudaEventRecord(fork, cap);
-    // the step chain is the long pole: start it first
+    // the step chains are the long poles: start them first
     for (int b = 0; b < branches && err == cudaSuccess; ++b) {
-      const int i = (b + branches - 1) % branches;
+      const int i = (b + nwarp) % branches;
       err = cudaStreamWaitEvent(side[i], fork, 0);
       if (err == cudaSuccess)
-        err = (i < (int)warp_classes.size()) ? launch_warp(p, i, side[i]) : launch_steps(p, side[i]);
+        err = (i < nwarp) ? launch_warp(p, i, side[i]) : launch_chain(p, i - nwarp, side[i]);
       if (err == cudaSuccess) err = cudaEventRecord(join[i], side[i]);
       if (err == cudaSuccess) err = cudaStreamWaitEvent(cap, join[i], 0);
     }
@@ -364,9 +440,12 @@ int Plan::num_kernel_groups() const { return (int)warp_classes.size() + (nstep_s
 
 int Plan::launches_per_execute() const {
   int l = (int)warp_classes.size();
-  if (nstep_sys) {
-    if (solve_only) return l + 2;
-    for (const Step& s : steps) l += (int)s.panels.size() + 1;
+  for (const Chain& ch : chains) {
+    if (solve_only) {
+      l += 2;
+      continue;
+    }
+    for (const Step& s : ch.steps) l += (int)s.panels.size() + 1;
     l += 1;
   }
   return l;
@@ -561,6 +640,8 @@ int nppb_plan_destroy(nppb_plan* plan) {
 
 int nppb_plan_num_classes(const nppb_plan* plan) { return plan ? plan->p.num_kernel_groups() : 0; }
 
+int nppb_plan_num_launches(const nppb_plan* plan) { return plan ? plan->p.launches_per_execute() : 0; }
+
 int nppb_plan_class_info(const nppb_plan* plan, int c, int* is_warp, int* bound, int64_t* systems,
                          double* flops, double* bytes) {
   if (!plan || c < 0 || c >= plan->p.num_kernel_groups()) {
@@ -615,6 +696,22 @@ int nppb_plan_time_classes(nppb_plan* plan, const double* dA, const double* dB, 
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     return rc;
+  });
+}
+
+int nppb_plan_time_kernels(nppb_plan* plan, const double* dA, const double* dB, double* dX,
+                           double* dInv, double* dDet, double* dSign, double* dLogabs, int32_t* dinfo,
+                           void* stream, double* ms_out, double* flops_out) {
+  return guarded([&]() -> int {
+    if (!plan || !ms_out) {
+      nppb::set_error("bad plan or ms_out");
+      return NPPB_E_ARG;
+    }
+    Plan& pl = plan->p;
+    if (flops_out)
+      for (int k = 0; k < Plan::kKinds; ++k) flops_out[k] = pl.kind_flops[k];
+    return pl.time_kernels(dev_ptrs(pl, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo),
+                           static_cast<cudaStream_t>(stream), ms_out);
   });
 }
 

@@ -44,6 +44,14 @@ class Plan {
     int64_t item_first = 0, item_count = 0;
     int nmax = 0;
   };
+  // An independent sequence of steps over a subset of the step-wise systems;
+  // chains run on separate graph branches so one chain's latency-bound panels
+  // overlap another chain's tensor-core updates.
+  struct Chain {
+    std::vector<Step> steps;
+    int64_t back_first = 0, back_count = 0;
+    int nmax = 0;
+  };
 
   Plan() = default;
   Plan(const Plan&) = delete;
@@ -56,8 +64,16 @@ class Plan {
             const int64_t* b_off, const int64_t* inv_off, int flags, bool solve_only, bool own_lu);
   int execute(const Ptrs& p, cudaStream_t st);
   cudaError_t launch_warp(const Ptrs& p, int cls, cudaStream_t st) const;
-  cudaError_t launch_steps(const Ptrs& p, cudaStream_t st) const;
+  cudaError_t launch_chain(const Ptrs& p, int chain, cudaStream_t st) const;
+  // Every launch of one execution in order, each between two CUDA events on
+  // `st`; ms[kind] accumulates the durations per kernel kind (KernelKind).
+  int time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const;
+  cudaError_t launch_steps(const Ptrs& p, cudaStream_t st) const;  // every chain, in order
   int num_kernel_groups() const;
+  // Work each kernel kind does per execution (flops of the arithmetic it runs,
+  // triangular parts counted as triangles) and the launches per kind.
+  enum KernelKind { kKindWarp = 0, kKindPanel = 1, kKindUpdate = 2, kKindBack = 3, kKinds = 4 };
+  double kind_flops[kKinds] = {0, 0, 0, 0};
   int launches_per_execute() const;
 
   int dev = -1;
@@ -67,7 +83,8 @@ class Plan {
   bool use_graph = true;
   int64_t a_elems = 0, b_elems = 0, inv_elems = 0, lu_elems = 0, piv_elems = 0;
   std::vector<WarpClass> warp_classes;
-  std::vector<Step> steps;
+  std::vector<Chain> chains;
+  int nchains = 3;
   int64_t nstep_sys = 0, nback = 0;
   int step_nmax = 0;
   double step_flops = 0.0, step_bytes = 0.0;

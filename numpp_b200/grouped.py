@@ -60,6 +60,21 @@ class Plan:
                                              st, reps, ms))
         return [ms[i] for i in range(nc)]
 
+    KINDS = ("warp_lu", "panel", "update", "back")
+
+    def launches(self) -> int:
+        """Kernel launches per execution (nodes of the replayed graph)."""
+        return int(self.L.nppb_plan_num_launches(self.h))
+
+    def time_kernels(self, A, B, X, Inv, Det, Sign, Logabs, info, stream=None):
+        """{kind: (ms, flops)} summed over the launches of one execution."""
+        ms = (C.c_double * 4)()
+        fl = (C.c_double * 4)()
+        st = stream if isinstance(stream, int) or stream is None else stream.cuda_stream
+        _check(self.L.nppb_plan_time_kernels(self.h, *(_lib.ptr(x) for x in (A, B, X, Inv, Det, Sign, Logabs, info)),
+                                             st, ms, fl))
+        return {k: (ms[i], fl[i]) for i, k in enumerate(self.KINDS)}
+
     def close(self):
         if getattr(self, "h", None):
             self.L.nppb_plan_destroy(self.h)

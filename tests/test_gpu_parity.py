@@ -131,8 +131,8 @@ def test_singular_systems(lib, oracle, n):
     rng = np.random.default_rng(n)
     A = rng.standard_normal((4, n, n))
     A[1] = 0.0                      # zero matrix: first pivot is zero
-    A[2, n - 1] = A[2, 0]           # duplicate row: exact zero pivot later
-    A[3, :, n // 2] = 0.0           # zero column
+    A[2, n // 3] = 0.0              # zero row: stays zero, exact zero pivot at the end
+    A[3, :, n // 2] = 0.0           # zero column: exact zero pivot at that column
     det = np.zeros(4)
     assert lib.nppb_det_batched(4, n, P(A), P(det)) == 0
     do = oracle.det(A)
@@ -149,6 +149,13 @@ def test_singular_systems(lib, oracle, n):
     assert info[0] == 0 and np.all(info[1:] > 0)
     assert np.array_equal(info == 0, ok == 1)
     assert info[1] == 1                # zero matrix stops at the first column
+    # a duplicated row is singular only up to rounding: no exact-zero promise either side
+    D = A[:1].copy()
+    D[0, n - 1] = D[0, 0]
+    dd = np.zeros(1)
+    assert lib.nppb_det_batched(1, n, P(D), P(dd)) == 0
+    scale = np.prod(np.linalg.norm(D[0], axis=1))
+    assert abs(dd[0]) <= 1e-10 * scale and abs(oracle.det(D)[0]) <= 1e-10 * scale
 
 
 def test_zero_order_and_empty(lib):
