@@ -44,10 +44,11 @@ template <int NT, int RPT>
 __global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
 k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   constexpr int NW = NT / 32;
-  __shared__ double cand_row[2][NW][NB];
+  __shared__ __align__(16) double cand_row[2][NW][NB];
   __shared__ double cand_v[2][NW];
   __shared__ int cand_k[2][NW];
   __shared__ double L11[NB][LS];
+  __shared__ double Xinv[NB][LS];
   __shared__ double pvals[NB];
   __shared__ int s_ndisp;
 
@@ -80,64 +81,103 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   }
   if (tid == 0) s_ndisp = 0;
 
+  // Column loop. Each row is kept rotated so that the current block of 8
+  // columns always sits in a[q][0..7]: the body below is written once for 8
+  // columns (compile-time register indices) and run 4 times, with an 8-place
+  // circular rotation in between; after the 4th rotation the row is back in
+  // column order. The multiplier L (rows below the pivot) overwrites the
+  // column entry it came from. Small code, few moves per column.
   int info = 0;
   int nswap = 0;
-  {
-#pragma unroll 32
-    for (int j = 0; j < NB; ++j) {
-      if (j >= kb || info) continue;
-      double best = -1.0;
-      int key = INT_MAX;
+#pragma unroll 1
+  for (int jb = 0; jb < NB; jb += 8) {
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (valid[q] && pos[q] >= j) {
-          const double v = fabs(a[q][j]);
-          if (v > best || (v == best && pos[q] < key)) { best = v; key = pos[q]; }
+    for (int u = 0; u < 8; ++u) {
+      const int j = jb + u;
+      if (j < kb && !info) {  // uniform across the CTA
+        double best = -1.0;
+        int key = INT_MAX;
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          if (valid[q] && pos[q] >= j) {
+            const double v = fabs(a[q][u]);
+            if (v > best || (v == best && pos[q] < key)) { best = v; key = pos[q]; }
+          }
+        }
+        warp_argmax_abs(best, key);
+        const int par = j & 1;
+        if (lane == 0) { cand_v[par][warp] = best; cand_k[par][warp] = key; }
+        // the candidate row is published with its finished columns (rotated
+        // slots past lim) zeroed, so the update below needs no predicates
+        const int lim = NB - 1 - jb;
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          if (valid[q] && pos[q] == key) {
+            double2* cr = reinterpret_cast<double2*>(cand_row[par][warp]);
+#pragma unroll
+            for (int c = 0; c < NB / 2; ++c)
+              cr[c] = make_double2(2 * c <= lim ? a[q][2 * c] : 0.0, 2 * c + 1 <= lim ? a[q][2 * c + 1] : 0.0);
+          }
+        }
+        __syncthreads();
+        double gb = -1.0;
+        int gk = INT_MAX, gw = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+          const double v = cand_v[par][w];
+          const int k = cand_k[par][w];
+          if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
+        }
+        if (gb == 0.0) {
+          info = k0 + j + 1;
+        } else {
+          const double2* pr2 = reinterpret_cast<const double2*>(cand_row[par][gw]);
+          const double pj = cand_row[par][gw][u];
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            if (valid[q]) {
+              if (pos[q] == j) pos[q] = gk;
+              else if (pos[q] == gk) pos[q] = j;
+            }
+          }
+          if (tid == 0) {
+            pvals[j] = pj;
+            if (sa.ipiv) sa.ipiv[d.piv_off + k0 + j] = k0 + gk;
+          }
+          nswap += (gk != j);
+          // rotated columns u+1 .. lim hold the trailing columns j+1 .. 31; the
+          // published pivot row is zero beyond lim, so those slots stay as they are
+          const double rp = 1.0 / pj;
+          double f[RPT];
+#pragma unroll
+          for (int q = 0; q < RPT; ++q) {
+            const bool below = valid[q] && pos[q] > j;
+            f[q] = below ? a[q][u] * rp : 0.0;
+            if (below) a[q][u] = f[q];
+          }
+#pragma unroll
+          for (int c2 = (u + 1) / 2; c2 < NB / 2; ++c2) {
+            const double2 t = pr2[c2];
+            const int c = 2 * c2;
+#pragma unroll
+            for (int q = 0; q < RPT; ++q) {
+              if (c > u) a[q][c] = fma(-f[q], t.x, a[q][c]);
+              a[q][c + 1] = fma(-f[q], t.y, a[q][c + 1]);
+            }
+          }
         }
       }
-      warp_argmax_abs(best, key);
-      const int par = j & 1;
-      if (lane == 0) { cand_v[par][warp] = best; cand_k[par][warp] = key; }
+    }
+    // circular rotation by 8
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (valid[q] && pos[q] == key) {
-#pragma unroll 32
-          for (int c = 0; c < NB; ++c) cand_row[par][warp][c] = a[q][c];
-        }
-      }
-      __syncthreads();
-      double gb = -1.0;
-      int gk = INT_MAX, gw = 0;
+    for (int q = 0; q < RPT; ++q) {
+      double t[8];
 #pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        const double v = cand_v[par][w];
-        const int k = cand_k[par][w];
-        if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
-      }
-      if (gb == 0.0) { info = k0 + j + 1; continue; }
-      const double* prow = cand_row[par][gw];
-      const double pj = prow[j];
+      for (int c = 0; c < 8; ++c) t[c] = a[q][c];
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (valid[q]) {
-          if (pos[q] == j) pos[q] = gk;
-          else if (pos[q] == gk) pos[q] = j;
-        }
-      }
-      if (tid == 0) {
-        pvals[j] = pj;
-        if (sa.ipiv) sa.ipiv[d.piv_off + k0 + j] = k0 + gk;
-      }
-      nswap += (gk != j);
+      for (int c = 0; c < NB - 8; ++c) a[q][c] = a[q][c + 8];
 #pragma unroll
-      for (int q = 0; q < RPT; ++q) {
-        if (valid[q] && pos[q] > j) {
-          const double f = a[q][j] / pj;
-          a[q][j] = f;
-#pragma unroll 32
-          for (int c = j + 1; c < NB; ++c) a[q][c] = fma(-f, prow[c], a[q][c]);
-        }
-      }
+      for (int c = 0; c < 8; ++c) a[q][NB - 8 + c] = t[c];
     }
   }
 
@@ -184,22 +224,30 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   __syncthreads();
   if (tid == 0) sc->ndisp = s_ndisp;
 
-  // L11^-1 (unit lower, identity-padded past kb): lane c builds column c
+  // L11^-1 (unit lower, identity-padded past kb): lane c builds column c in
+  // shared memory; four partial sums per entry shorten the dependent chain
   if (warp == 0) {
-    double x[NB];
-#pragma unroll 32
+#pragma unroll 1
     for (int i = 0; i < NB; ++i) {
-      double s = (i == lane) ? 1.0 : 0.0;
-#pragma unroll 32
-      for (int q = 0; q < i; ++q) s = fma(-L11[i][q], x[q], s);
-      x[i] = s;
+      double p0 = (i == lane) ? 1.0 : 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+      int q = 0;
+#pragma unroll 1
+      for (; q + 3 < i; q += 4) {
+        p0 = fma(-L11[i][q], Xinv[q][lane], p0);
+        p1 = fma(-L11[i][q + 1], Xinv[q + 1][lane], p1);
+        p2 = fma(-L11[i][q + 2], Xinv[q + 2][lane], p2);
+        p3 = fma(-L11[i][q + 3], Xinv[q + 3][lane], p3);
+      }
+#pragma unroll 1
+      for (; q < i; ++q) p0 = fma(-L11[i][q], Xinv[q][lane], p0);
+      const double x = (p0 + p1) + (p2 + p3);
+      Xinv[i][lane] = x;
+      sc->linv[i * NB + lane] = x;
     }
-#pragma unroll 32
-    for (int i = 0; i < NB; ++i) sc->linv[i * NB + lane] = x[i];
   }
 
   // det / slogdet: pivots folded in the reference's order (linalg.cpp:400-403, 425-431)
-  if (warp == 0) {
+  if (warp == (NW > 1 ? 1 : 0)) {
     const double lg = lane < kb ? log(fabs(pvals[lane])) : 0.0;
     const int ns = nswap;  // every thread counted the same exchanges
     double det = sc->det, la = sc->logabs, sg = sc->sign;
