@@ -98,8 +98,35 @@ int d_linalg(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA
   if ((flags & NPPB_WANT_SLOGDET) && (!dSign || !dLogabs)) return arg_error("slogdet needs Sign and Logabs");
   if ((flags & NPPB_WANT_LU) && nn && (!dLU || !dipiv)) return arg_error("keeping factors needs LU and ipiv");
   if (!device()) return NPPB_E_NODEV;
+  if (n > 32 && !(flags & NPPB_WANT_LU)) {
+    // step-wise kernels in uniform mode: workspace and per-system scratch only
+    DevMem lu_m, sc_m;
+    double* LU = dLU;
+    if (!LU) {
+      NPPB_RC(scratch<double>(lu_m, (size_t)count * nn, st));
+      LU = lu_m.as<double>();
+    }
+    NPPB_RC(scratch<StepScratch>(sc_m, (size_t)count, st));
+    StepArgs sa{};
+    sa.scratch = sc_m.as<StepScratch>();
+    sa.A = (dA == LU) ? nullptr : dA;
+    sa.LU = LU;
+    sa.ipiv = dipiv;
+    sa.B = dB; sa.X = dX;
+    sa.inv = (flags & NPPB_WANT_INV) ? dInv : nullptr;
+    sa.det = (flags & NPPB_WANT_DET) ? dDet : nullptr;
+    sa.sign = (flags & NPPB_WANT_SLOGDET) ? dSign : nullptr;
+    sa.logabs = (flags & NPPB_WANT_SLOGDET) ? dLogabs : nullptr;
+    sa.info = dinfo;
+    sa.un = n;
+    sa.unrhs = (flags & NPPB_WANT_SOLVE) ? nrhs : 0;
+    sa.uinv = (flags & NPPB_WANT_INV) ? 1 : 0;
+    NPPB_CUDA(run_step_uniform(sa, (int)count, st), "batched LU launch");
+    return NPPB_OK;
+  }
   if (n > 32) {
-    // step-wise path through a cached uniform plan
+    // factors kept (getrf): a cached uniform plan also carries the row moves
+    // into the columns left of each panel
     int rc = NPPB_OK;
     const bool own_lu = dLU == nullptr;
     auto pl = uniform_plan(count, n, nrhs, flags, false, own_lu, &rc);

@@ -39,6 +39,52 @@ constexpr int LS = NB + 1;   // 33: stride of 32-wide shared tiles
 constexpr int WS = 64 + 1;   // 65: stride of 64-wide shared tiles
 
 // ---------------------------------------------------------------------------
+// System descriptor: from the list, or derived for a uniform batch.
+__device__ __forceinline__ SysDesc step_desc(const StepArgs& sa, int s) {
+  if (sa.desc) return sa.desc[s];
+  SysDesc d;
+  const int64_t n = sa.un, nn = n * n;
+  d.n = sa.un;
+  d.nrhs = sa.unrhs;
+  d.idx = s;
+  d.pad_ = s;
+  d.a_off = s * nn;
+  d.lu_off = s * nn;
+  d.b_off = s * n * sa.unrhs;
+  d.inv_off = sa.uinv ? s * nn : -1;
+  d.piv_off = s * n;
+  return d;
+}
+
+__device__ __forceinline__ StepItem uniform_item(const StepArgs& sa, int b, int k0, bool back) {
+  const int n = sa.un;
+  const int trail = n - k0 - NB;
+  const int nm = back ? 0 : (trail > 0 ? (trail + 63) / 64 : 0);
+  const int nr = (sa.unrhs + 63) / 64;
+  const int ni = sa.uinv ? (n + 63) / 64 : 0;
+  const int per = nm + nr + ni;
+  StepItem it;
+  it.sys = b / per;
+  int r = b % per;
+  it.pad_ = 0;
+  if (r < nm) {
+    it.kind = kSegMatrix;
+    it.c0 = k0 + NB + 64 * r;
+    it.width = (int16_t)min(64, n - it.c0);
+  } else if ((r -= nm) < nr) {
+    it.kind = kSegRhs;
+    it.c0 = 64 * r;
+    it.width = (int16_t)min(64, sa.unrhs - it.c0);
+  } else {
+    r -= nr;
+    it.kind = kSegInv;
+    it.c0 = 64 * r;
+    it.width = (int16_t)min(64, n - it.c0);
+  }
+  return it;
+}
+
+// ---------------------------------------------------------------------------
 // k_panel
 template <int NT, int RPT>
 __global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
@@ -53,7 +99,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   __shared__ int s_ndisp;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const SysDesc d = sa.desc[list[blockIdx.x]];
+  const SysDesc d = step_desc(sa, list ? list[blockIdx.x] : (int)blockIdx.x);
   StepScratch* sc = sa.scratch + d.pad_;
   const int n = d.n, m = n - k0, kb = min(NB, m);
   if (k0 == 0) {
@@ -380,8 +426,8 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
   int* dmap = dsrc + NB;             // m entries: displaced index of each row, or -1
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const StepItem it = items[blockIdx.x];
-  const SysDesc d = sa.desc[it.sys];
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, k0, false);
+  const SysDesc d = step_desc(sa, it.sys);
   const StepScratch* sc = sa.scratch + d.pad_;
   if (sc->info) return;
   const int n = d.n, m = n - k0, kb = min(NB, m), w = it.width, c0 = it.c0;
@@ -548,8 +594,8 @@ k_back(StepArgs sa, const StepItem* __restrict__ items) {
   __shared__ double Xb[NB * WS];
   __shared__ double As[64 * LS];
   const int tid = threadIdx.x;
-  const StepItem it = items[blockIdx.x];
-  const SysDesc d = sa.desc[it.sys];
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
   if (!sa.solve_only && sa.scratch[d.pad_].info) return;
   const int n = d.n, w = it.width, c0 = it.c0;
   const double* U = sa.LU + d.lu_off;
@@ -603,8 +649,8 @@ k_forward(StepArgs sa, const StepItem* __restrict__ items) {
   double* As = Xb + NB * WS;     // 64 x LS
   int* perm = reinterpret_cast<int*>(As + 64 * LS);
   const int tid = threadIdx.x;
-  const StepItem it = items[blockIdx.x];
-  const SysDesc d = sa.desc[it.sys];
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
   const int n = d.n, w = it.width, c0 = it.c0, ld = d.nrhs;
   const double* L = sa.LU + d.lu_off;
   const int32_t* ipiv = sa.ipiv + d.piv_off;

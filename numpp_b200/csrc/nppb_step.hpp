@@ -52,10 +52,26 @@ struct StepArgs {
   double* logabs;
   int32_t* info;
   int solve_only;    // getrs from stored factors: no factorisation state to consult
+  // Uniform batch (desc == nullptr): system s has order un, unrhs right-hand
+  // sides, A / LU / inverse at s*un*un, B / X at s*un*unrhs, ipiv at s*un,
+  // scratch slot s; an inverse for every system when uinv != 0.
+  int un, unrhs, uinv;
 };
+
+// Work items of a uniform batch at step k0 (k_update) and of its back
+// substitution, per system; grids are count times these.
+__host__ __device__ inline int uniform_update_strips(int n, int nrhs, int inv, int k0) {
+  const int trail = n - k0 - kStepNB;
+  return (trail > 0 ? (trail + 63) / 64 : 0) + (nrhs + 63) / 64 + (inv ? (n + 63) / 64 : 0);
+}
+__host__ __device__ inline int uniform_back_strips(int n, int nrhs, int inv) {
+  return (nrhs + 63) / 64 + (inv ? (n + 63) / 64 : 0);
+}
 
 cudaError_t step_prepare();
 // Panel of every listed system at column k0; mmax = largest n - k0 among them.
+// list == nullptr: systems 0..nsys-1 of a uniform batch. Likewise items ==
+// nullptr below means the uniform-batch items, derived from the block index.
 cudaError_t launch_panel(const StepArgs& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st);
 // Row moves + U12 + trailing update for each strip item of step k0 (nmax >= n of any item).

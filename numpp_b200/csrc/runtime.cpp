@@ -2,6 +2,7 @@
 // order -> kernel choice for uniform batches. C++20.
 #include "runtime.hpp"
 
+#include <climits>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -103,6 +104,22 @@ void DevMem::release() {
 }
 
 cudaError_t prepare_kernels() { return step_prepare(); }
+
+cudaError_t run_step_uniform(const StepArgs& sa, int count, cudaStream_t st) {
+  const int n = sa.un;
+  if (n <= 32 || n > kStepMaxN || count <= 0) return cudaErrorInvalidValue;
+  for (int k0 = 0; k0 < n; k0 += kStepNB) {
+    cudaError_t e = launch_panel(sa, nullptr, count, n - k0, k0, st);
+    if (e != cudaSuccess) return e;
+    const int64_t items = (int64_t)count * uniform_update_strips(n, sa.unrhs, sa.uinv, k0);
+    if (items > INT32_MAX) return cudaErrorInvalidValue;
+    e = launch_update(sa, nullptr, (int)items, n, k0, st);
+    if (e != cudaSuccess) return e;
+  }
+  const int64_t back = (int64_t)count * uniform_back_strips(n, sa.unrhs, sa.uinv);
+  if (back > INT32_MAX) return cudaErrorInvalidValue;
+  return launch_back(sa, nullptr, (int)back, st);
+}
 
 cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
   if (n > 32) return cudaErrorInvalidValue;
