@@ -120,6 +120,23 @@ int nppb_d_linalg_batched(int64_t count, int32_t n, int32_t nrhs, int flags, con
 int nppb_d_getrs_batched(int64_t count, int32_t n, int32_t nrhs, const double* dLU,
                          const int32_t* dipiv, const double* dB, double* dX, void* stream);
 
+/* Allocation-free solve. No counterpart in the reference: NumPP's CUDA
+ * backend allocates per call (src/backend/cuda_backend.cu:126-146,189-206).
+ * For callers that must not allocate device memory while they run (code in a
+ * CUDA graph being captured, hosts whose device memory is reserved up front,
+ * fixed-pool allocators): X = A^-1 B for a uniform batch on device buffers,
+ * with no cudaMalloc / cudaFree or allocating call. Orders above 32 use a
+ * fixed 32 MiB scratch array inside the library, so count * (8*n*n + 8616)
+ * bytes must fit in 32 MiB (NPPB_E_RANGE otherwise, before any GPU work);
+ * orders up to 32 need no scratch. The first call on each device looks up the
+ * array's device address, so make that first call before any stream capture;
+ * each device that has set it up keeps the 32 MiB until the process exits.
+ * Every call shares the array: calls that overlap on the GPU (other streams,
+ * other threads) race and must be ordered by the caller. info as for the
+ * other solves; dX must not alias dB. */
+int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA,
+                                 const double* dB, double* dX, int32_t* dinfo, void* stream);
+
 /* ---- uneven batches ------------------------------------------------------ */
 /* A plan packs `count` systems of different orders n[i] and right-hand-side
  * counts nrhs[i] into size classes, one persistent launch per class, and

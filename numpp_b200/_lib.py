@@ -42,6 +42,7 @@ SIGNATURES = {
     "nppb_solve_det_batched": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "nppb_d_linalg_batched": (_int, [_i64, _i32, _i32, _int] + [_vp] * 10 + [_vp]),
     "nppb_d_getrs_batched": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "nppb_d_solve_batched_noalloc": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "nppb_plan_create": (_int, [C.POINTER(_vp), _i64, _vp, _vp, _vp, _vp, _vp, _int]),
     "nppb_plan_sizes": (_int, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "nppb_plan_execute": (_int, [_vp] * 10),
