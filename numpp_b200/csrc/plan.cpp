@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <list>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <string>
@@ -494,6 +495,28 @@ using nppb::Plan;
 
 struct nppb_plan {
   Plan p;
+  // Host-buffer execution pipelined over chunks of systems: the copy of chunk
+  // c+1 runs while chunk c computes (needs a packed layout: offsets ascending).
+  struct Chunk {
+    std::unique_ptr<Plan> plan;
+    int64_t lo = 0, hi = 0;          // systems [lo, hi)
+    int64_t a_lo = 0, a_hi = 0, b_lo = 0, b_hi = 0, i_lo = 0, i_hi = 0;
+    cudaEvent_t in = nullptr, out = nullptr;
+  };
+  std::vector<int32_t> n, nrhs;
+  std::vector<int64_t> a_off, b_off, inv_off;
+  int flags = 0;
+  bool packed = false;
+  std::vector<Chunk> chunks;
+  cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+  ~nppb_plan() {
+    for (auto& c : chunks) {
+      if (c.in) cudaEventDestroy(c.in);
+      if (c.out) cudaEventDestroy(c.out);
+    }
+    for (cudaStream_t st : {s_in, s_comp, s_out})
+      if (st) cudaStreamDestroy(st);
+  }
 };
 
 namespace {
@@ -550,6 +573,32 @@ int nppb_plan_create(nppb_plan** plan, int64_t count, const int32_t* n, const in
       delete pl;
       return rc;
     }
+    const bool solve = flags & NPPB_WANT_SOLVE, inv = flags & NPPB_WANT_INV;
+    pl->flags = flags & ~NPPB_WANT_LU;
+    pl->n.assign(n, n + count);
+    pl->nrhs.assign(count, 0);
+    pl->a_off.assign(a_off, a_off + count);
+    pl->b_off.assign(count, 0);
+    pl->inv_off.assign(count, -1);
+    if (solve) {
+      pl->nrhs.assign(nrhs, nrhs + count);
+      pl->b_off.assign(b_off, b_off + count);
+    }
+    if (inv) pl->inv_off.assign(inv_off, inv_off + count);
+    // packed: every system starts at or after the end of the previous one
+    bool packed = true;
+    int64_t ae = 0, be = 0, ie = 0;
+    for (int64_t i = 0; i < count && packed; ++i) {
+      const int64_t nn = (int64_t)n[i] * n[i];
+      packed = pl->a_off[i] >= ae && pl->b_off[i] >= be;
+      ae = pl->a_off[i] + nn;
+      be = pl->b_off[i] + (int64_t)n[i] * pl->nrhs[i];
+      if (pl->inv_off[i] >= 0) {
+        packed = packed && pl->inv_off[i] >= ie;
+        ie = pl->inv_off[i] + nn;
+      }
+    }
+    pl->packed = packed;
     *plan = pl;
     return NPPB_OK;
   });
@@ -582,6 +631,61 @@ int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, doubl
   });
 }
 
+namespace {
+
+// Splits a packed plan into chunks of systems with their own sub-plans (built
+// on first use).
+int build_chunks(nppb_plan& P) {
+  if (!P.chunks.empty()) return NPPB_OK;
+  int K = 4;
+  if (const char* e = std::getenv("NPPB_HOST_CHUNKS")) K = std::max(1, std::atoi(e));
+  const int64_t count = P.p.count;
+  K = (int)std::min<int64_t>(K, std::max<int64_t>(1, count / 256));
+  for (int c = 0; c < K; ++c) {
+    nppb_plan::Chunk ch;
+    ch.lo = count * c / K;
+    ch.hi = count * (c + 1) / K;
+    if (ch.hi <= ch.lo) continue;
+    const int64_t m = ch.hi - ch.lo;
+    ch.a_lo = P.a_off[ch.lo];
+    ch.b_lo = P.b_off[ch.lo];
+    ch.i_lo = -1;
+    std::vector<int64_t> ao(m), bo(m), io(m);
+    for (int64_t i = 0; i < m; ++i) {
+      const int64_t s = ch.lo + i, nn = (int64_t)P.n[s] * P.n[s];
+      ao[i] = P.a_off[s] - ch.a_lo;
+      bo[i] = P.b_off[s] - ch.b_lo;
+      ch.a_hi = P.a_off[s] + nn;
+      ch.b_hi = std::max(ch.b_hi, P.b_off[s] + (int64_t)P.n[s] * P.nrhs[s]);
+      if (P.inv_off[s] >= 0) {
+        if (ch.i_lo < 0) ch.i_lo = P.inv_off[s];
+        ch.i_hi = P.inv_off[s] + nn;
+      }
+    }
+    if (ch.b_hi < ch.b_lo) ch.b_hi = ch.b_lo;
+    if (ch.i_lo < 0) ch.i_lo = ch.i_hi = 0;
+    for (int64_t i = 0; i < m; ++i) {
+      const int64_t s = ch.lo + i;
+      io[i] = P.inv_off[s] >= 0 ? P.inv_off[s] - ch.i_lo : -1;
+    }
+    ch.plan = std::make_unique<Plan>();
+    const int rc = ch.plan->build(m, P.n.data() + ch.lo, P.nrhs.data() + ch.lo, ao.data(), bo.data(),
+                                  io.data(), P.flags, false, true);
+    if (rc != NPPB_OK) {
+      P.chunks.clear();
+      return rc;
+    }
+    NPPB_CUDA(cudaEventCreateWithFlags(&ch.in, cudaEventDisableTiming), "event");
+    NPPB_CUDA(cudaEventCreateWithFlags(&ch.out, cudaEventDisableTiming), "event");
+    P.chunks.push_back(std::move(ch));
+  }
+  for (cudaStream_t* st : {&P.s_in, &P.s_comp, &P.s_out})
+    NPPB_CUDA(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "stream");
+  return NPPB_OK;
+}
+
+}  // namespace
+
 int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X, double* Inv,
                            double* Det, double* Sign, double* Logabs, int32_t* info) {
   return guarded([&]() -> int {
@@ -608,6 +712,52 @@ int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, do
     if ((f & NPPB_WANT_SOLVE) && pl.b_elems && (!B || !X)) {
       nppb::set_error("solve needs B and X");
       return NPPB_E_ARG;
+    }
+    const bool pipelined = plan->packed && pl.count >= 512 && !std::getenv("NPPB_NO_HOST_PIPELINE");
+    if (pipelined) {
+      rc = build_chunks(*plan);
+      if (rc != NPPB_OK) return rc;
+    }
+    if (pipelined && plan->chunks.size() > 1) {
+      auto cp = [](void* dst, const void* src, size_t bytes, cudaMemcpyKind k, cudaStream_t st) {
+        return (bytes && dst && src) ? cudaMemcpyAsync(dst, src, bytes, k, st) : cudaSuccess;
+      };
+      const size_t D = sizeof(double);
+      for (auto& ch : plan->chunks) {
+        NPPB_CUDA(cp(pl.hA + ch.a_lo, A + ch.a_lo, D * (ch.a_hi - ch.a_lo), cudaMemcpyHostToDevice, plan->s_in),
+                  "host to device copy");
+        if (f & NPPB_WANT_SOLVE)
+          NPPB_CUDA(cp(pl.hB + ch.b_lo, B + ch.b_lo, D * (ch.b_hi - ch.b_lo), cudaMemcpyHostToDevice, plan->s_in),
+                    "host to device copy");
+        NPPB_CUDA(cudaEventRecord(ch.in, plan->s_in), "event record");
+        NPPB_CUDA(cudaStreamWaitEvent(plan->s_comp, ch.in, 0), "stream wait");
+        Plan::Ptrs p = dev_ptrs(*ch.plan, pl.hA + ch.a_lo, pl.hB ? pl.hB + ch.b_lo : nullptr,
+                                pl.hX ? pl.hX + ch.b_lo : nullptr, pl.hInv ? pl.hInv + ch.i_lo : nullptr,
+                                pl.hDet ? pl.hDet + ch.lo : nullptr, pl.hSign ? pl.hSign + ch.lo : nullptr,
+                                pl.hLog ? pl.hLog + ch.lo : nullptr, pl.hInfo + ch.lo);
+        rc = ch.plan->execute(p, plan->s_comp);
+        if (rc != NPPB_OK) return rc;
+        NPPB_CUDA(cudaEventRecord(ch.out, plan->s_comp), "event record");
+        NPPB_CUDA(cudaStreamWaitEvent(plan->s_out, ch.out, 0), "stream wait");
+        const size_t m = (size_t)(ch.hi - ch.lo);
+        if (f & NPPB_WANT_SOLVE)
+          NPPB_CUDA(cp(X + ch.b_lo, pl.hX + ch.b_lo, D * (ch.b_hi - ch.b_lo), cudaMemcpyDeviceToHost, plan->s_out),
+                    "device to host copy");
+        if (f & NPPB_WANT_INV)
+          NPPB_CUDA(cp(Inv + ch.i_lo, pl.hInv + ch.i_lo, D * (ch.i_hi - ch.i_lo), cudaMemcpyDeviceToHost, plan->s_out),
+                    "device to host copy");
+        if (f & NPPB_WANT_DET)
+          NPPB_CUDA(cp(Det + ch.lo, pl.hDet + ch.lo, D * m, cudaMemcpyDeviceToHost, plan->s_out), "device to host copy");
+        if (f & NPPB_WANT_SLOGDET) {
+          NPPB_CUDA(cp(Sign + ch.lo, pl.hSign + ch.lo, D * m, cudaMemcpyDeviceToHost, plan->s_out), "device to host copy");
+          NPPB_CUDA(cp(Logabs + ch.lo, pl.hLog + ch.lo, D * m, cudaMemcpyDeviceToHost, plan->s_out), "device to host copy");
+        }
+        NPPB_CUDA(cp(info + ch.lo, pl.hInfo + ch.lo, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, plan->s_out),
+                  "device to host copy");
+      }
+      NPPB_CUDA(cudaStreamSynchronize(plan->s_out), "stream synchronize");
+      NPPB_CUDA(cudaStreamSynchronize(plan->s_comp), "stream synchronize");
+      return NPPB_OK;
     }
     cudaStream_t st = nppb::thread_stream();
     auto h2d = [&](void* d, const void* h, size_t bytes) {
