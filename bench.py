@@ -279,7 +279,7 @@ def run_b200(args):
     tfile = os.path.join(ROOT, "profiles", "k_update_uneven8192_traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get("bytes_per_launch")
+            traffic = json.load(f).get("bytes_per_step")
 
     # end to end through the C ABI with host buffers (pinned), copies inside the timed region
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
