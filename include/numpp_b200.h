@@ -137,6 +137,30 @@ int nppb_d_getrs_batched(int64_t count, int32_t n, int32_t nrhs, const double* d
 int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                  const double* dB, double* dX, int32_t* dinfo, void* stream);
 
+/* ---- mixed precision: FP32 factors, FP64 iterative refinement ---------- */
+/* No counterpart in the reference (NumPP solves in double only,
+ * src/linalg/linalg.cpp:92-103). X = A^-1 B for a uniform batch: power-of-two
+ * row/column equilibration, LU in FP32 on the step-wise kernels, then FP64
+ * refinement (R = B - A X in FP64, correction solved with the FP32 factors,
+ * added in FP64) until the normwise backward error
+ * eta = max|R| / (||A||_inf max|X| + max|B|) <= tol. A system whose eta stops
+ * halving is stalled; stalled systems, FP32 zero pivots and systems still
+ * refining after max_iter corrections are refactored and solved in FP64.
+ * Per system: berr (final eta), ferr (max|X - Xtrue| / max|Xtrue|, when Xtrue
+ * is given), iters (corrections applied), fallback (1 = the FP64 solve ran),
+ * info (of the FP64 solve, when it ran). Orders <= 32 always take the FP64
+ * warp kernel (fallback = 1). The device form synchronises `stream` (it reads
+ * convergence counts back between corrections). */
+enum { NPPB_MIXED_NO_EQUILIBRATE = 1, NPPB_MIXED_NO_FALLBACK = 2 };
+int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA,
+                               const double* dB, double* dX, const double* dXtrue, double tol,
+                               int32_t max_iter, int flags, int32_t* dinfo, double* dBerr,
+                               double* dFerr, int32_t* dIters, int32_t* dFallback, void* stream);
+int nppb_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* A, const double* B,
+                             double* X, const double* Xtrue, double tol, int32_t max_iter, int flags,
+                             int32_t* info, double* berr, double* ferr, int32_t* iters,
+                             int32_t* fallback);
+
 /* ---- uneven batches ------------------------------------------------------ */
 /* A plan packs `count` systems of different orders n[i] and right-hand-side
  * counts nrhs[i] into size classes, one persistent launch per class, and

@@ -15,6 +15,7 @@ OK, DECLINED = 0, 1
 E_ARG, E_NODEV, E_CUDA, E_NOMEM, E_RANGE = -1, -2, -3, -4, -5
 DT_FLOAT32, DT_FLOAT64 = 10, 11
 WANT_LU, WANT_SOLVE, WANT_DET, WANT_SLOGDET, WANT_INV = 1, 2, 4, 8, 16
+MIXED_NO_EQUILIBRATE, MIXED_NO_FALLBACK = 1, 2
 
 _vp = C.c_void_p
 _i32 = C.c_int32
@@ -43,6 +44,10 @@ SIGNATURES = {
     "nppb_d_linalg_batched": (_int, [_i64, _i32, _i32, _int] + [_vp] * 10 + [_vp]),
     "nppb_d_getrs_batched": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "nppb_d_solve_batched_noalloc": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "nppb_d_solve_mixed_batched": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, C.c_double, _i32, _int,
+                                          _vp, _vp, _vp, _vp, _vp, _vp]),
+    "nppb_solve_mixed_batched": (_int, [_i64, _i32, _i32, _vp, _vp, _vp, _vp, C.c_double, _i32, _int,
+                                        _vp, _vp, _vp, _vp, _vp]),
     "nppb_plan_create": (_int, [C.POINTER(_vp), _i64, _vp, _vp, _vp, _vp, _vp, _int]),
     "nppb_plan_sizes": (_int, [_vp, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
     "nppb_plan_execute": (_int, [_vp] * 10),

@@ -39,4 +39,13 @@ __device__ __forceinline__ void warp_argmax_abs(double& v, int& key) {
   key = k;
 }
 
+// The same for FP32 magnitudes: one 32-bit key.
+__device__ __forceinline__ void warp_argmax_abs(float& v, int& key) {
+  const unsigned bits = v > 0.f ? __float_as_uint(v) : 0u;
+  const unsigned m = __reduce_max_sync(0xffffffffu, bits);
+  const int k = __reduce_min_sync(0xffffffffu, bits == m ? key : INT_MAX);
+  v = __uint_as_float(m);
+  key = k;
+}
+
 }  // namespace nppb

@@ -16,17 +16,21 @@
 //  k_update  one CTA per (system, 64-column strip) of the trailing matrix, of
 //            the right-hand sides (augmented columns: forward substitution rides
 //            along) and of the identity (inverse): apply the row moves,
-//            U12 = L11^-1 A12 and A22 -= L21 U12 on FP64 DMMA (mma.m8n8k4).
+//            U12 = L11^-1 A12 and A22 -= L21 U12.
 //  k_back    one CTA per (system, 64-column strip) of X / inverse: blocked back
-//            substitution with U (diagonal blocks by substitution, the rest DMMA).
+//            substitution with U (diagonal blocks by substitution).
 //  k_forward getrs from stored factors: row gather through the pivots and
 //            blocked forward substitution with the unit-lower L.
 //
-// Step 0 reads A / B / I directly and writes the workspace, so no copy pass is
-// needed. Exact-zero pivots stop the system (info = k+1) and later launches
-// skip it, as the reference stops (linalg.cpp:56).
+// Every kernel is instantiated for FP64 factors (tile products on the FP64
+// tensor pipe, mma.m8n8k4) and for FP32 factors (the mixed-precision path:
+// tile products on FP32 FMA). Step 0 reads A / B / I directly and writes the
+// workspace, so no copy pass is needed. Exact-zero pivots stop the system
+// (info = k+1) and later launches skip it, as the reference stops
+// (linalg.cpp:56).
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "dmma.cuh"
 #include "nppb_step.hpp"
@@ -37,10 +41,12 @@ namespace {
 constexpr int NB = kStepNB;  // 32
 constexpr int LS = NB + 1;   // 33: stride of 32-wide shared tiles
 constexpr int WS = 64 + 1;   // 65: stride of 64-wide shared tiles
+constexpr int UT = 128;      // threads of the strip kernels
 
 // ---------------------------------------------------------------------------
 // System descriptor: from the list, or derived for a uniform batch.
-__device__ __forceinline__ SysDesc step_desc(const StepArgs& sa, int s) {
+template <class T>
+__device__ __forceinline__ SysDesc step_desc(const StepArgsT<T>& sa, int s) {
   if (sa.desc) return sa.desc[s];
   SysDesc d;
   const int64_t n = sa.un, nn = n * n;
@@ -56,13 +62,15 @@ __device__ __forceinline__ SysDesc step_desc(const StepArgs& sa, int s) {
   return d;
 }
 
-__device__ __forceinline__ StepItem uniform_item(const StepArgs& sa, int b, int k0, bool back) {
+template <class T>
+__device__ __forceinline__ StepItem uniform_item(const StepArgsT<T>& sa, int b, int k0, bool back) {
   const int n = sa.un;
   const int trail = n - k0 - NB;
   const int nm = back ? 0 : (trail > 0 ? (trail + 63) / 64 : 0);
   const int nr = (sa.unrhs + 63) / 64;
   const int ni = sa.uinv ? (n + 63) / 64 : 0;
-  const int per = nm + nr + ni;
+  const int nl = (!back && sa.uleft) ? (k0 + 63) / 64 : 0;
+  const int per = nm + nr + ni + nl;
   StepItem it;
   it.sys = b / per;
   int r = b % per;
@@ -75,32 +83,48 @@ __device__ __forceinline__ StepItem uniform_item(const StepArgs& sa, int b, int 
     it.kind = kSegRhs;
     it.c0 = 64 * r;
     it.width = (int16_t)min(64, sa.unrhs - it.c0);
-  } else {
-    r -= nr;
+  } else if ((r -= nr) < ni) {
     it.kind = kSegInv;
     it.c0 = 64 * r;
     it.width = (int16_t)min(64, n - it.c0);
+  } else {
+    r -= ni;
+    it.kind = kSegLeft;
+    it.c0 = 64 * r;
+    it.width = (int16_t)min(64, k0 - it.c0);
   }
   return it;
 }
 
+template <class T> struct Pair;
+template <> struct Pair<double> { using type = double2; };
+template <> struct Pair<float> { using type = float2; };
+template <class T>
+__device__ __forceinline__ typename Pair<T>::type make_pair2(T x, T y) {
+  typename Pair<T>::type p;
+  p.x = x;
+  p.y = y;
+  return p;
+}
+
 // ---------------------------------------------------------------------------
 // k_panel
-template <int NT, int RPT>
+template <class T, int NT, int RPT>
 __global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
-k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
+k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
+  using P2 = typename Pair<T>::type;
   constexpr int NW = NT / 32;
-  __shared__ __align__(16) double cand_row[2][NW][NB];
-  __shared__ double cand_v[2][NW];
+  __shared__ __align__(16) T cand_row[2][NW][NB];
+  __shared__ T cand_v[2][NW];
   __shared__ int cand_k[2][NW];
-  __shared__ double L11[NB][LS];
-  __shared__ double Xinv[NB][LS];
-  __shared__ double pvals[NB];
+  __shared__ T L11[NB][LS];
+  __shared__ T Xinv[NB][LS];
+  __shared__ T pvals[NB];
   __shared__ int s_ndisp;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const SysDesc d = step_desc(sa, list ? list[blockIdx.x] : (int)blockIdx.x);
-  StepScratch* sc = sa.scratch + d.pad_;
+  StepScratchT<T>* sc = sa.scratch + d.pad_;
   const int n = d.n, m = n - k0, kb = min(NB, m);
   if (k0 == 0) {
     if (tid == 0) {
@@ -110,10 +134,10 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   } else if (sc->info) {
     return;
   }
-  double* dst = sa.LU + d.lu_off;
-  const double* src = (k0 == 0 && sa.A) ? sa.A + d.a_off : dst;
+  T* dst = sa.LU + d.lu_off;
+  const T* src = (k0 == 0 && sa.A) ? sa.A + d.a_off : dst;
 
-  double a[RPT][NB];
+  T a[RPT][NB];
   int pos[RPT];
   bool valid[RPT];
 #pragma unroll
@@ -121,9 +145,9 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
     const int r = tid + q * NT;
     valid[q] = r < m;
     pos[q] = r;
-    const double* row = src + (int64_t)(k0 + r) * n + k0;
+    const T* row = src + (int64_t)(k0 + r) * n + k0;
 #pragma unroll
-    for (int c = 0; c < NB; ++c) a[q][c] = (valid[q] && c < kb) ? row[c] : 0.0;
+    for (int c = 0; c < NB; ++c) a[q][c] = (valid[q] && c < kb) ? row[c] : T(0);
   }
   if (tid == 0) s_ndisp = 0;
 
@@ -141,12 +165,12 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
     for (int u = 0; u < 8; ++u) {
       const int j = jb + u;
       if (j < kb && !info) {  // uniform across the CTA
-        double best = -1.0;
+        T best = T(-1);
         int key = INT_MAX;
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
           if (valid[q] && pos[q] >= j) {
-            const double v = fabs(a[q][u]);
+            const T v = fabs(a[q][u]);
             if (v > best || (v == best && pos[q] < key)) { best = v; key = pos[q]; }
           }
         }
@@ -159,26 +183,26 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
 #pragma unroll
         for (int q = 0; q < RPT; ++q) {
           if (valid[q] && pos[q] == key) {
-            double2* cr = reinterpret_cast<double2*>(cand_row[par][warp]);
+            P2* cr = reinterpret_cast<P2*>(cand_row[par][warp]);
 #pragma unroll
             for (int c = 0; c < NB / 2; ++c)
-              cr[c] = make_double2(2 * c <= lim ? a[q][2 * c] : 0.0, 2 * c + 1 <= lim ? a[q][2 * c + 1] : 0.0);
+              cr[c] = make_pair2<T>(2 * c <= lim ? a[q][2 * c] : T(0), 2 * c + 1 <= lim ? a[q][2 * c + 1] : T(0));
           }
         }
         __syncthreads();
-        double gb = -1.0;
+        T gb = T(-1);
         int gk = INT_MAX, gw = 0;
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
-          const double v = cand_v[par][w];
+          const T v = cand_v[par][w];
           const int k = cand_k[par][w];
           if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
         }
-        if (gb == 0.0) {
+        if (gb == T(0)) {
           info = k0 + j + 1;
         } else {
-          const double2* pr2 = reinterpret_cast<const double2*>(cand_row[par][gw]);
-          const double pj = cand_row[par][gw][u];
+          const P2* pr2 = reinterpret_cast<const P2*>(cand_row[par][gw]);
+          const T pj = cand_row[par][gw][u];
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             if (valid[q]) {
@@ -193,17 +217,17 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
           nswap += (gk != j);
           // rotated columns u+1 .. lim hold the trailing columns j+1 .. 31; the
           // published pivot row is zero beyond lim, so those slots stay as they are
-          const double rp = 1.0 / pj;
-          double f[RPT];
+          const T rp = T(1) / pj;
+          T f[RPT];
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             const bool below = valid[q] && pos[q] > j;
-            f[q] = below ? a[q][u] * rp : 0.0;
+            f[q] = below ? a[q][u] * rp : T(0);
             if (below) a[q][u] = f[q];
           }
 #pragma unroll
           for (int c2 = (u + 1) / 2; c2 < NB / 2; ++c2) {
-            const double2 t = pr2[c2];
+            const P2 t = pr2[c2];
             const int c = 2 * c2;
 #pragma unroll
             for (int q = 0; q < RPT; ++q) {
@@ -217,7 +241,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
     // circular rotation by 8
 #pragma unroll
     for (int q = 0; q < RPT; ++q) {
-      double t[8];
+      T t[8];
 #pragma unroll
       for (int c = 0; c < 8; ++c) t[c] = a[q][c];
 #pragma unroll
@@ -241,13 +265,13 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   // panel back at the pivoted positions; L11 into shared memory
   for (int idx = tid; idx < NB * NB; idx += NT) {
     const int i = idx / NB, c = idx % NB;
-    L11[i][c] = (i == c) ? 1.0 : 0.0;
+    L11[i][c] = (i == c) ? T(1) : T(0);
   }
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
     if (valid[q]) {
-      double* row = dst + (int64_t)(k0 + pos[q]) * n + k0;
+      T* row = dst + (int64_t)(k0 + pos[q]) * n + k0;
 #pragma unroll 32
       for (int c = 0; c < NB; ++c)
         if (c < kb) row[c] = a[q][c];
@@ -275,7 +299,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
   if (warp == 0) {
 #pragma unroll 1
     for (int i = 0; i < NB; ++i) {
-      double p0 = (i == lane) ? 1.0 : 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
+      T p0 = (i == lane) ? T(1) : T(0), p1 = T(0), p2 = T(0), p3 = T(0);
       int q = 0;
 #pragma unroll 1
       for (; q + 3 < i; q += 4) {
@@ -286,7 +310,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
       }
 #pragma unroll 1
       for (; q < i; ++q) p0 = fma(-L11[i][q], Xinv[q][lane], p0);
-      const double x = (p0 + p1) + (p2 + p3);
+      const T x = (p0 + p1) + (p2 + p3);
       Xinv[i][lane] = x;
       sc->linv[i * NB + lane] = x;
     }
@@ -294,7 +318,7 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
 
   // det / slogdet: pivots folded in the reference's order (linalg.cpp:400-403, 425-431)
   if (warp == (NW > 1 ? 1 : 0)) {
-    const double lg = lane < kb ? log(fabs(pvals[lane])) : 0.0;
+    const double lg = lane < kb ? log(fabs((double)pvals[lane])) : 0.0;
     const int ns = nswap;  // every thread counted the same exchanges
     double det = sc->det, la = sc->logabs, sg = sc->sign;
     if (ns & 1) { det = -det; sg = -sg; }
@@ -320,23 +344,27 @@ k_panel(StepArgs sa, const int32_t* __restrict__ list, int k0) {
 
 // ---------------------------------------------------------------------------
 // Shared helpers for the 64-column strip kernels.
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool pred) {
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool pred) {
   const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(pred ? 8 : 0));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(BYTES),
+               "r"(pred ? BYTES : 0));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+template <class T>
 struct Seg {
-  double* dst;         // where the strip lives
-  const double* src;   // where it is read from (== dst after step 0)
+  T* dst;         // where the strip lives
+  const T* src;   // where it is read from (== dst after step 0)
   int ld;
-  bool ident;          // source is the identity (inverse at step 0)
+  bool ident;     // source is the identity (inverse at step 0)
 };
 
-__device__ inline Seg segment(const StepArgs& sa, const SysDesc& d, int kind, int k0) {
-  Seg s;
+template <class T>
+__device__ inline Seg<T> segment(const StepArgsT<T>& sa, const SysDesc& d, int kind, int k0) {
+  Seg<T> s;
   if (kind == kSegMatrix || kind == kSegLeft) {
     s.dst = sa.LU + d.lu_off;
     s.src = (k0 == 0 && sa.A) ? sa.A + d.a_off : s.dst;
@@ -356,82 +384,175 @@ __device__ inline Seg segment(const StepArgs& sa, const SysDesc& d, int kind, in
   return s;
 }
 
-__device__ __forceinline__ double seg_load(const Seg& s, int row, int col) {
-  return s.ident ? (row == col ? 1.0 : 0.0) : s.src[(int64_t)row * s.ld + col];
+template <class T>
+__device__ __forceinline__ T seg_load(const Seg<T>& s, int row, int col) {
+  return s.ident ? (row == col ? T(1) : T(0)) : s.src[(int64_t)row * s.ld + col];
 }
 
-// C[rows r0.., 64 cols] -= A[rows r0.., 32] * Bs[32][64] for rows [r0, rend), one
-// 64x64 tile per call, 4 warps in 2x2. As holds the A rows (64 x LS), Bs the
-// 32 x 64 right operand (WS stride). `crow(r, cc)` reads the input value of row
-// r, column cc; `cstore(r, cc, v)` writes it.
-template <class Load, class Store>
-__device__ __forceinline__ void tile_update(const double* As, const double* Bs, int r0, int rend,
-                                            int w, Load cload, Store cstore) {
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int g = lane >> 2, tq = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  double acc[4][4][2];
-#pragma unroll
-  for (int mi = 0; mi < 4; ++mi) {
-    const int r = r0 + wm + mi * 8 + g;
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
-#pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int cc = wn + ni * 8 + 2 * tq + e;
-        acc[mi][ni][e] = (r < rend && cc < w) ? cload(r, cc) : 0.0;
-      }
-    }
-  }
-#pragma unroll
-  for (int kk = 0; kk < NB; kk += 4) {
-    double af[4], bf[4];
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi) af[mi] = -As[(wm + mi * 8 + g) * LS + kk + tq];
-#pragma unroll
-    for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * WS + wn + ni * 8 + g];
+// A 64 x 64 accumulator tile spread over the 128 threads of a strip kernel.
+// each(f) visits (row, column, value&) of the thread's elements;
+// sub_mma(As, Bs) does tile -= As(64 x 32, stride LS) * Bs(32 x 64, stride WS).
+template <class T> struct Acc64;
+
+template <> struct Acc64<double> {  // 2 x 2 warps of 32 x 32, DMMA fragments
+  double v[4][4][2];
+  template <class F>
+  __device__ __forceinline__ void each(F&& f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], af[mi], bf[ni]);
+      for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) f(wm + mi * 8 + g, wn + ni * 8 + 2 * tq + e, v[mi][ni][e]);
   }
+  __device__ __forceinline__ void sub_mma(const double* As, const double* Bs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
 #pragma unroll
-  for (int mi = 0; mi < 4; ++mi) {
-    const int r = r0 + wm + mi * 8 + g;
+    for (int kk = 0; kk < NB; kk += 4) {
+      double af[4], bf[4];
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
+      for (int mi = 0; mi < 4; ++mi) af[mi] = -As[(wm + mi * 8 + g) * LS + kk + tq];
 #pragma unroll
-      for (int e = 0; e < 2; ++e) {
-        const int cc = wn + ni * 8 + 2 * tq + e;
-        if (r < rend && cc < w) cstore(r, cc, acc[mi][ni][e]);
-      }
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * WS + wn + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma884(v[mi][ni], af[mi], bf[ni]);
     }
   }
+};
+
+template <> struct Acc64<float> {  // 4 x 8 elements per thread, FP32 FMA
+  float v[4][8];
+  template <class F>
+  __device__ __forceinline__ void each(F&& f) {
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) f(ty * 4 + i, tx * 8 + j, v[i][j]);
+  }
+  __device__ __forceinline__ void sub_mma(const float* As, const float* Bs) {
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;
+#pragma unroll 4
+    for (int k = 0; k < NB; ++k) {
+      float a[4], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[(ty * 4 + i) * LS + k];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) b[j] = Bs[k * WS + tx * 8 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) v[i][j] = fmaf(-a[i], b[j], v[i][j]);
+    }
+  }
+};
+
+// The 32 x 64 tile of U12 = L11^-1 A12 (plain product, no negation).
+template <class T> struct Acc32;
+
+template <> struct Acc32<double> {  // warp w owns columns [16w, 16w+16)
+  double v[4][2][2];
+  template <class F>
+  __device__ __forceinline__ void each(F&& f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) f(mi * 8 + g, warp * 16 + ni * 8 + 2 * tq + e, v[mi][ni][e]);
+  }
+  __device__ __forceinline__ void mma(const double* As, const double* Bs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) v[mi][ni][0] = v[mi][ni][1] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < NB; kk += 4) {
+      double af[4], bf[2];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) af[mi] = As[(mi * 8 + g) * LS + kk + tq];
+#pragma unroll
+      for (int ni = 0; ni < 2; ++ni) bf[ni] = Bs[(kk + tq) * WS + warp * 16 + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) dmma884(v[mi][ni], af[mi], bf[ni]);
+    }
+  }
+};
+
+template <> struct Acc32<float> {  // 4 x 4 elements per thread
+  float v[4][4];
+  template <class F>
+  __device__ __forceinline__ void each(F&& f) {
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) f(ty * 4 + i, tx * 4 + j, v[i][j]);
+  }
+  __device__ __forceinline__ void mma(const float* As, const float* Bs) {
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) v[i][j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < NB; ++k) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[(ty * 4 + i) * LS + k];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k * WS + tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[i][j] = fmaf(a[i], b[j], v[i][j]);
+    }
+  }
+};
+
+// C[rows r0.., 64 cols] -= As * Bs for rows [r0, rend), columns < w, one tile.
+template <class T, class Load, class Store>
+__device__ __forceinline__ void tile_update(const T* As, const T* Bs, int r0, int rend, int w, Load cload,
+                                            Store cstore) {
+  Acc64<T> acc;
+  acc.each([&](int r, int cc, T& x) { x = (r0 + r < rend && cc < w) ? cload(r0 + r, cc) : T(0); });
+  acc.sub_mma(As, Bs);
+  acc.each([&](int r, int cc, T& x) {
+    if (r0 + r < rend && cc < w) cstore(r0 + r, cc, x);
+  });
 }
 
 // ---------------------------------------------------------------------------
 // k_update
-constexpr int UT = 128;
-
+template <class T>
 __global__ void __launch_bounds__(UT)
-k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
-  extern __shared__ __align__(16) double smem[];
-  double* Us = smem;                 // 32 x WS   U12 strip
-  double* D = Us + NB * WS;          // 32 x WS   displaced rows
-  double* T = D + NB * WS;           // 64 x LS   A12 (permuted, 32 x WS), then L21 buffer 1
-  double* As = T + 64 * LS;          // 64 x LS   L11^-1, then L21 buffer 0
+k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Us = reinterpret_cast<T*>(smem_raw);  // 32 x WS   U12 strip
+  T* D = Us + NB * WS;                     // 32 x WS   displaced rows
+  T* Tm = D + NB * WS;                     // 64 x LS   A12 (permuted, 32 x WS), then L21 buffer 1
+  T* As = Tm + 64 * LS;                    // 64 x LS   L11^-1, then L21 buffer 0
   int* tsrc = reinterpret_cast<int*>(As + 64 * LS);
   int* ddst = tsrc + NB;
   int* dsrc = ddst + NB;
-  int* dmap = dsrc + NB;             // m entries: displaced index of each row, or -1
+  int* dmap = dsrc + NB;                   // m entries: displaced index of each row, or -1
 
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, k0, false);
   const SysDesc d = step_desc(sa, it.sys);
-  const StepScratch* sc = sa.scratch + d.pad_;
+  const StepScratchT<T>* sc = sa.scratch + d.pad_;
   if (sc->info) return;
   const int n = d.n, m = n - k0, kb = min(NB, m), w = it.width, c0 = it.c0;
-  const Seg s = segment(sa, d, it.kind, k0);
+  const Seg<T> s = segment(sa, d, it.kind, k0);
   const int nd = sc->ndisp;
 
   if (tid < NB) {
@@ -444,14 +565,14 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
   for (int idx = tid; idx < NB * 64; idx += UT) {
     const int i = idx >> 6, c = idx & 63;
     const bool in = c < w;
-    T[i * WS + c] = (in && i < kb) ? seg_load(s, k0 + tsrc[i], c0 + c) : 0.0;
-    D[i * WS + c] = (in && i < nd) ? seg_load(s, k0 + dsrc[i], c0 + c) : 0.0;
+    Tm[i * WS + c] = (in && i < kb) ? seg_load(s, k0 + tsrc[i], c0 + c) : T(0);
+    D[i * WS + c] = (in && i < nd) ? seg_load(s, k0 + dsrc[i], c0 + c) : T(0);
   }
   if (it.kind == kSegLeft) {
     __syncthreads();
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
-      if (c < w && i < kb) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = T[i * WS + c];
+      if (c < w && i < kb) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = Tm[i * WS + c];
       if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
     }
     return;
@@ -461,79 +582,46 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
   __syncthreads();
   if (tid < nd) dmap[ddst[tid] - kb] = tid;
 
-  // U12 = L11^-1 T (32 x 64): warp w owns columns [16w, 16w+16)
+  // U12 = L11^-1 A12 (32 x 64)
   {
-    const int g = lane >> 2, tq = lane & 3;
-    double acc[4][2][2];
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-      for (int ni = 0; ni < 2; ++ni) acc[mi][ni][0] = acc[mi][ni][1] = 0.0;
-#pragma unroll
-    for (int kk = 0; kk < NB; kk += 4) {
-      double af[4], bf[2];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi) af[mi] = As[(mi * 8 + g) * LS + kk + tq];
-#pragma unroll
-      for (int ni = 0; ni < 2; ++ni) bf[ni] = T[(kk + tq) * WS + warp * 16 + ni * 8 + g];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni) dmma884(acc[mi][ni], af[mi], bf[ni]);
-    }
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      const int i = mi * 8 + g;
-#pragma unroll
-      for (int ni = 0; ni < 2; ++ni) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int c = warp * 16 + ni * 8 + 2 * tq + e;
-          const double v = (i < kb) ? acc[mi][ni][e] : 0.0;
-          Us[i * WS + c] = v;
-          if (i < kb && c < w) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = v;
-        }
-      }
-    }
+    Acc32<T> u;
+    u.mma(As, Tm);
+    u.each([&](int i, int c, T& x) {
+      const T v = (i < kb) ? x : T(0);
+      Us[i * WS + c] = v;
+      if (i < kb && c < w) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = v;
+    });
   }
   __syncthreads();
   if (kb < NB) return;  // last panel: nothing below it
-  // A22 strip -= L21 U12 in 64-row tiles, software-pipelined: while the tensor
-  // pipe works on tile t, tile t+1's L21 rows stream into shared memory
-  // (cp.async) and its accumulator inputs into registers.
-  const double* L = sa.LU + d.lu_off;
-  const int g = lane >> 2, tq = lane & 3;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  // L21 buffers: As (L11^-1 is consumed) and T (A12 is consumed once U12 is in Us)
+  // A22 strip -= L21 U12 in 64-row tiles, software-pipelined: while tile t is
+  // multiplied, tile t+1's L21 rows stream into shared memory (cp.async) and
+  // its accumulator inputs into registers.
+  const T* L = sa.LU + d.lu_off;
+  // L21 buffers: As (L11^-1 is consumed) and Tm (A12 is consumed once U12 is in Us)
   auto prefetch_a = [&](int buf, int r0) {
-    double* dstb = buf ? T : As;
+    T* dstb = buf ? Tm : As;
 #pragma unroll 4
     for (int idx = tid; idx < 64 * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
       const bool ok = r0 + i < n;
-      cp_async8(dstb + i * LS + q, ok ? L + (int64_t)(r0 + i) * n + k0 + q : L, ok);
+      cp_async<sizeof(T)>(dstb + i * LS + q, ok ? L + (int64_t)(r0 + i) * n + k0 + q : L, ok);
     }
     cp_async_commit();
   };
-  auto load_c = [&](double (&c)[4][4][2], int r0) {
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      const int r = r0 + wm + mi * 8 + g;
-      const int dm = r < n ? dmap[r - k0 - kb] : -1;
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int cc = wn + ni * 8 + 2 * tq + e;
-          double v = 0.0;
-          if (r < n && cc < w) v = dm >= 0 ? D[dm * WS + cc] : seg_load(s, r, c0 + cc);
-          c[mi][ni][e] = v;
-        }
+  auto load_c = [&](Acc64<T>& c, int r0) {
+    c.each([&](int rr, int cc, T& x) {
+      const int r = r0 + rr;
+      T v = T(0);
+      if (r < n && cc < w) {
+        const int dm = dmap[r - k0 - kb];
+        v = dm >= 0 ? D[dm * WS + cc] : seg_load(s, r, c0 + cc);
       }
-    }
+      x = v;
+    });
   };
   const int r_first = k0 + NB;
-  double cur[4][4][2], nxt[4][4][2];
+  Acc64<T> cur, nxt;
   prefetch_a(0, r_first);
   load_c(cur, r_first);
   int buf = 0;
@@ -547,40 +635,12 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
       cp_async_wait<0>();
     }
     __syncthreads();
-    const double* Ab = buf ? T : As;
-#pragma unroll
-    for (int kk = 0; kk < NB; kk += 4) {
-      double af[4], bf[4];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi) af[mi] = -Ab[(wm + mi * 8 + g) * LS + kk + tq];
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = Us[(kk + tq) * WS + wn + ni * 8 + g];
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) dmma884(cur[mi][ni], af[mi], bf[ni]);
-    }
-#pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      const int r = r0 + wm + mi * 8 + g;
-#pragma unroll
-      for (int ni = 0; ni < 4; ++ni) {
-#pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int cc = wn + ni * 8 + 2 * tq + e;
-          if (r < n && cc < w) s.dst[(int64_t)r * s.ld + c0 + cc] = cur[mi][ni][e];
-        }
-      }
-    }
-    if (more) {
-#pragma unroll
-      for (int mi = 0; mi < 4; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-          cur[mi][ni][0] = nxt[mi][ni][0];
-          cur[mi][ni][1] = nxt[mi][ni][1];
-        }
-    }
+    cur.sub_mma(buf ? Tm : As, Us);
+    cur.each([&](int rr, int cc, T& x) {
+      const int r = r0 + rr;
+      if (r < n && cc < w) s.dst[(int64_t)r * s.ld + c0 + cc] = x;
+    });
+    if (more) cur = nxt;
     buf ^= 1;
     __syncthreads();  // buffer `buf` is refilled by the next iteration's prefetch
   }
@@ -588,33 +648,34 @@ k_update(StepArgs sa, const StepItem* __restrict__ items, int k0) {
 
 // ---------------------------------------------------------------------------
 // k_back: X = U^-1 Y on a 64-column strip, blocks from the bottom.
+template <class T>
 __global__ void __launch_bounds__(UT)
-k_back(StepArgs sa, const StepItem* __restrict__ items) {
-  __shared__ double Ub[NB * LS];
-  __shared__ double Xb[NB * WS];
-  __shared__ double As[64 * LS];
+k_back(StepArgsT<T> sa, const StepItem* __restrict__ items) {
+  __shared__ T Ub[NB * LS];
+  __shared__ T Xb[NB * WS];
+  __shared__ T As[64 * LS];
   const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
   if (!sa.solve_only && sa.scratch[d.pad_].info) return;
   const int n = d.n, w = it.width, c0 = it.c0;
-  const double* U = sa.LU + d.lu_off;
-  double* X = (it.kind == kSegRhs) ? sa.X + d.b_off : sa.inv + d.inv_off;
+  const T* U = sa.LU + d.lu_off;
+  T* X = (it.kind == kSegRhs) ? sa.X + d.b_off : sa.inv + d.inv_off;
   const int ld = (it.kind == kSegRhs) ? d.nrhs : n;
   for (int kb0 = ((n - 1) / NB) * NB; kb0 >= 0; kb0 -= NB) {
     const int bw = min(NB, n - kb0);
     for (int idx = tid; idx < NB * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
-      Ub[i * LS + q] = (i < bw && q < bw) ? U[(int64_t)(kb0 + i) * n + kb0 + q] : 0.0;
+      Ub[i * LS + q] = (i < bw && q < bw) ? U[(int64_t)(kb0 + i) * n + kb0 + q] : T(0);
     }
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
-      Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : 0.0;
+      Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : T(0);
     }
     __syncthreads();
     if (tid < w) {
       for (int i = bw - 1; i >= 0; --i) {
-        double x = Xb[i * WS + tid];
+        T x = Xb[i * WS + tid];
         for (int q = i + 1; q < bw; ++q) x = fma(-Ub[i * LS + q], Xb[q * WS + tid], x);
         Xb[i * WS + tid] = x / Ub[i * LS + i];
       }
@@ -627,12 +688,12 @@ k_back(StepArgs sa, const StepItem* __restrict__ items) {
     for (int r0 = 0; r0 < kb0; r0 += 64) {
       for (int idx = tid; idx < 64 * NB; idx += UT) {
         const int i = idx >> 5, q = idx & 31;
-        As[i * LS + q] = (r0 + i < kb0 && q < bw) ? U[(int64_t)(r0 + i) * n + kb0 + q] : 0.0;
+        As[i * LS + q] = (r0 + i < kb0 && q < bw) ? U[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
       }
       __syncthreads();
-      tile_update(
+      tile_update<T>(
           As, Xb, r0, kb0, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
-          [&](int r, int cc, double v) { X[(int64_t)r * ld + c0 + cc] = v; });
+          [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
       __syncthreads();
     }
   }
@@ -641,21 +702,22 @@ k_back(StepArgs sa, const StepItem* __restrict__ items) {
 // ---------------------------------------------------------------------------
 // k_forward: getrs from stored factors, X[p] = B[perm[p]] then unit-lower
 // substitution, blocks from the top. X must not alias B.
+template <class T>
 __global__ void __launch_bounds__(UT)
-k_forward(StepArgs sa, const StepItem* __restrict__ items) {
-  extern __shared__ __align__(16) double fsm[];
-  double* Lb = fsm;              // 32 x LS
-  double* Xb = Lb + NB * LS;     // 32 x WS
-  double* As = Xb + NB * WS;     // 64 x LS
+k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items) {
+  extern __shared__ __align__(16) unsigned char fsm_raw[];
+  T* Lb = reinterpret_cast<T*>(fsm_raw);  // 32 x LS
+  T* Xb = Lb + NB * LS;                   // 32 x WS
+  T* As = Xb + NB * WS;                   // 64 x LS
   int* perm = reinterpret_cast<int*>(As + 64 * LS);
   const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
   const int n = d.n, w = it.width, c0 = it.c0, ld = d.nrhs;
-  const double* L = sa.LU + d.lu_off;
+  const T* L = sa.LU + d.lu_off;
   const int32_t* ipiv = sa.ipiv + d.piv_off;
-  const double* B = sa.B + d.b_off;
-  double* X = sa.X + d.b_off;
+  const T* B = sa.B + d.b_off;
+  T* X = sa.X + d.b_off;
   if (tid == 0) {
     for (int i = 0; i < n; ++i) perm[i] = i;
     for (int k = 0; k < n; ++k) {
@@ -674,16 +736,16 @@ k_forward(StepArgs sa, const StepItem* __restrict__ items) {
     const int bw = min(NB, n - kb0), kb1 = kb0 + bw;
     for (int idx = tid; idx < NB * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
-      Lb[i * LS + q] = (i < bw && q < bw) ? L[(int64_t)(kb0 + i) * n + kb0 + q] : 0.0;
+      Lb[i * LS + q] = (i < bw && q < bw) ? L[(int64_t)(kb0 + i) * n + kb0 + q] : T(0);
     }
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
-      Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : 0.0;
+      Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : T(0);
     }
     __syncthreads();
     if (tid < w) {
       for (int i = 1; i < bw; ++i) {
-        double x = Xb[i * WS + tid];
+        T x = Xb[i * WS + tid];
         for (int q = 0; q < i; ++q) x = fma(-Lb[i * LS + q], Xb[q * WS + tid], x);
         Xb[i * WS + tid] = x;
       }
@@ -696,63 +758,85 @@ k_forward(StepArgs sa, const StepItem* __restrict__ items) {
     for (int r0 = kb1; r0 < n; r0 += 64) {
       for (int idx = tid; idx < 64 * NB; idx += UT) {
         const int i = idx >> 5, q = idx & 31;
-        As[i * LS + q] = (r0 + i < n && q < bw) ? L[(int64_t)(r0 + i) * n + kb0 + q] : 0.0;
+        As[i * LS + q] = (r0 + i < n && q < bw) ? L[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
       }
       __syncthreads();
-      tile_update(
+      tile_update<T>(
           As, Xb, r0, n, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
-          [&](int r, int cc, double v) { X[(int64_t)r * ld + c0 + cc] = v; });
+          [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
       __syncthreads();
     }
   }
 }
 
+template <class T>
 size_t update_smem(int nmax) {
-  return sizeof(double) * (2 * NB * WS + 2 * 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
+  return sizeof(T) * (2 * NB * WS + 2 * 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
 }
+template <class T>
 size_t forward_smem(int nmax) {
-  return sizeof(double) * (NB * LS + NB * WS + 64 * LS) + sizeof(int) * (size_t)nmax;
+  return sizeof(T) * (NB * LS + NB * WS + 64 * LS) + sizeof(int) * (size_t)nmax;
+}
+
+template <class T>
+cudaError_t prepare_t() {
+  cudaError_t e = cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)update_smem<T>(kStepMaxN));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)forward_smem<T>(kStepMaxN));
 }
 
 }  // namespace
 
 cudaError_t step_prepare() {
-  cudaError_t e = cudaFuncSetAttribute(k_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)update_smem(kStepMaxN));
+  cudaError_t e = prepare_t<double>();
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_forward, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)forward_smem(kStepMaxN));
+  return prepare_t<float>();
 }
 
-cudaError_t launch_panel(const StepArgs& sa, const int32_t* list, int nsys, int mmax, int k0,
+template <class T>
+cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st) {
   if (nsys <= 0) return cudaSuccess;
-  if (mmax <= 64) k_panel<64, 1><<<nsys, 64, 0, st>>>(sa, list, k0);
-  else if (mmax <= 128) k_panel<128, 1><<<nsys, 128, 0, st>>>(sa, list, k0);
-  else if (mmax <= 256) k_panel<256, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
-  else if (mmax <= 512) k_panel<256, 2><<<nsys, 256, 0, st>>>(sa, list, k0);
+  if (mmax <= 64) k_panel<T, 64, 1><<<nsys, 64, 0, st>>>(sa, list, k0);
+  else if (mmax <= 128) k_panel<T, 128, 1><<<nsys, 128, 0, st>>>(sa, list, k0);
+  else if (mmax <= 256) k_panel<T, 256, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
+  else if (mmax <= 512) k_panel<T, 256, 2><<<nsys, 256, 0, st>>>(sa, list, k0);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 
-cudaError_t launch_update(const StepArgs& sa, const StepItem* items, int nitems, int nmax, int k0,
+template <class T>
+cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_update<<<nitems, UT, update_smem(nmax), st>>>(sa, items, k0);
+  k_update<T><<<nitems, UT, update_smem<T>(nmax), st>>>(sa, items, k0);
   return cudaGetLastError();
 }
 
-cudaError_t launch_back(const StepArgs& sa, const StepItem* items, int nitems, cudaStream_t st) {
+template <class T>
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_back<<<nitems, UT, 0, st>>>(sa, items);
+  k_back<T><<<nitems, UT, 0, st>>>(sa, items);
   return cudaGetLastError();
 }
 
-cudaError_t launch_forward(const StepArgs& sa, const StepItem* items, int nitems, int nmax,
+template <class T>
+cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
                            cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_forward<<<nitems, UT, forward_smem(nmax), st>>>(sa, items);
+  k_forward<T><<<nitems, UT, forward_smem<T>(nmax), st>>>(sa, items);
   return cudaGetLastError();
 }
+
+#define NPPB_STEP_INSTANTIATE(T)                                                                          \
+  template cudaError_t launch_panel<T>(const StepArgsT<T>&, const int32_t*, int, int, int, cudaStream_t);     \
+  template cudaError_t launch_update<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);   \
+  template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, cudaStream_t);               \
+  template cudaError_t launch_forward<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);
+NPPB_STEP_INSTANTIATE(double)
+NPPB_STEP_INSTANTIATE(float)
+#undef NPPB_STEP_INSTANTIATE
 
 }  // namespace nppb

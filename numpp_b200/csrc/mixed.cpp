@@ -1,0 +1,246 @@
+// Mixed-precision batched solve: FP32 factors, FP64 iterative refinement. C++20.
+//
+// No counterpart in the reference (NumPP solves in double only,
+// src/linalg/linalg.cpp:92-103). For a uniform batch of order n:
+//  1. equilibrate: power-of-two row/column scales, the scaled matrix in FP32;
+//  2. factor in FP32 on the step-wise kernels (pivots and row moves kept),
+//     the first solution riding along as augmented columns;
+//  3. refine in FP64: R = B - A X, eta = normwise backward error; systems with
+//     eta <= tol stop, systems whose eta no longer halves are marked stalled;
+//     the others solve A d = R with the FP32 factors and add d in FP64;
+//  4. every system that did not converge (stalled, FP32 zero pivot, or out of
+//     iterations) is refactored and solved in FP64;
+//  5. report per system: eta, forward error when X_true is given, corrections
+//     applied, and whether the FP64 fallback ran.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/numpp_b200.h"
+#include "mixed.hpp"
+#include "runtime.hpp"
+
+using namespace nppb;
+
+namespace {
+
+#define NPPB_CUDA(call, what)                            \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_status(e_, what); \
+  } while (0)
+#define NPPB_RC(expr)               \
+  do {                              \
+    int rc_ = (expr);               \
+    if (rc_ != NPPB_OK) return rc_; \
+  } while (0)
+
+int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const double* dB, double* dX,
+          const double* dXtrue, double tol, int32_t max_iter, int flags, int32_t* dinfo, double* dBerr,
+          double* dFerr, int32_t* dIters, int32_t* dFallback, cudaStream_t st) {
+  if (count64 < 0 || n < 0 || nrhs < 0 || max_iter < 0 || !(tol >= 0.0)) {
+    set_error("negative count, order, nrhs or max_iter, or bad tolerance");
+    return NPPB_E_ARG;
+  }
+  if (n > kMixedMaxN || count64 > INT32_MAX) {
+    set_error("order above 512 or count above 2^31-1");
+    return NPPB_E_RANGE;
+  }
+  if (count64 == 0 || n == 0 || nrhs == 0) return NPPB_OK;
+  if (!dA || !dB || !dX) {
+    set_error("A, B and X are required");
+    return NPPB_E_ARG;
+  }
+  if (!device()) return NPPB_E_NODEV;
+  const int count = (int)count64;
+  const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs, c = (size_t)count;
+  DevMem a32, piv, sc32, b32, y32, rsm, csm, stm, info32, act;
+  NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
+  NPPB_CUDA(piv.alloc(sizeof(int32_t) * c * n, st), "workspace");
+  NPPB_CUDA(sc32.alloc(sizeof(StepScratchT<float>) * c, st), "workspace");
+  NPPB_CUDA(b32.alloc(sizeof(float) * c * nb, st), "workspace");
+  NPPB_CUDA(y32.alloc(sizeof(float) * c * nb, st), "workspace");
+  NPPB_CUDA(rsm.alloc(sizeof(double) * c * n, st), "workspace");
+  NPPB_CUDA(csm.alloc(sizeof(double) * c * n, st), "workspace");
+  NPPB_CUDA(stm.alloc(sizeof(RefineState) * c, st), "workspace");
+  NPPB_CUDA(info32.alloc(sizeof(int32_t) * c, st), "workspace");
+  NPPB_CUDA(act.alloc(sizeof(int), st), "workspace");
+  RefineState* S = stm.as<RefineState>();
+  const bool equil = !(flags & NPPB_MIXED_NO_EQUILIBRATE);
+  NPPB_CUDA(mixed_equilibrate(dA, count, n, equil ? 1 : 0, a32.as<float>(), rsm.as<double>(), csm.as<double>(), S,
+                              st),
+            "equilibrate");
+  NPPB_CUDA(mixed_scale_rhs(dB, count, n, nrhs, rsm.as<double>(), b32.as<float>(), S, st), "scale rhs");
+
+  std::vector<RefineState> hs(c);
+  std::vector<int32_t> fallback(c, 0);
+  bool any_fallback = false;
+  if (n > 32) {
+    StepArgsT<float> sa{};
+    sa.scratch = sc32.as<StepScratchT<float>>();
+    sa.A = nullptr;  // factor the scaled FP32 matrix in place
+    sa.LU = a32.as<float>();
+    sa.ipiv = piv.as<int32_t>();
+    sa.B = b32.as<float>();
+    sa.X = y32.as<float>();
+    sa.info = info32.as<int32_t>();
+    sa.un = n;
+    sa.unrhs = nrhs;
+    sa.uleft = 1;
+    NPPB_CUDA(run_step_uniform<float>(sa, count, st), "FP32 factorisation");
+    NPPB_CUDA(mixed_mark_fp32_failures(info32.as<int32_t>(), S, count, st), "mark");
+    NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 1, st), "apply");
+    int h_act = 0;
+    for (int it = 0;; ++it) {
+      NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
+      NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), S, tol, it, 1,
+                               act.as<int>(), st),
+                "residual");
+      NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
+      NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+      if (h_act == 0 || it >= max_iter) break;
+      StepArgsT<float> sb = sa;  // correction: solve with the stored FP32 factors
+      sb.B = b32.as<float>();
+      sb.X = y32.as<float>();
+      NPPB_CUDA(run_step_solve_uniform<float>(sb, count, st), "FP32 correction solve");
+      NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 0, st), "apply");
+    }
+    NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
+    NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+    for (size_t s = 0; s < c; ++s) {
+      if (hs[s].status != kRefineConverged && !(flags & NPPB_MIXED_NO_FALLBACK)) {
+        fallback[s] = 1;
+        any_fallback = true;
+      }
+    }
+  } else {
+    // orders <= 32 are one warp-resident FP64 solve already: no refinement to gain
+    std::fill(fallback.begin(), fallback.end(), 1);
+    any_fallback = true;
+  }
+
+  std::vector<int32_t> hinfo(c, 0);
+  if (any_fallback) {
+    std::vector<int> idx;
+    for (size_t s = 0; s < c; ++s)
+      if (fallback[s]) idx.push_back((int)s);
+    const size_t k = idx.size();
+    DevMem ca, cb, cx, ci;
+    NPPB_CUDA(ca.alloc(sizeof(double) * k * nn, st), "fallback workspace");
+    NPPB_CUDA(cb.alloc(sizeof(double) * k * nb, st), "fallback workspace");
+    NPPB_CUDA(cx.alloc(sizeof(double) * k * nb, st), "fallback workspace");
+    NPPB_CUDA(ci.alloc(sizeof(int32_t) * k, st), "fallback workspace");
+    for (size_t q = 0; q < k; ++q) {
+      const size_t s = idx[q];
+      NPPB_CUDA(cudaMemcpyAsync(ca.as<double>() + q * nn, dA + s * nn, sizeof(double) * nn, cudaMemcpyDeviceToDevice, st),
+                "gather");
+      NPPB_CUDA(cudaMemcpyAsync(cb.as<double>() + q * nb, dB + s * nb, sizeof(double) * nb, cudaMemcpyDeviceToDevice, st),
+                "gather");
+    }
+    NPPB_RC(nppb_d_linalg_batched((int64_t)k, n, nrhs, NPPB_WANT_SOLVE, ca.as<double>(), cb.as<double>(),
+                                  cx.as<double>(), nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                  ci.as<int32_t>(), st));
+    for (size_t q = 0; q < k; ++q) {
+      const size_t s = idx[q];
+      NPPB_CUDA(cudaMemcpyAsync(dX + s * nb, cx.as<double>() + q * nb, sizeof(double) * nb, cudaMemcpyDeviceToDevice, st),
+                "scatter");
+    }
+    std::vector<int32_t> cinfo(k);
+    if (k) NPPB_CUDA(cudaMemcpyAsync(cinfo.data(), ci.as<int32_t>(), sizeof(int32_t) * k, cudaMemcpyDeviceToHost, st),
+                     "readback");
+    NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+    for (size_t q = 0; q < k; ++q) hinfo[idx[q]] = cinfo[q];
+  }
+  // final backward error of every system, whatever path produced it
+  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, S, tol, 0, 0, act.as<int>(), st),
+            "residual");
+  if (dFerr && dXtrue) NPPB_CUDA(mixed_ferr(dX, dXtrue, count, n, nrhs, dFerr, st), "forward error");
+  NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
+  NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+  std::vector<double> berr(c);
+  std::vector<int32_t> iters(c);
+  for (size_t s = 0; s < c; ++s) {
+    berr[s] = hs[s].eta;
+    iters[s] = n > 32 ? hs[s].iters : 0;
+  }
+  if (dBerr) NPPB_CUDA(cudaMemcpyAsync(dBerr, berr.data(), sizeof(double) * c, cudaMemcpyHostToDevice, st), "write");
+  if (dIters) NPPB_CUDA(cudaMemcpyAsync(dIters, iters.data(), sizeof(int32_t) * c, cudaMemcpyHostToDevice, st), "write");
+  if (dFallback)
+    NPPB_CUDA(cudaMemcpyAsync(dFallback, fallback.data(), sizeof(int32_t) * c, cudaMemcpyHostToDevice, st), "write");
+  if (dinfo) NPPB_CUDA(cudaMemcpyAsync(dinfo, hinfo.data(), sizeof(int32_t) * c, cudaMemcpyHostToDevice, st), "write");
+  NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+  return NPPB_OK;
+}
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    clear_error();
+    return f();
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return NPPB_E_NOMEM;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA, const double* dB,
+                               double* dX, const double* dXtrue, double tol, int32_t max_iter, int flags,
+                               int32_t* dinfo, double* dBerr, double* dFerr, int32_t* dIters,
+                               int32_t* dFallback, void* stream) {
+  return guarded([&]() -> int {
+    return mixed(count, n, nrhs, dA, dB, dX, dXtrue, tol, max_iter, flags, dinfo, dBerr, dFerr, dIters,
+                 dFallback, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int nppb_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* A, const double* B, double* X,
+                             const double* Xtrue, double tol, int32_t max_iter, int flags, int32_t* info,
+                             double* berr, double* ferr, int32_t* iters, int32_t* fallback) {
+  return guarded([&]() -> int {
+    if (count <= 0 || n <= 0 || nrhs <= 0) {
+      if (count < 0 || n < 0 || nrhs < 0) {
+        set_error("negative count, order or nrhs");
+        return NPPB_E_ARG;
+      }
+      return NPPB_OK;
+    }
+    if (!device()) return NPPB_E_NODEV;
+    cudaStream_t st = thread_stream();
+    const size_t nn = (size_t)count * n * n, nb = (size_t)count * n * nrhs, c = (size_t)count;
+    DevMem dA, dB, dX, dT, dI, dBe, dFe, dIt, dFb;
+    NPPB_CUDA(dA.alloc(sizeof(double) * nn, st), "allocation");
+    NPPB_CUDA(dB.alloc(sizeof(double) * nb, st), "allocation");
+    NPPB_CUDA(dX.alloc(sizeof(double) * nb, st), "allocation");
+    NPPB_CUDA(dI.alloc(sizeof(int32_t) * c, st), "allocation");
+    NPPB_CUDA(dBe.alloc(sizeof(double) * c, st), "allocation");
+    NPPB_CUDA(dFe.alloc(sizeof(double) * c, st), "allocation");
+    NPPB_CUDA(dIt.alloc(sizeof(int32_t) * c, st), "allocation");
+    NPPB_CUDA(dFb.alloc(sizeof(int32_t) * c, st), "allocation");
+    if (Xtrue) NPPB_CUDA(dT.alloc(sizeof(double) * nb, st), "allocation");
+    NPPB_CUDA(cudaMemcpyAsync(dA.as<double>(), A, sizeof(double) * nn, cudaMemcpyHostToDevice, st), "copy");
+    NPPB_CUDA(cudaMemcpyAsync(dB.as<double>(), B, sizeof(double) * nb, cudaMemcpyHostToDevice, st), "copy");
+    if (Xtrue) NPPB_CUDA(cudaMemcpyAsync(dT.as<double>(), Xtrue, sizeof(double) * nb, cudaMemcpyHostToDevice, st), "copy");
+    NPPB_RC(mixed(count, n, nrhs, dA.as<double>(), dB.as<double>(), dX.as<double>(), Xtrue ? dT.as<double>() : nullptr,
+                  tol, max_iter, flags, dI.as<int32_t>(), dBe.as<double>(), dFe.as<double>(), dIt.as<int32_t>(),
+                  dFb.as<int32_t>(), st));
+    NPPB_CUDA(cudaMemcpyAsync(X, dX.as<double>(), sizeof(double) * nb, cudaMemcpyDeviceToHost, st), "copy");
+    if (info) NPPB_CUDA(cudaMemcpyAsync(info, dI.as<int32_t>(), sizeof(int32_t) * c, cudaMemcpyDeviceToHost, st), "copy");
+    if (berr) NPPB_CUDA(cudaMemcpyAsync(berr, dBe.as<double>(), sizeof(double) * c, cudaMemcpyDeviceToHost, st), "copy");
+    if (ferr && Xtrue)
+      NPPB_CUDA(cudaMemcpyAsync(ferr, dFe.as<double>(), sizeof(double) * c, cudaMemcpyDeviceToHost, st), "copy");
+    if (iters) NPPB_CUDA(cudaMemcpyAsync(iters, dIt.as<int32_t>(), sizeof(int32_t) * c, cudaMemcpyDeviceToHost, st), "copy");
+    if (fallback)
+      NPPB_CUDA(cudaMemcpyAsync(fallback, dFb.as<int32_t>(), sizeof(int32_t) * c, cudaMemcpyDeviceToHost, st), "copy");
+    NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+    return NPPB_OK;
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,38 @@
+// Mixed-precision solve: shared declarations of k_mixed.cu and mixed.cpp.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace nppb {
+
+constexpr int kMixedMaxN = 512;
+
+enum : int { kRefineActive = 0, kRefineConverged = 1, kRefineStalled = 2 };
+
+// Per-system refinement state (device).
+struct RefineState {
+  double anorm;  // ||A||_inf
+  double bnorm;  // max |B|
+  double eta;    // last normwise backward error
+  double prev;   // eta of the previous iteration
+  int status;    // kRefine*
+  int iters;     // corrections applied
+};
+
+cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, float* A32, double* rs,
+                              double* cs, RefineState* st, cudaStream_t s);
+cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,
+                            RefineState* st, cudaStream_t s);
+cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, int n, int nrhs,
+                        const RefineState* st, int init, cudaStream_t s);
+// decide = 1: update status / iters and count the still-active systems into *active.
+cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
+                           const double* rs, float* R32, RefineState* st, double tol, int iter, int decide,
+                           int* active, cudaStream_t s);
+cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,
+                       cudaStream_t s);
+cudaError_t mixed_mark_fp32_failures(const int32_t* info32, RefineState* st, int count, cudaStream_t s);
+
+}  // namespace nppb

@@ -13,9 +13,10 @@ constexpr int kStepNB = 32;     // panel width
 constexpr int kStepMaxN = 512;  // largest order the register panel holds (2 rows x 256 threads)
 
 // Per-system state carried from one step to the next (one slot per system,
-// SysDesc::pad_ is the slot index).
-struct StepScratch {
-  double linv[kStepNB * kStepNB];  // L11^-1 of the current panel, row-major
+// SysDesc::pad_ is the slot index). T is the factor precision.
+template <class T>
+struct StepScratchT {
+  T linv[kStepNB * kStepNB];       // L11^-1 of the current panel, row-major
   int top_src[kStepNB];            // panel-relative source row of each top position
   int disp_dst[kStepNB];           // displaced old top rows: their new positions
   int disp_src[kStepNB];           //   ... and their old positions
@@ -25,6 +26,7 @@ struct StepScratch {
   int pad_;
   double det, logabs, sign;        // running det / log|det| / sign
 };
+using StepScratch = StepScratchT<double>;
 
 // Strip kinds.
 enum : int16_t { kSegMatrix = 0, kSegRhs = 1, kSegInv = 2, kSegLeft = 3 };
@@ -38,15 +40,16 @@ struct StepItem {
   int32_t pad_;
 };
 
-struct StepArgs {
+template <class T>
+struct StepArgsT {
   const SysDesc* desc;
-  StepScratch* scratch;
-  const double* A;   // step-0 source of the matrices (nullptr: factor LU in place)
-  double* LU;
+  StepScratchT<T>* scratch;
+  const T* A;        // step-0 source of the matrices (nullptr: factor LU in place)
+  T* LU;
   int32_t* ipiv;
-  const double* B;
-  double* X;
-  double* inv;
+  const T* B;
+  T* X;
+  T* inv;
   double* det;
   double* sign;
   double* logabs;
@@ -56,13 +59,16 @@ struct StepArgs {
   // sides, A / LU / inverse at s*un*un, B / X at s*un*unrhs, ipiv at s*un,
   // scratch slot s; an inverse for every system when uinv != 0.
   int un, unrhs, uinv;
+  int uleft;         // uniform batch keeps its factors: carry row moves left of each panel
 };
+using StepArgs = StepArgsT<double>;
 
 // Work items of a uniform batch at step k0 (k_update) and of its back
 // substitution, per system; grids are count times these.
-__host__ __device__ inline int uniform_update_strips(int n, int nrhs, int inv, int k0) {
+__host__ __device__ inline int uniform_update_strips(int n, int nrhs, int inv, int k0, int left = 0) {
   const int trail = n - k0 - kStepNB;
-  return (trail > 0 ? (trail + 63) / 64 : 0) + (nrhs + 63) / 64 + (inv ? (n + 63) / 64 : 0);
+  return (trail > 0 ? (trail + 63) / 64 : 0) + (nrhs + 63) / 64 + (inv ? (n + 63) / 64 : 0) +
+         (left ? (k0 + 63) / 64 : 0);
 }
 __host__ __device__ inline int uniform_back_strips(int n, int nrhs, int inv) {
   return (nrhs + 63) / 64 + (inv ? (n + 63) / 64 : 0);
@@ -72,13 +78,18 @@ cudaError_t step_prepare();
 // Panel of every listed system at column k0; mmax = largest n - k0 among them.
 // list == nullptr: systems 0..nsys-1 of a uniform batch. Likewise items ==
 // nullptr below means the uniform-batch items, derived from the block index.
-cudaError_t launch_panel(const StepArgs& sa, const int32_t* list, int nsys, int mmax, int k0,
+// T = double (FP64 DMMA updates) or float (FP32 factors for the mixed path).
+template <class T>
+cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st);
 // Row moves + U12 + trailing update for each strip item of step k0 (nmax >= n of any item).
-cudaError_t launch_update(const StepArgs& sa, const StepItem* items, int nitems, int nmax, int k0,
+template <class T>
+cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st);
-cudaError_t launch_back(const StepArgs& sa, const StepItem* items, int nitems, cudaStream_t st);
-cudaError_t launch_forward(const StepArgs& sa, const StepItem* items, int nitems, int nmax,
+template <class T>
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, cudaStream_t st);
+template <class T>
+cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
                            cudaStream_t st);
 
 }  // namespace nppb

@@ -105,13 +105,14 @@ void DevMem::release() {
 
 cudaError_t prepare_kernels() { return step_prepare(); }
 
-cudaError_t run_step_uniform(const StepArgs& sa, int count, cudaStream_t st) {
+template <class T>
+cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st) {
   const int n = sa.un;
   if (n <= 32 || n > kStepMaxN || count <= 0) return cudaErrorInvalidValue;
   for (int k0 = 0; k0 < n; k0 += kStepNB) {
     cudaError_t e = launch_panel(sa, nullptr, count, n - k0, k0, st);
     if (e != cudaSuccess) return e;
-    const int64_t items = (int64_t)count * uniform_update_strips(n, sa.unrhs, sa.uinv, k0);
+    const int64_t items = (int64_t)count * uniform_update_strips(n, sa.unrhs, sa.uinv, k0, sa.uleft);
     if (items > INT32_MAX) return cudaErrorInvalidValue;
     e = launch_update(sa, nullptr, (int)items, n, k0, st);
     if (e != cudaSuccess) return e;
@@ -120,6 +121,22 @@ cudaError_t run_step_uniform(const StepArgs& sa, int count, cudaStream_t st) {
   if (back > INT32_MAX) return cudaErrorInvalidValue;
   return launch_back(sa, nullptr, (int)back, st);
 }
+template cudaError_t run_step_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
+template cudaError_t run_step_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
+
+template <class T>
+cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st) {
+  const int64_t items = (int64_t)count * uniform_back_strips(sa.un, sa.unrhs, 0);
+  if (sa.un <= 32 || items > INT32_MAX || count <= 0) return cudaErrorInvalidValue;
+  StepArgsT<T> s2 = sa;
+  s2.solve_only = 1;
+  s2.uinv = 0;
+  cudaError_t e = launch_forward(s2, nullptr, (int)items, sa.un, st);
+  if (e != cudaSuccess) return e;
+  return launch_back(s2, nullptr, (int)items, st);
+}
+template cudaError_t run_step_solve_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
+template cudaError_t run_step_solve_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
 
 cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
   if (n > 32) return cudaErrorInvalidValue;

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "nppb_internal.hpp"
+#include "nppb_step.hpp"
 
 namespace nppb {
 
@@ -59,7 +60,11 @@ cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t
 // Uniform batch of orders 33..512 on the step-wise kernels (descriptors and
 // work items derived from block indices, no plan). sa carries the pointers,
 // the LU workspace, the per-system scratch and un / unrhs / uinv.
-cudaError_t run_step_uniform(const struct StepArgs& sa, int count, cudaStream_t st);
+template <class T>
+cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st);
+// getrs on a uniform batch from factors (LU, ipiv) a uleft=1 factorisation left: B -> X.
+template <class T>
+cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st);
 
 // One-time kernel attribute setup (dynamic shared memory opt-in), done before
 // any stream capture.

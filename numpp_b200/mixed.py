@@ -1,0 +1,29 @@
+"""Mixed-precision batched solve (FP32 factors, FP64 refinement) on the C ABI."""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .linalg import _check
+
+
+def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equilibrate: bool = True,
+                fallback: bool = True):
+    """X for a (count, n, n) / (count, n, nrhs) float64 batch; returns
+    (X, report) with report = dict(berr, ferr, iters, fallback, info) per system."""
+    L = _lib.load()
+    A = np.ascontiguousarray(A, np.float64)
+    B = np.ascontiguousarray(B, np.float64)
+    cnt, n, k = B.shape[0], A.shape[-1], B.shape[-1]
+    X = np.zeros_like(B)
+    info = np.zeros(cnt, np.int32)
+    berr = np.zeros(cnt)
+    ferr = np.full(cnt, np.nan)
+    iters = np.zeros(cnt, np.int32)
+    fb = np.zeros(cnt, np.int32)
+    Xt = None if X_true is None else np.ascontiguousarray(X_true, np.float64)
+    flags = (0 if equilibrate else _lib.MIXED_NO_EQUILIBRATE) | (0 if fallback else _lib.MIXED_NO_FALLBACK)
+    P = _lib.ptr
+    _check(L.nppb_solve_mixed_batched(cnt, n, k, P(A), P(B), P(X), P(Xt), tol, max_iter, flags, P(info),
+                                      P(berr), P(ferr), P(iters), P(fb)))
+    return X, {"berr": berr, "ferr": ferr, "iters": iters, "fallback": fb, "info": info}

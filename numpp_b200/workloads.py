@@ -100,3 +100,22 @@ def uneven_bytes(sys: dict) -> float:
     nb = sys["n"].astype(np.float64) * sys["nrhs"]
     inv = sys["inv_off"] >= 0
     return float(8 * nn.sum() + 16 * nb.sum() + 8 * nn[inv].sum() + 20 * len(nn))
+
+
+def conditioned_batch(seed: int, count: int, n: int, kappa: float, nrhs: int = 1,
+                      row_scale_decades: float = 0.0):
+    """A = Q1 diag(sigma) Q2^T with Q from the QR of N(0,1) matrices and sigma
+    log-spaced from 1 to kappa; optionally rows scaled by 10^U(-d, d); x_true
+    = N(0,1); b = A x_true in FP64. Returns (A, B, X_true)."""
+    rng = np.random.default_rng(seed)
+    sigma = np.logspace(0.0, np.log10(kappa), n)
+    A = np.empty((count, n, n))
+    for i in range(count):
+        q1, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        q2, _ = np.linalg.qr(rng.standard_normal((n, n)))
+        A[i] = (q1 * sigma) @ q2.T
+    if row_scale_decades:
+        A *= 10.0 ** rng.uniform(-row_scale_decades, row_scale_decades, size=(count, n, 1))
+    X = rng.standard_normal((count, n, nrhs))
+    B = A @ X
+    return A, B, X
