@@ -2,14 +2,15 @@
 //
 // No counterpart in the reference, which solves in double only
 // (src/linalg/linalg.cpp:20-26,92-103). Per system of a uniform batch:
-//  k_equilibrate  power-of-two row and column scales r, c (exact in FP64) so
+//  k_equil_rows / k_equil_apply
+//                 power-of-two row and column scales r, c (exact in FP64) so
 //                 that every row and column of diag(r) A diag(c) peaks in
 //                 [1, 2); writes that matrix in FP32 and ||A||_inf
 //  k_scale_rhs    r * B in FP32 (the first right-hand side), ||B||_max
 //  k_apply        X = c * Y (first solution) or X += c * Y (correction), FP64
-//  k_residual     R = B - A X in FP64, eta = max|R| / (||A||_inf max|X| + max|B|)
-//                 (normwise backward error), r * R in FP32 for the next
-//                 correction, and the convergence / stall decision
+//  k_residual     R = B - A X in FP64 and r * R in FP32 for the next correction
+//  k_refine_decide eta = max|R| / (||A||_inf max|X| + max|B|) (normwise
+//                 backward error) and the convergence / stall decision
 //  k_ferr         forward error max|X - Xtrue| / max|Xtrue| when Xtrue is known
 #include <cfloat>
 #include <cmath>
@@ -49,15 +50,24 @@ __device__ double block_max(double v, double* red) {
   return warp_max(r);
 }
 
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* bits, double v) {
+  // non-negative doubles (and NaN, which then wins) order like their bit patterns
+  atomicMax(bits, (unsigned long long)__double_as_longlong(v));
+}
+
+// Row pass, one CTA per (system, kMixedRows rows): row scales, ||A||_inf, and
+// the column maxima of diag(r) |A| over this CTA's rows.
 __global__ void __launch_bounds__(MT)
-k_equilibrate(const double* __restrict__ A, int n, int equil, float* __restrict__ A32,
-              double* __restrict__ rs, double* __restrict__ cs, RefineState* __restrict__ st) {
-  __shared__ double rsc[kMixedMaxN];
+k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict__ rs,
+             double* __restrict__ cmax, RefineState* __restrict__ st) {
+  __shared__ double rsc[kMixedRows];
   __shared__ double red[MT / 32];
-  const int s = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const double* a = A + (int64_t)s * n * n;
+  const int s = blockIdx.x, r0 = blockIdx.y * kMixedRows;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int rows = min(kMixedRows, n - r0);
+  const double* a = A + (int64_t)s * n * n + (int64_t)r0 * n;
   double arow = 0.0;
-  for (int i = warp; i < n; i += MT / 32) {
+  for (int i = warp; i < rows; i += MT / 32) {
     double m = 0.0, sum = 0.0;
     for (int j = lane; j < n; j += 32) {
       const double v = fabs(a[(int64_t)i * n + j]);
@@ -66,25 +76,45 @@ k_equilibrate(const double* __restrict__ A, int n, int equil, float* __restrict_
     }
     m = warp_max(m);
     sum = warp_sum(sum);
-    if (lane == 0) rsc[i] = equil ? pow2_scale(m) : 1.0;
+    const double r = equil ? pow2_scale(m) : 1.0;
+    if (lane == 0) {
+      rsc[i] = r;
+      rs[(int64_t)s * n + r0 + i] = r;
+    }
     arow = fmax(arow, sum);
   }
   const double anorm = block_max(arow, red);  // includes the barrier publishing rsc
+  if (tid == 0) atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&st[s].anorm), anorm);
+  if (!equil) return;
   for (int j = tid; j < n; j += MT) {
     double m = 0.0;
-    for (int i = 0; i < n; ++i) m = fmax(m, rsc[i] * fabs(a[(int64_t)i * n + j]));
-    cs[(int64_t)s * n + j] = equil ? pow2_scale(m) : 1.0;
+    for (int i = 0; i < rows; ++i) m = fmax(m, rsc[i] * fabs(a[(int64_t)i * n + j]));
+    atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), m);
   }
-  for (int i = tid; i < n; i += MT) rs[(int64_t)s * n + i] = rsc[i];
+}
+
+// Column scales from the maxima, the scaled matrix in FP32, and the state of
+// every system (by the CTA of its first rows).
+__global__ void __launch_bounds__(MT)
+k_equil_apply(const double* __restrict__ A, int n, int equil, const double* __restrict__ rs,
+              const double* __restrict__ cmax, double* __restrict__ cs, float* __restrict__ A32,
+              RefineState* __restrict__ st) {
+  __shared__ double csc[kMixedMaxN];
+  const int s = blockIdx.x, r0 = blockIdx.y * kMixedRows, tid = threadIdx.x;
+  const int rows = min(kMixedRows, n - r0);
+  for (int j = tid; j < n; j += MT) {
+    const double c = equil ? pow2_scale(cmax[(int64_t)s * n + j]) : 1.0;
+    csc[j] = c;
+    if (blockIdx.y == 0) cs[(int64_t)s * n + j] = c;
+  }
   __syncthreads();
-  const double* c = cs + (int64_t)s * n;
-  float* a32 = A32 + (int64_t)s * n * n;
-  for (int64_t idx = tid; idx < (int64_t)n * n; idx += MT) {
-    const int i = (int)(idx / n), j = (int)(idx % n);
-    a32[idx] = (float)(rsc[i] * a[idx] * c[j]);
+  const double* a = A + (int64_t)s * n * n + (int64_t)r0 * n;
+  float* a32 = A32 + (int64_t)s * n * n + (int64_t)r0 * n;
+  for (int i = 0; i < rows; ++i) {
+    const double r = rs[(int64_t)s * n + r0 + i];
+    for (int j = tid; j < n; j += MT) a32[(int64_t)i * n + j] = (float)(r * a[(int64_t)i * n + j] * csc[j]);
   }
-  if (tid == 0) {
-    st[s].anorm = anorm;
+  if (blockIdx.y == 0 && tid == 0) {
     st[s].eta = INFINITY;
     st[s].prev = INFINITY;
     st[s].status = kRefineActive;
@@ -121,77 +151,115 @@ k_apply(double* __restrict__ X, const float* __restrict__ Y, const double* __res
   }
 }
 
-// One CTA per system; right-hand sides in chunks of 8 held in shared memory,
-// one warp per row of A (coalesced row reads, shuffle reductions).
+// One CTA per (system, kMixedRows rows of A): R = B - A X for those rows,
+// right-hand sides in chunks of RC, X staged through shared memory in blocks
+// of CB rows; each warp keeps kMixedRows / 8 rows' sums in registers and reads
+// its rows of A coalesced. max |R| (and, by the first CTA, max |X|) go to the
+// system's running maxima; k_refine_decide turns them into eta.
 constexpr int RC = 8;
+constexpr int CB = 512;
+constexpr int RW = kMixedRows / (MT / 32);  // rows per warp
 
 __global__ void __launch_bounds__(MT)
 k_residual(const double* __restrict__ A, const double* __restrict__ B, const double* __restrict__ X,
            int n, int nrhs, const double* __restrict__ rs, float* __restrict__ R32,
-           RefineState* __restrict__ st, double tol, int iter, int decide, int* __restrict__ active) {
-  __shared__ double xs[kMixedMaxN * RC];
+           RefineState* __restrict__ st, int only_active) {
+  __shared__ double xs[CB * RC];
   __shared__ double red[MT / 32];
-  __shared__ double ax_s[MT / 32][RC];
-  const int s = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if (decide && st[s].status != kRefineActive) return;
+  __shared__ double ax_s[MT / 32][RW][RC];
+  const int s = blockIdx.x, r0 = blockIdx.y * kMixedRows;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (only_active && st[s].status != kRefineActive) return;
   const int64_t nb = (int64_t)n * nrhs;
   const double* a = A + (int64_t)s * n * n;
   const double* b = B + (int64_t)s * nb;
   const double* x = X + (int64_t)s * nb;
+  const bool first = blockIdx.y == 0;
   double rmax = 0.0, xmax = 0.0;
   for (int k0 = 0; k0 < nrhs; k0 += RC) {
     const int kc = min(RC, nrhs - k0);
-    __syncthreads();
-    for (int idx = tid; idx < n * RC; idx += MT) {
-      const int j = idx / RC, k = idx % RC;
-      const double v = k < kc ? x[(int64_t)j * nrhs + k0 + k] : 0.0;
-      xs[idx] = v;
-      xmax = fmax(xmax, fabs(v));
+    double acc[RW][RC];
+#pragma unroll
+    for (int q = 0; q < RW; ++q)
+#pragma unroll
+      for (int k = 0; k < RC; ++k) acc[q][k] = 0.0;
+    for (int j0 = 0; j0 < n; j0 += CB) {
+      const int jn = min(CB, n - j0);
+      __syncthreads();
+      for (int idx = tid; idx < jn * RC; idx += MT) {
+        const int j = idx / RC, k = idx % RC;
+        const double v = k < kc ? x[(int64_t)(j0 + j) * nrhs + k0 + k] : 0.0;
+        xs[idx] = v;
+        if (first) xmax = fmax(xmax, fabs(v));
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < RW; ++q) {
+        const int i = r0 + warp * RW + q;
+        if (i < n) {
+          for (int j = lane; j < jn; j += 32) {
+            const double aij = a[(int64_t)i * n + j0 + j];
+#pragma unroll
+            for (int k = 0; k < RC; ++k) acc[q][k] = fma(aij, xs[j * RC + k], acc[q][k]);
+          }
+        }
+      }
     }
-    __syncthreads();
-    for (int i = warp; i < n; i += MT / 32) {
-      double acc[RC];
 #pragma unroll
-      for (int k = 0; k < RC; ++k) acc[k] = 0.0;
-      for (int j = lane; j < n; j += 32) {
-        const double aij = a[(int64_t)i * n + j];
+    for (int q = 0; q < RW; ++q)
 #pragma unroll
-        for (int k = 0; k < RC; ++k) acc[k] = fma(aij, xs[j * RC + k], acc[k]);
-      }
+      for (int k = 0; k < RC; ++k) acc[q][k] = warp_sum(acc[q][k]);
+    if (lane == 0) {
 #pragma unroll
-      for (int k = 0; k < RC; ++k) acc[k] = warp_sum(acc[k]);
-      if (lane == 0) {
+      for (int q = 0; q < RW; ++q)
 #pragma unroll
-        for (int k = 0; k < RC; ++k) ax_s[warp][k] = acc[k];
-      }
-      __syncwarp();
-      if (lane < kc) {
-        const double ax = ax_s[warp][lane];
-        const double r = b[(int64_t)i * nrhs + k0 + lane] - ax;
+        for (int k = 0; k < RC; ++k) ax_s[warp][q][k] = acc[q][k];
+    }
+    __syncwarp();
+    if (lane < RW * RC) {
+      const int q = lane / RC, k = lane % RC;
+      const int i = r0 + warp * RW + q;
+      if (i < n && k < kc) {
+        const double r = b[(int64_t)i * nrhs + k0 + k] - ax_s[warp][q][k];
         rmax = fmax(rmax, fabs(r));
-        if (R32) R32[(int64_t)s * nb + (int64_t)i * nrhs + k0 + lane] = (float)(rs[(int64_t)s * n + i] * r);
+        if (R32) R32[(int64_t)s * nb + (int64_t)i * nrhs + k0 + k] = (float)(rs[(int64_t)s * n + i] * r);
       }
-      __syncwarp();
     }
+    __syncwarp();
   }
   rmax = block_max(rmax, red);
-  xmax = block_max(xmax, red);
-  if (tid == 0) {
-    RefineState& q = st[s];
-    const double eta = rmax / (q.anorm * xmax + q.bnorm);
-    q.eta = eta;
-    if (decide) {
-      q.iters = iter;
-      if (eta <= tol) {
-        q.status = kRefineConverged;
-      } else if (iter > 0 && !(eta <= 0.5 * q.prev)) {
-        q.status = kRefineStalled;  // not halving any more (or NaN): refinement has stalled
-      } else {
-        atomicAdd(active, 1);
-      }
-      q.prev = eta;
-    }
+  if (tid == 0) atomic_max_nonneg(&st[s].rmax_bits, rmax);
+  if (first) {
+    xmax = block_max(xmax, red);
+    if (tid == 0) atomic_max_nonneg(&st[s].xmax_bits, xmax);
   }
+}
+
+// eta = max|R| / (||A||_inf max|X| + max|B|) per system; with decide, the
+// convergence / stall decision and the count of systems still refining.
+// Clears the running maxima for the next residual pass.
+__global__ void k_refine_decide(RefineState* __restrict__ st, int count, double tol, int iter, int decide,
+                                int* __restrict__ active) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= count) return;
+  RefineState& q = st[s];
+  if (decide && q.status != kRefineActive) return;
+  const double rmax = __longlong_as_double((long long)q.rmax_bits);
+  const double xmax = __longlong_as_double((long long)q.xmax_bits);
+  q.rmax_bits = 0;
+  q.xmax_bits = 0;
+  const double eta = rmax / (q.anorm * xmax + q.bnorm);
+  q.eta = eta;
+  if (!decide) return;
+  q.iters = iter;
+  if (eta <= tol) {
+    q.status = kRefineConverged;
+  } else if (iter > 0 && !(eta <= 0.5 * q.prev)) {
+    q.status = kRefineStalled;  // not halving any more (or NaN): refinement has stalled
+  } else {
+    atomicAdd(active, 1);
+  }
+  q.prev = eta;
 }
 
 __global__ void __launch_bounds__(MT)
@@ -218,8 +286,12 @@ __global__ void k_mark_fp32_failures(const int32_t* __restrict__ info32, RefineS
 }  // namespace
 
 cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, float* A32, double* rs, double* cs,
-                              RefineState* st, cudaStream_t s) {
-  k_equilibrate<<<count, MT, 0, s>>>(A, n, equil, A32, rs, cs, st);
+                              double* cmax, RefineState* st, cudaStream_t s) {
+  const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
+  k_equil_rows<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, st);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_equil_apply<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, cs, A32, st);
   return cudaGetLastError();
 }
 cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,
@@ -235,7 +307,11 @@ cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, 
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
                            const double* rs, float* R32, RefineState* st, double tol, int iter, int decide,
                            int* active, cudaStream_t s) {
-  k_residual<<<count, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, st, tol, iter, decide, active);
+  const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
+  k_residual<<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, st, decide);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  k_refine_decide<<<(count + 255) / 256, 256, 0, s>>>(st, count, tol, iter, decide, active);
   return cudaGetLastError();
 }
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,

@@ -5,22 +5,29 @@
 // same elimination is blocked by 32-column panels and run for every system of
 // the batch at once, one step (panel) per pair of launches:
 //
-//  k_panel   one CTA per active system: the (n-k0) x 32 panel lives in
-//            registers (row r of the panel in thread r mod NT), the pivot of each
-//            column is the first largest |a| in position order (the reference's
-//            rule, linalg.cpp:55-57) found with one barrier per column; a row
-//            exchange only swaps the two rows' position labels. It writes the
-//            panel at its pivoted positions, the pivots, L11^-1 (for the update)
-//            and the row moves the panel implies for every other column, and
-//            folds the pivots into det / slogdet in the reference's order.
+//  k_panel   one CTA (n - k0 <= 512) or one thread-block cluster of 2..8 CTAs
+//            (up to 4096 rows) per active system: the (n-k0) x 32 panel lives in
+//            registers (row r of the panel in thread r mod NT of CTA r / (NT*RPT)),
+//            the pivot of each column is the first largest |a| in position order
+//            (the reference's rule, linalg.cpp:55-57) found with one barrier per
+//            column (plus one cluster barrier, the CTAs' candidates exchanged
+//            through distributed shared memory); a row exchange only swaps the
+//            two rows' position labels. It writes the panel at its pivoted
+//            positions, the pivots, L11^-1 (for the update) and the row moves the
+//            panel implies for every other column, and folds the pivots into
+//            det / slogdet in the reference's order.
 //  k_update  one CTA per (system, 64-column strip) of the trailing matrix, of
 //            the right-hand sides (augmented columns: forward substitution rides
 //            along) and of the identity (inverse): apply the row moves,
 //            U12 = L11^-1 A12 and A22 -= L21 U12.
 //  k_back    one CTA per (system, 64-column strip) of X / inverse: blocked back
-//            substitution with U (diagonal blocks by substitution).
-//  k_forward getrs from stored factors: row gather through the pivots and
-//            blocked forward substitution with the unit-lower L.
+//            substitution with U (diagonal blocks by substitution) inside a
+//            256-row window; k_back_update then applies the solved window to
+//            every row above it, one CTA per (strip, 64-row tile). Windows run
+//            from the bottom, one pass per window.
+//  k_forward getrs from stored factors: k_permute gathers the rows through the
+//            pivots, then windows from the top with the unit-lower L
+//            (k_forward + k_forward_update).
 //
 // Every kernel is instantiated for FP64 factors (tile products on the FP64
 // tensor pipe, mma.m8n8k4) and for FP32 factors (the mixed-precision path:
@@ -28,6 +35,8 @@
 // workspace, so no copy pass is needed. Exact-zero pivots stop the system
 // (info = k+1) and later launches skip it, as the reference stops
 // (linalg.cpp:56).
+#include <cooperative_groups.h>
+
 #include <climits>
 #include <cmath>
 #include <type_traits>
@@ -42,6 +51,9 @@ constexpr int NB = kStepNB;  // 32
 constexpr int LS = NB + 1;   // 33: stride of 32-wide shared tiles
 constexpr int WS = 64 + 1;   // 65: stride of 64-wide shared tiles
 constexpr int UT = 128;      // threads of the strip kernels
+constexpr int SB = 256;      // rows of one substitution window
+
+namespace cg = cooperative_groups;
 
 // ---------------------------------------------------------------------------
 // System descriptor: from the list, or derived for a uniform batch.
@@ -109,7 +121,10 @@ __device__ __forceinline__ typename Pair<T>::type make_pair2(T x, T y) {
 
 // ---------------------------------------------------------------------------
 // k_panel
-template <class T, int NT, int RPT>
+// CS CTAs per system (a cluster when CS > 1); CTA `rank` holds panel rows
+// [rank*NT*RPT, (rank+1)*NT*RPT). Rank 0 holds the top rows and does the
+// per-panel bookkeeping (pivots, L11^-1, det, row moves of the top rows).
+template <class T, int NT, int RPT, int CS>
 __global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
 k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
   using P2 = typename Pair<T>::type;
@@ -117,32 +132,42 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
   __shared__ __align__(16) T cand_row[2][NW][NB];
   __shared__ T cand_v[2][NW];
   __shared__ int cand_k[2][NW];
+  __shared__ __align__(16) T xc_row[2][CS][NB];  // each CTA's candidate, pushed by every CTA of the cluster
+  __shared__ T xc_v[2][CS];
+  __shared__ int xc_k[2][CS];
   __shared__ T L11[NB][LS];
   __shared__ T Xinv[NB][LS];
   __shared__ T pvals[NB];
   __shared__ int s_ndisp;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const SysDesc d = step_desc(sa, list ? list[blockIdx.x] : (int)blockIdx.x);
+  const int rank = CS > 1 ? (int)blockIdx.x % CS : 0;
+  const int sysb = (int)blockIdx.x / CS;
+  const SysDesc d = step_desc(sa, list ? list[sysb] : sysb);
   StepScratchT<T>* sc = sa.scratch + d.pad_;
   const int n = d.n, m = n - k0, kb = min(NB, m);
   if (k0 == 0) {
-    if (tid == 0) {
+    if (tid == 0 && rank == 0) {
       sc->info = 0; sc->nswap = 0; sc->det = 1.0; sc->logabs = 0.0; sc->sign = 1.0;
     }
-    __syncthreads();
   } else if (sc->info) {
-    return;
+    return;  // the same for every CTA of the cluster
   }
   T* dst = sa.LU + d.lu_off;
   const T* src = (k0 == 0 && sa.A) ? sa.A + d.a_off : dst;
+  if (rank == 0) {
+    for (int idx = tid; idx < NB * NB; idx += NT) {
+      const int i = idx / NB, c = idx % NB;
+      L11[i][c] = (i == c) ? T(1) : T(0);
+    }
+  }
 
   T a[RPT][NB];
   int pos[RPT];
   bool valid[RPT];
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
-    const int r = tid + q * NT;
+    const int r = rank * NT * RPT + tid + q * NT;
     valid[q] = r < m;
     pos[q] = r;
     const T* row = src + (int64_t)(k0 + r) * n + k0;
@@ -198,11 +223,40 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
           const int k = cand_k[par][w];
           if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
         }
+        const T* prow = cand_row[par][gw];
+        if constexpr (CS > 1) {
+          // every CTA pushes its candidate into slot `rank` of every CTA, then
+          // one cluster barrier; the slots alternate with the column parity, so
+          // a slot is rewritten only after every CTA has passed the next barrier
+          cg::cluster_group cl = cg::this_cluster();
+          if (warp == 0) {
+            const T rv = prow[lane];
+#pragma unroll 1
+            for (int to = 0; to < CS; ++to) {
+              cl.map_shared_rank(&xc_row[par][rank][0], to)[lane] = rv;
+              if (lane == 0) {
+                *cl.map_shared_rank(&xc_v[par][rank], to) = gb;
+                *cl.map_shared_rank(&xc_k[par][rank], to) = gk;
+              }
+            }
+          }
+          cl.sync();
+          gb = T(-1);
+          gk = INT_MAX;
+          int gr = 0;
+#pragma unroll
+          for (int r = 0; r < CS; ++r) {
+            const T v = xc_v[par][r];
+            const int k = xc_k[par][r];
+            if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gr = r; }
+          }
+          prow = xc_row[par][gr];
+        }
         if (gb == T(0)) {
           info = k0 + j + 1;
         } else {
-          const P2* pr2 = reinterpret_cast<const P2*>(cand_row[par][gw]);
-          const T pj = cand_row[par][gw][u];
+          const P2* pr2 = reinterpret_cast<const P2*>(prow);
+          const T pj = prow[u];
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
             if (valid[q]) {
@@ -210,7 +264,7 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
               else if (pos[q] == gk) pos[q] = j;
             }
           }
-          if (tid == 0) {
+          if (tid == 0 && rank == 0) {
             pvals[j] = pj;
             if (sa.ipiv) sa.ipiv[d.piv_off + k0 + j] = k0 + gk;
           }
@@ -252,7 +306,7 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
   }
 
   if (info) {
-    if (tid == 0) {
+    if (tid == 0 && rank == 0) {
       sc->info = info;
       if (sa.det) sa.det[d.idx] = 0.0;
       if (sa.sign) sa.sign[d.idx] = 0.0;
@@ -262,12 +316,10 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
     return;
   }
 
-  // panel back at the pivoted positions; L11 into shared memory
-  for (int idx = tid; idx < NB * NB; idx += NT) {
-    const int i = idx / NB, c = idx % NB;
-    L11[i][c] = (i == c) ? T(1) : T(0);
-  }
-  __syncthreads();
+  // panel back at the pivoted positions; the strictly lower part of L11 into
+  // rank 0's shared memory (identity-initialised before the column loop)
+  T(*L11r)[LS] = L11;
+  if constexpr (CS > 1) L11r = reinterpret_cast<T(*)[LS]>(cg::this_cluster().map_shared_rank(&L11[0][0], 0));
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
     if (valid[q]) {
@@ -278,10 +330,10 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
       if (pos[q] < kb) {
 #pragma unroll 32
         for (int c = 0; c < NB; ++c)
-          if (c < pos[q]) L11[pos[q]][c] = a[q][c];
+          if (c < pos[q]) L11r[pos[q]][c] = a[q][c];
       }
-      // row moves for the other columns
-      const int r = tid + q * NT;
+      // row moves for the other columns (rows r < kb all live in rank 0)
+      const int r = rank * NT * RPT + tid + q * NT;
       if (pos[q] < kb) {
         sc->top_src[pos[q]] = r;
       } else if (r < kb) {
@@ -291,7 +343,12 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
       }
     }
   }
-  __syncthreads();
+  if constexpr (CS > 1) {
+    cg::this_cluster().sync();  // no shared memory of another CTA is touched after this
+    if (rank != 0) return;
+  } else {
+    __syncthreads();
+  }
   if (tid == 0) sc->ndisp = s_ndisp;
 
   // L11^-1 (unit lower, identity-padded past kb): lane c builds column c in
@@ -647,10 +704,32 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
 }
 
 // ---------------------------------------------------------------------------
-// k_back: X = U^-1 Y on a 64-column strip, blocks from the bottom.
+// Substitution windows: rows [jw*SB, min(n, (jw+1)*SB)) of a system. Back
+// substitution takes window jw = (n-1)/SB - pass (from the bottom), forward
+// substitution window jw = pass (from the top); a system without that window
+// skips the pass.
+__device__ __forceinline__ bool back_window(int n, int pass, int& lo, int& hi) {
+  const int jw = (n - 1) / SB - pass;
+  lo = jw * SB;
+  hi = min(n, lo + SB);
+  return jw >= 0;
+}
+__device__ __forceinline__ bool forward_window(int n, int pass, int& lo, int& hi) {
+  lo = pass * SB;
+  hi = min(n, lo + SB);
+  return lo < n;
+}
+
+template <class T>
+__device__ __forceinline__ T* strip_base(const StepArgsT<T>& sa, const StepItem& it, const SysDesc& d, int& ld) {
+  ld = (it.kind == kSegRhs) ? d.nrhs : d.n;
+  return (it.kind == kSegRhs) ? sa.X + d.b_off : sa.inv + d.inv_off;
+}
+
+// k_back: X = U^-1 Y on a 64-column strip inside one window, blocks from the bottom.
 template <class T>
 __global__ void __launch_bounds__(UT)
-k_back(StepArgsT<T> sa, const StepItem* __restrict__ items) {
+k_back(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
   __shared__ T Ub[NB * LS];
   __shared__ T Xb[NB * WS];
   __shared__ T As[64 * LS];
@@ -659,10 +738,11 @@ k_back(StepArgsT<T> sa, const StepItem* __restrict__ items) {
   const SysDesc d = step_desc(sa, it.sys);
   if (!sa.solve_only && sa.scratch[d.pad_].info) return;
   const int n = d.n, w = it.width, c0 = it.c0;
+  int lo, hi, ld;
+  if (!back_window(n, pass, lo, hi)) return;
   const T* U = sa.LU + d.lu_off;
-  T* X = (it.kind == kSegRhs) ? sa.X + d.b_off : sa.inv + d.inv_off;
-  const int ld = (it.kind == kSegRhs) ? d.nrhs : n;
-  for (int kb0 = ((n - 1) / NB) * NB; kb0 >= 0; kb0 -= NB) {
+  T* X = strip_base(sa, it, d, ld);
+  for (int kb0 = ((hi - 1) / NB) * NB; kb0 >= lo; kb0 -= NB) {
     const int bw = min(NB, n - kb0);
     for (int idx = tid; idx < NB * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
@@ -685,7 +765,7 @@ k_back(StepArgsT<T> sa, const StepItem* __restrict__ items) {
       const int i = idx >> 6, c = idx & 63;
       if (i < bw && c < w) X[(int64_t)(kb0 + i) * ld + c0 + c] = Xb[i * WS + c];
     }
-    for (int r0 = 0; r0 < kb0; r0 += 64) {
+    for (int r0 = lo; r0 < kb0; r0 += 64) {
       for (int idx = tid; idx < 64 * NB; idx += UT) {
         const int i = idx >> 5, q = idx & 31;
         As[i * LS + q] = (r0 + i < kb0 && q < bw) ? U[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
@@ -699,27 +779,67 @@ k_back(StepArgsT<T> sa, const StepItem* __restrict__ items) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// k_forward: getrs from stored factors, X[p] = B[perm[p]] then unit-lower
-// substitution, blocks from the top. X must not alias B.
+// X[r0 .. r0+63] -= M[r0 .. r0+63, lo:hi] X[lo:hi] on one strip (rows < rend):
+// the solved window applied to a 64-row tile outside it.
+template <class T>
+__device__ __forceinline__ void window_apply(const T* __restrict__ M, int n, T* X, int ld, int c0, int w, int r0,
+                                             int rend, int lo, int hi) {
+  __shared__ T As[64 * LS];
+  __shared__ T Bs[NB * WS];
+  const int tid = threadIdx.x;
+  Acc64<T> acc;
+  acc.each([&](int r, int cc, T& x) { x = (r0 + r < rend && cc < w) ? X[(int64_t)(r0 + r) * ld + c0 + cc] : T(0); });
+  for (int kc = lo; kc < hi; kc += NB) {
+    const int kw = min(NB, hi - kc);
+    for (int idx = tid; idx < 64 * NB; idx += UT) {
+      const int i = idx >> 5, q = idx & 31;
+      As[i * LS + q] = (r0 + i < rend && q < kw) ? M[(int64_t)(r0 + i) * n + kc + q] : T(0);
+    }
+    for (int idx = tid; idx < NB * 64; idx += UT) {
+      const int i = idx >> 6, c = idx & 63;
+      Bs[i * WS + c] = (i < kw && c < w) ? X[(int64_t)(kc + i) * ld + c0 + c] : T(0);
+    }
+    __syncthreads();
+    acc.sub_mma(As, Bs);
+    __syncthreads();
+  }
+  acc.each([&](int r, int cc, T& x) {
+    if (r0 + r < rend && cc < w) X[(int64_t)(r0 + r) * ld + c0 + cc] = x;
+  });
+}
+
+// Rows above the window of this pass: one CTA per (strip, 64-row tile = blockIdx.y).
 template <class T>
 __global__ void __launch_bounds__(UT)
-k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items) {
-  extern __shared__ __align__(16) unsigned char fsm_raw[];
-  T* Lb = reinterpret_cast<T*>(fsm_raw);  // 32 x LS
-  T* Xb = Lb + NB * LS;                   // 32 x WS
-  T* As = Xb + NB * WS;                   // 64 x LS
-  int* perm = reinterpret_cast<int*>(As + 64 * LS);
+k_back_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
+  if (!sa.solve_only && sa.scratch[d.pad_].info) return;
+  int lo, hi, ld;
+  if (!back_window(d.n, pass, lo, hi)) return;
+  const int r0 = (int)blockIdx.y * 64;
+  if (r0 >= lo) return;
+  T* X = strip_base(sa, it, d, ld);
+  window_apply<T>(sa.LU + d.lu_off, d.n, X, ld, it.c0, it.width, r0, lo, lo, hi);
+}
+
+// ---------------------------------------------------------------------------
+// getrs from stored factors. k_permute: X[p] = B[perm[p]], perm from the swap
+// list; then forward windows with the unit-lower L. X must not alias B.
+template <class T>
+__global__ void __launch_bounds__(UT)
+k_permute(StepArgsT<T> sa, const StepItem* __restrict__ items) {
+  extern __shared__ int perm[];
   const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
   const int n = d.n, w = it.width, c0 = it.c0, ld = d.nrhs;
-  const T* L = sa.LU + d.lu_off;
   const int32_t* ipiv = sa.ipiv + d.piv_off;
   const T* B = sa.B + d.b_off;
   T* X = sa.X + d.b_off;
+  for (int i = tid; i < n; i += UT) perm[i] = i;
+  __syncthreads();
   if (tid == 0) {
-    for (int i = 0; i < n; ++i) perm[i] = i;
     for (int k = 0; k < n; ++k) {
       int p = ipiv[k];
       if (p < k || p >= n) p = k;  // a swap list only names rows >= k
@@ -731,8 +851,23 @@ k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items) {
     const int p = idx >> 6, c = idx & 63;
     if (c < w) X[(int64_t)p * ld + c0 + c] = B[(int64_t)perm[p] * ld + c0 + c];
   }
-  __syncthreads();
-  for (int kb0 = 0; kb0 < n; kb0 += NB) {
+}
+
+template <class T>
+__global__ void __launch_bounds__(UT)
+k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+  __shared__ T Lb[NB * LS];
+  __shared__ T Xb[NB * WS];
+  __shared__ T As[64 * LS];
+  const int tid = threadIdx.x;
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
+  const int n = d.n, w = it.width, c0 = it.c0, ld = d.nrhs;
+  int lo, hi;
+  if (!forward_window(n, pass, lo, hi)) return;
+  const T* L = sa.LU + d.lu_off;
+  T* X = sa.X + d.b_off;
+  for (int kb0 = lo; kb0 < hi; kb0 += NB) {
     const int bw = min(NB, n - kb0), kb1 = kb0 + bw;
     for (int idx = tid; idx < NB * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
@@ -755,18 +890,31 @@ k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items) {
       const int i = idx >> 6, c = idx & 63;
       if (i < bw && c < w) X[(int64_t)(kb0 + i) * ld + c0 + c] = Xb[i * WS + c];
     }
-    for (int r0 = kb1; r0 < n; r0 += 64) {
+    for (int r0 = kb1; r0 < hi; r0 += 64) {
       for (int idx = tid; idx < 64 * NB; idx += UT) {
         const int i = idx >> 5, q = idx & 31;
-        As[i * LS + q] = (r0 + i < n && q < bw) ? L[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
+        As[i * LS + q] = (r0 + i < hi && q < bw) ? L[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
       }
       __syncthreads();
       tile_update<T>(
-          As, Xb, r0, n, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
+          As, Xb, r0, hi, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
           [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
       __syncthreads();
     }
   }
+}
+
+// Rows below the window of this pass: one CTA per (strip, 64-row tile = blockIdx.y).
+template <class T>
+__global__ void __launch_bounds__(UT)
+k_forward_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
+  int lo, hi;
+  if (!forward_window(d.n, pass, lo, hi)) return;
+  const int r0 = hi + (int)blockIdx.y * 64;
+  if (r0 >= d.n) return;
+  window_apply<T>(sa.LU + d.lu_off, d.n, sa.X + d.b_off, d.nrhs, it.c0, it.width, r0, d.n, lo, hi);
 }
 
 template <class T>
@@ -774,17 +922,33 @@ size_t update_smem(int nmax) {
   return sizeof(T) * (2 * NB * WS + 2 * 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
 }
 template <class T>
-size_t forward_smem(int nmax) {
-  return sizeof(T) * (NB * LS + NB * WS + 64 * LS) + sizeof(int) * (size_t)nmax;
+cudaError_t prepare_t() {
+  return cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)update_smem<T>(kStepMaxN));
 }
 
+// Passes over windows of SB rows; between two windows, the solved one is
+// applied to the rows on the far side (tiles of 64 rows: blockIdx.y).
 template <class T>
-cudaError_t prepare_t() {
-  cudaError_t e = cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)update_smem<T>(kStepMaxN));
-  if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_forward<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)forward_smem<T>(kStepMaxN));
+cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, bool forward,
+                     cudaStream_t st) {
+  const int passes = (nmax + SB - 1) / SB;
+  for (int p = 0; p < passes; ++p) {
+    if (forward) k_forward<T><<<nitems, UT, 0, st>>>(sa, items, p);
+    else k_back<T><<<nitems, UT, 0, st>>>(sa, items, p);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // rows left on the far side of this pass's window, largest system first
+    const int far = forward ? nmax - (p + 1) * SB : ((nmax - 1) / SB - p) * SB;
+    if (p + 1 < passes && far > 0) {
+      const dim3 grid((unsigned)nitems, (unsigned)((far + 63) / 64));
+      if (forward) k_forward_update<T><<<grid, UT, 0, st>>>(sa, items, p);
+      else k_back_update<T><<<grid, UT, 0, st>>>(sa, items, p);
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+    }
+  }
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -795,14 +959,34 @@ cudaError_t step_prepare() {
   return prepare_t<float>();
 }
 
+template <class T, int CS>
+cudaError_t launch_cluster_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int k0, cudaStream_t st) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)nsys * CS);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = CS;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_panel<T, 256, 2, CS>, sa, list, k0);
+}
+
 template <class T>
 cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st) {
   if (nsys <= 0) return cudaSuccess;
-  if (mmax <= 64) k_panel<T, 64, 1><<<nsys, 64, 0, st>>>(sa, list, k0);
-  else if (mmax <= 128) k_panel<T, 128, 1><<<nsys, 128, 0, st>>>(sa, list, k0);
-  else if (mmax <= 256) k_panel<T, 256, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
-  else if (mmax <= 512) k_panel<T, 256, 2><<<nsys, 256, 0, st>>>(sa, list, k0);
+  if (mmax <= 64) k_panel<T, 64, 1, 1><<<nsys, 64, 0, st>>>(sa, list, k0);
+  else if (mmax <= 128) k_panel<T, 128, 1, 1><<<nsys, 128, 0, st>>>(sa, list, k0);
+  else if (mmax <= 256) k_panel<T, 256, 1, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
+  else if (mmax <= 512) k_panel<T, 256, 2, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
+  else if (mmax <= 1024) return launch_cluster_panel<T, 2>(sa, list, nsys, k0, st);
+  else if (mmax <= 2048) return launch_cluster_panel<T, 4>(sa, list, nsys, k0, st);
+  else if (mmax <= 4096) return launch_cluster_panel<T, 8>(sa, list, nsys, k0, st);
   else return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
@@ -816,24 +1000,25 @@ cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nit
 }
 
 template <class T>
-cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, cudaStream_t st) {
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_back<T><<<nitems, UT, 0, st>>>(sa, items);
-  return cudaGetLastError();
+  return windowed<T>(sa, items, nitems, nmax, false, st);
 }
 
 template <class T>
 cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
                            cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_forward<T><<<nitems, UT, forward_smem<T>(nmax), st>>>(sa, items);
-  return cudaGetLastError();
+  k_permute<T><<<nitems, UT, sizeof(int) * (size_t)nmax, st>>>(sa, items);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  return windowed<T>(sa, items, nitems, nmax, true, st);
 }
 
 #define NPPB_STEP_INSTANTIATE(T)                                                                          \
   template cudaError_t launch_panel<T>(const StepArgsT<T>&, const int32_t*, int, int, int, cudaStream_t);     \
   template cudaError_t launch_update<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);   \
-  template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, cudaStream_t);               \
+  template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);          \
   template cudaError_t launch_forward<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);
 NPPB_STEP_INSTANTIATE(double)
 NPPB_STEP_INSTANTIATE(float)

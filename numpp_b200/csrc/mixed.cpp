@@ -46,7 +46,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     return NPPB_E_ARG;
   }
   if (n > kMixedMaxN || count64 > INT32_MAX) {
-    set_error("order above 512 or count above 2^31-1");
+    set_error("order above " + std::to_string(kMixedMaxN) + " or count above 2^31-1");
     return NPPB_E_RANGE;
   }
   if (count64 == 0 || n == 0 || nrhs == 0) return NPPB_OK;
@@ -57,7 +57,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   if (!device()) return NPPB_E_NODEV;
   const int count = (int)count64;
   const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs, c = (size_t)count;
-  DevMem a32, piv, sc32, b32, y32, rsm, csm, stm, info32, act;
+  DevMem a32, piv, sc32, b32, y32, rsm, csm, cmx, stm, info32, act;
   NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
   NPPB_CUDA(piv.alloc(sizeof(int32_t) * c * n, st), "workspace");
   NPPB_CUDA(sc32.alloc(sizeof(StepScratchT<float>) * c, st), "workspace");
@@ -65,13 +65,16 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   NPPB_CUDA(y32.alloc(sizeof(float) * c * nb, st), "workspace");
   NPPB_CUDA(rsm.alloc(sizeof(double) * c * n, st), "workspace");
   NPPB_CUDA(csm.alloc(sizeof(double) * c * n, st), "workspace");
+  NPPB_CUDA(cmx.alloc(sizeof(double) * c * n, st), "workspace");
   NPPB_CUDA(stm.alloc(sizeof(RefineState) * c, st), "workspace");
+  NPPB_CUDA(cudaMemsetAsync(cmx.as<void>(), 0, sizeof(double) * c * n, st), "memset");
+  NPPB_CUDA(cudaMemsetAsync(stm.as<void>(), 0, sizeof(RefineState) * c, st), "memset");
   NPPB_CUDA(info32.alloc(sizeof(int32_t) * c, st), "workspace");
   NPPB_CUDA(act.alloc(sizeof(int), st), "workspace");
   RefineState* S = stm.as<RefineState>();
   const bool equil = !(flags & NPPB_MIXED_NO_EQUILIBRATE);
-  NPPB_CUDA(mixed_equilibrate(dA, count, n, equil ? 1 : 0, a32.as<float>(), rsm.as<double>(), csm.as<double>(), S,
-                              st),
+  NPPB_CUDA(mixed_equilibrate(dA, count, n, equil ? 1 : 0, a32.as<float>(), rsm.as<double>(), csm.as<double>(),
+                              cmx.as<double>(), S, st),
             "equilibrate");
   NPPB_CUDA(mixed_scale_rhs(dB, count, n, nrhs, rsm.as<double>(), b32.as<float>(), S, st), "scale rhs");
 

@@ -7,7 +7,8 @@
 
 namespace nppb {
 
-constexpr int kMixedMaxN = 512;
+constexpr int kMixedMaxN = 4096;
+constexpr int kMixedRows = 32;  // rows of A per CTA in the equilibration and residual kernels
 
 enum : int { kRefineActive = 0, kRefineConverged = 1, kRefineStalled = 2 };
 
@@ -19,10 +20,15 @@ struct RefineState {
   double prev;   // eta of the previous iteration
   int status;    // kRefine*
   int iters;     // corrections applied
+  // running maxima of non-negative doubles, as their bit patterns (atomicMax);
+  // zero at the start of every residual pass
+  unsigned long long rmax_bits;  // max |R|
+  unsigned long long xmax_bits;  // max |X|
 };
 
+// st and cmax (count * n doubles of column maxima) must be zero on entry.
 cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, float* A32, double* rs,
-                              double* cs, RefineState* st, cudaStream_t s);
+                              double* cs, double* cmax, RefineState* st, cudaStream_t s);
 cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,
                             RefineState* st, cudaStream_t s);
 cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, int n, int nrhs,

@@ -66,7 +66,7 @@ extern "C" int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nr
     return NPPB_E_ARG;
   }
   if (n > kStepMaxN || count > INT32_MAX) {
-    set_error("order above 512 or count above 2^31-1");
+    set_error("order above " + std::to_string(kStepMaxN) + " or count above 2^31-1");
     return NPPB_E_RANGE;
   }
   const size_t lu_bytes = ((size_t)count * n * n * sizeof(double) + 255) / 256 * 256;

@@ -10,7 +10,7 @@
 namespace nppb {
 
 constexpr int kStepNB = 32;     // panel width
-constexpr int kStepMaxN = 512;  // largest order the register panel holds (2 rows x 256 threads)
+constexpr int kStepMaxN = 4096;  // largest order: a cluster of 8 CTAs x 256 threads x 2 panel rows
 
 // Per-system state carried from one step to the next (one slot per system,
 // SysDesc::pad_ is the slot index). T is the factor precision.
@@ -86,8 +86,9 @@ cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, 
 template <class T>
 cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st);
+// Back substitution of each strip item (nmax >= n of any item).
 template <class T>
-cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, cudaStream_t st);
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, cudaStream_t st);
 template <class T>
 cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
                            cudaStream_t st);

@@ -5,7 +5,7 @@
 // calls there. A plan takes a whole (possibly uneven) batch at once:
 //  * orders <= 32 go to the warp-per-system kernel, one launch per padded order
 //    class (8 / 16 / 32);
-//  * orders 33..512 go to the step-wise path: systems sorted by order, step s
+//  * orders 33..4096 go to the step-wise path: systems sorted by order, step s
 //    (columns 32s..32s+31) is one panel launch per panel-height class plus one
 //    update launch over every (system, 64-column strip) still active, then one
 //    back-substitution launch.
@@ -48,7 +48,10 @@ int upload(T** d, const std::vector<T>& h) {
   return NPPB_OK;
 }
 
-int panel_class(int m) { return m <= 64 ? 0 : m <= 128 ? 1 : m <= 256 ? 2 : 3; }
+// one class per k_panel configuration (CTA size, rows per thread, cluster size)
+int panel_class(int m) {
+  return m <= 64 ? 0 : m <= 128 ? 1 : m <= 256 ? 2 : m <= 512 ? 3 : m <= 1024 ? 4 : m <= 2048 ? 5 : 6;
+}
 
 void add_strips(std::vector<StepItem>& out, int32_t sys, int16_t kind, int c0, int c1) {
   for (int c = c0; c < c1; c += 64) {
@@ -313,7 +316,7 @@ cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
   if (solve_only) {
     cudaError_t e = launch_forward(sa, back, (int)ch.back_count, ch.nmax, st);
     if (e != cudaSuccess) return e;
-    return launch_back(sa, back, (int)ch.back_count, st);
+    return launch_back(sa, back, (int)ch.back_count, ch.nmax, st);
   }
   for (const Step& s : ch.steps) {
     for (const auto& pr : s.panels) {
@@ -323,7 +326,7 @@ cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
     cudaError_t e = launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st);
     if (e != cudaSuccess) return e;
   }
-  return launch_back(sa, back, (int)ch.back_count, st);
+  return launch_back(sa, back, (int)ch.back_count, ch.nmax, st);
 }
 
 int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
@@ -355,7 +358,7 @@ int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
         timed(kKindUpdate, [&] { return launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st); });
       }
     }
-    timed(kKindBack, [&] { return launch_back(sa, back, (int)ch.back_count, st); });
+    timed(kKindBack, [&] { return launch_back(sa, back, (int)ch.back_count, ch.nmax, st); });
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -119,7 +119,7 @@ cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st)
   }
   const int64_t back = (int64_t)count * uniform_back_strips(n, sa.unrhs, sa.uinv);
   if (back > INT32_MAX) return cudaErrorInvalidValue;
-  return launch_back(sa, nullptr, (int)back, st);
+  return launch_back(sa, nullptr, (int)back, sa.un, st);
 }
 template cudaError_t run_step_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
 template cudaError_t run_step_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
@@ -133,7 +133,7 @@ cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream
   s2.uinv = 0;
   cudaError_t e = launch_forward(s2, nullptr, (int)items, sa.un, st);
   if (e != cudaSuccess) return e;
-  return launch_back(s2, nullptr, (int)items, st);
+  return launch_back(s2, nullptr, (int)items, s2.un, st);
 }
 template cudaError_t run_step_solve_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
 template cudaError_t run_step_solve_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);

@@ -57,7 +57,7 @@ cudaError_t launch_fill_i32(int32_t* p, int64_t n, int32_t v, cudaStream_t st);
 // Uniform batch of order n <= 32 on the warp-per-system kernel.
 cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st);
 
-// Uniform batch of orders 33..512 on the step-wise kernels (descriptors and
+// Uniform batch of orders 33..4096 on the step-wise kernels (descriptors and
 // work items derived from block indices, no plan). sa carries the pointers,
 // the LU workspace, the per-system scratch and un / unrhs / uinv.
 template <class T>

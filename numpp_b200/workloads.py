@@ -58,6 +58,29 @@ def uneven_batch(seed: int, count: int = 8192, n_lo: int = 4, n_hi: int = 512,
     }
 
 
+def packed_batch(seed: int, n, nrhs, want_inv, shift: bool = False) -> dict:
+    """A packed batch of given orders / right-hand-side counts / inverse mask:
+    A = N(0,1) (+ n*I with shift), b = N(0,1), matrices then right-hand sides
+    drawn from one generator in system order."""
+    rng = np.random.default_rng(seed)
+    n = np.asarray(n, np.int32)
+    nrhs = np.asarray(nrhs, np.int32)
+    want = np.asarray(want_inv, bool)
+    nn = n.astype(np.int64) ** 2
+    nb = n.astype(np.int64) * nrhs
+    a_off = np.concatenate([[0], np.cumsum(nn)[:-1]]).astype(np.int64)
+    b_off = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.int64)
+    inv_sizes = np.where(want, nn, 0)
+    inv_off = np.where(want, np.concatenate([[0], np.cumsum(inv_sizes)[:-1]]), -1).astype(np.int64)
+    A = rng.standard_normal(int(nn.sum()))
+    if shift:
+        for i, ni in enumerate(n):
+            A[a_off[i]:a_off[i] + ni * ni].reshape(ni, ni)[np.diag_indices(ni)] += ni
+    B = rng.standard_normal(int(nb.sum()))
+    return {"n": n, "nrhs": nrhs, "a_off": a_off, "b_off": b_off, "inv_off": inv_off, "A": A, "B": B,
+            "inv_size": int(inv_sizes.sum()), "count": len(n)}
+
+
 def take(sys: dict, idx) -> dict:
     """Repack a subset of an uneven batch (for bounded CPU samples and parity cases)."""
     idx = np.asarray(idx)
