@@ -16,10 +16,11 @@
 //            positions, the pivots, L11^-1 (for the update) and the row moves the
 //            panel implies for every other column, and folds the pivots into
 //            det / slogdet in the reference's order.
-//  k_update  one CTA per (system, 64-column strip) of the trailing matrix, of
+//  k_rows    one CTA per (system, 64-column strip) of the trailing matrix, of
 //            the right-hand sides (augmented columns: forward substitution rides
-//            along) and of the identity (inverse): apply the row moves,
-//            U12 = L11^-1 A12 and A22 -= L21 U12.
+//            along) and of the identity (inverse): apply the row moves and
+//            write U12 = L11^-1 A12.
+//  k_update  one CTA per (strip, 512 rows below the panel): A22 -= L21 U12.
 //  k_back    one CTA per (system, 64-column strip) of X / inverse: blocked back
 //            substitution with U (diagonal blocks by substitution) inside a
 //            256-row window; k_back_update then applies the solved window to
@@ -40,6 +41,8 @@
 #include <climits>
 #include <cmath>
 #include <type_traits>
+
+#include <cuda_bf16.h>
 
 #include "dmma.cuh"
 #include "nppb_step.hpp"
@@ -464,6 +467,17 @@ template <> struct Acc64<double> {  // 2 x 2 warps of 32 x 32, DMMA fragments
 #pragma unroll
         for (int e = 0; e < 2; ++e) f(wm + mi * 8 + g, wn + ni * 8 + 2 * tq + e, v[mi][ni][e]);
   }
+  // (row, even column, the two elements of that column pair)
+  template <class F>
+  __device__ __forceinline__ void pairs(F&& f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) f(wm + mi * 8 + g, wn + ni * 8 + 2 * tq, v[mi][ni][0], v[mi][ni][1]);
+  }
+  template <int AST = LS, int BST = WS>
   __device__ __forceinline__ void sub_mma(const double* As, const double* Bs) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
@@ -471,9 +485,9 @@ template <> struct Acc64<double> {  // 2 x 2 warps of 32 x 32, DMMA fragments
     for (int kk = 0; kk < NB; kk += 4) {
       double af[4], bf[4];
 #pragma unroll
-      for (int mi = 0; mi < 4; ++mi) af[mi] = -As[(wm + mi * 8 + g) * LS + kk + tq];
+      for (int mi = 0; mi < 4; ++mi) af[mi] = -As[(wm + mi * 8 + g) * AST + kk + tq];
 #pragma unroll
-      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * WS + wn + ni * 8 + g];
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[(kk + tq) * BST + wn + ni * 8 + g];
 #pragma unroll
       for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -492,15 +506,24 @@ template <> struct Acc64<float> {  // 4 x 8 elements per thread, FP32 FMA
 #pragma unroll
       for (int j = 0; j < 8; ++j) f(ty * 4 + i, tx * 8 + j, v[i][j]);
   }
+  template <class F>
+  __device__ __forceinline__ void pairs(F&& f) {
+    const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) f(ty * 4 + i, tx * 8 + j, v[i][j], v[i][j + 1]);
+  }
+  template <int AST = LS, int BST = WS>
   __device__ __forceinline__ void sub_mma(const float* As, const float* Bs) {
     const int ty = threadIdx.x >> 3, tx = threadIdx.x & 7;
 #pragma unroll 4
     for (int k = 0; k < NB; ++k) {
       float a[4], b[8];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[(ty * 4 + i) * LS + k];
+      for (int i = 0; i < 4; ++i) a[i] = As[(ty * 4 + i) * AST + k];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) b[j] = Bs[k * WS + tx * 8 + j];
+      for (int j = 0; j < 8; ++j) b[j] = Bs[k * BST + tx * 8 + j];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -576,6 +599,111 @@ template <> struct Acc32<float> {  // 4 x 4 elements per thread
   }
 };
 
+// FP32 factors with the trailing product on the tensor cores: operands
+// rounded to TF32 (mma.m16n8k8) or BF16 (mma.m16n8k16), FP32 accumulation.
+// Same 64 x 64 tile and 2 x 2 warp split as Acc64; a warp holds 2 x 4
+// m16n8 accumulators.
+enum : int { kUpdFp32 = 0, kUpdTf32 = 1, kUpdBf16 = 2 };
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+template <int MODE>
+struct AccTC {
+  float v[2][4][4];
+  template <class F>
+  __device__ __forceinline__ void pairs(F&& f) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) {
+        f(wm + mi * 16 + g, wn + ni * 8 + 2 * tq, v[mi][ni][0], v[mi][ni][1]);
+        f(wm + mi * 16 + g + 8, wn + ni * 8 + 2 * tq, v[mi][ni][2], v[mi][ni][3]);
+      }
+  }
+  template <int AST, int BST>
+  __device__ __forceinline__ void sub_mma(const float* As, const float* Bs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    if constexpr (MODE == kUpdTf32) {
+#pragma unroll
+      for (int kk = 0; kk < NB; kk += 8) {
+        uint32_t a[2][4], b[4][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          const float* r0 = As + (wm + mi * 16 + g) * AST + kk + tq;
+          const float* r1 = r0 + 8 * AST;
+          a[mi][0] = to_tf32(-r0[0]);
+          a[mi][1] = to_tf32(-r1[0]);
+          a[mi][2] = to_tf32(-r0[4]);
+          a[mi][3] = to_tf32(-r1[4]);
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          const float* c = Bs + (kk + tq) * BST + wn + ni * 8 + g;
+          b[ni][0] = to_tf32(c[0]);
+          b[ni][1] = to_tf32(c[4 * BST]);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+            asm volatile(
+                "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                "{%0,%1,%2,%3};\n"
+                : "+f"(v[mi][ni][0]), "+f"(v[mi][ni][1]), "+f"(v[mi][ni][2]), "+f"(v[mi][ni][3])
+                : "r"(a[mi][0]), "r"(a[mi][1]), "r"(a[mi][2]), "r"(a[mi][3]), "r"(b[ni][0]), "r"(b[ni][1]));
+      }
+    } else {
+#pragma unroll
+      for (int kk = 0; kk < NB; kk += 16) {
+        uint32_t a[2][4], b[4][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          const float* r0 = As + (wm + mi * 16 + g) * AST + kk + 2 * tq;
+          const float* r1 = r0 + 8 * AST;
+          const float2 x0 = *reinterpret_cast<const float2*>(r0);
+          const float2 x1 = *reinterpret_cast<const float2*>(r1);
+          const float2 x2 = *reinterpret_cast<const float2*>(r0 + 8);
+          const float2 x3 = *reinterpret_cast<const float2*>(r1 + 8);
+          a[mi][0] = pack_bf16(-x0.x, -x0.y);
+          a[mi][1] = pack_bf16(-x1.x, -x1.y);
+          a[mi][2] = pack_bf16(-x2.x, -x2.y);
+          a[mi][3] = pack_bf16(-x3.x, -x3.y);
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          const float* c = Bs + (kk + 2 * tq) * BST + wn + ni * 8 + g;
+          b[ni][0] = pack_bf16(c[0], c[BST]);
+          b[ni][1] = pack_bf16(c[8 * BST], c[9 * BST]);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni)
+            asm volatile(
+                "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+                "{%0,%1,%2,%3};\n"
+                : "+f"(v[mi][ni][0]), "+f"(v[mi][ni][1]), "+f"(v[mi][ni][2]), "+f"(v[mi][ni][3])
+                : "r"(a[mi][0]), "r"(a[mi][1]), "r"(a[mi][2]), "r"(a[mi][3]), "r"(b[ni][0]), "r"(b[ni][1]));
+      }
+    }
+  }
+};
+
+template <class T, int MODE> struct AccSel { using type = Acc64<T>; };
+template <> struct AccSel<float, kUpdTf32> { using type = AccTC<kUpdTf32>; };
+template <> struct AccSel<float, kUpdBf16> { using type = AccTC<kUpdBf16>; };
+
 // C[rows r0.., 64 cols] -= As * Bs for rows [r0, rend), columns < w, one tile.
 template <class T, class Load, class Store>
 __device__ __forceinline__ void tile_update(const T* As, const T* Bs, int r0, int rend, int w, Load cload,
@@ -589,20 +717,19 @@ __device__ __forceinline__ void tile_update(const T* As, const T* Bs, int r0, in
 }
 
 // ---------------------------------------------------------------------------
-// k_update
+// k_rows: one CTA per strip item of step k0. Applies the panel's row moves to
+// the strip (top rows from their sources, displaced old top rows to their new
+// positions) and, except for strips left of the panel, writes
+// U12 = L11^-1 A12 over the top rows. After it, k_update reads every row of the
+// strip in its final place, except at step 0 out of place, where only the
+// displaced rows have been written to the destination yet.
 template <class T>
 __global__ void __launch_bounds__(UT)
-k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* Us = reinterpret_cast<T*>(smem_raw);  // 32 x WS   U12 strip
-  T* D = Us + NB * WS;                     // 32 x WS   displaced rows
-  T* Tm = D + NB * WS;                     // 64 x LS   A12 (permuted, 32 x WS), then L21 buffer 1
-  T* As = Tm + 64 * LS;                    // 64 x LS   L11^-1, then L21 buffer 0
-  int* tsrc = reinterpret_cast<int*>(As + 64 * LS);
-  int* ddst = tsrc + NB;
-  int* dsrc = ddst + NB;
-  int* dmap = dsrc + NB;                   // m entries: displaced index of each row, or -1
-
+k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
+  __shared__ T Tm[NB * WS];
+  __shared__ T D[NB * WS];
+  __shared__ T Li[NB * LS];
+  __shared__ int tsrc[NB], ddst[NB], dsrc[NB];
   const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, k0, false);
   const SysDesc d = step_desc(sa, it.sys);
@@ -611,95 +738,206 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
   const int n = d.n, m = n - k0, kb = min(NB, m), w = it.width, c0 = it.c0;
   const Seg<T> s = segment(sa, d, it.kind, k0);
   const int nd = sc->ndisp;
-
   if (tid < NB) {
     tsrc[tid] = tid < kb ? sc->top_src[tid] : 0;
     ddst[tid] = tid < nd ? sc->disp_dst[tid] : 0;
     dsrc[tid] = tid < nd ? sc->disp_src[tid] : 0;
   }
   __syncthreads();
-  // rows moved by this step's pivots: top rows from their sources, displaced rows
   for (int idx = tid; idx < NB * 64; idx += UT) {
     const int i = idx >> 6, c = idx & 63;
     const bool in = c < w;
     Tm[i * WS + c] = (in && i < kb) ? seg_load(s, k0 + tsrc[i], c0 + c) : T(0);
     D[i * WS + c] = (in && i < nd) ? seg_load(s, k0 + dsrc[i], c0 + c) : T(0);
   }
+  __syncthreads();
+  for (int idx = tid; idx < NB * 64; idx += UT) {
+    const int i = idx >> 6, c = idx & 63;
+    if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
+  }
   if (it.kind == kSegLeft) {
-    __syncthreads();
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
       if (c < w && i < kb) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = Tm[i * WS + c];
-      if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
     }
     return;
   }
-  for (int r = tid; r < m - kb; r += UT) dmap[r] = -1;
-  for (int idx = tid; idx < NB * NB; idx += UT) As[(idx >> 5) * LS + (idx & 31)] = sc->linv[idx];
+  for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = sc->linv[idx];
   __syncthreads();
-  if (tid < nd) dmap[ddst[tid] - kb] = tid;
+  Acc32<T> u;
+  u.mma(Li, Tm);
+  u.each([&](int i, int c, T& x) {
+    if (i < kb && c < w) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = x;
+  });
+}
 
-  // U12 = L11^-1 A12 (32 x 64)
-  {
-    Acc32<T> u;
-    u.mma(As, Tm);
-    u.each([&](int i, int c, T& x) {
-      const T v = (i < kb) ? x : T(0);
-      Us[i * WS + c] = v;
-      if (i < kb && c < w) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = v;
-    });
-  }
-  __syncthreads();
-  if (kb < NB) return;  // last panel: nothing below it
-  // A22 strip -= L21 U12 in 64-row tiles, software-pipelined: while tile t is
-  // multiplied, tile t+1's L21 rows stream into shared memory (cp.async) and
-  // its accumulator inputs into registers.
-  const T* L = sa.LU + d.lu_off;
-  // L21 buffers: As (L11^-1 is consumed) and Tm (A12 is consumed once U12 is in Us)
-  auto prefetch_a = [&](int buf, int r0) {
-    T* dstb = buf ? Tm : As;
+// ---------------------------------------------------------------------------
+// k_update: A22 -= L21 U12 on one strip, rows [k0+32 + RG*blockIdx.y, +RG), in
+// 64-row tiles, software-pipelined: while tile t is multiplied, tile t+1's L21
+// rows stream into shared memory (cp.async, 16-byte pieces when aligned) and
+// its accumulator inputs into registers (paired loads when aligned).
+constexpr int RG = 512;
+
+// Shared row strides (elements) for bank-conflict-free fragment reads; every
+// row starts on a 16-byte boundary.
+template <class T, int MODE> struct TileCfg;
+template <> struct TileCfg<double, kUpdFp32> {
+  static constexpr int AS = 36;  // L21 tile: banks 8g + 2tq (8-byte reads)
+  static constexpr int US = 68;  // U12: banks 8tq + 2g
+};
+template <> struct TileCfg<float, kUpdFp32> {
+  static constexpr int AS = 34;  // SIMT reads: banks 8 * (row group)
+  static constexpr int US = 68;
+};
+template <> struct TileCfg<float, kUpdTf32> {
+  static constexpr int AS = 36;  // banks 4g + tq
+  static constexpr int US = 72;  // banks 8tq + g
+};
+template <> struct TileCfg<float, kUpdBf16> {
+  static constexpr int AS = 40;  // 8-byte reads: banks 8g + 2tq
+  static constexpr int US = 68;  // banks 8tq + g
+};
+
+template <class T, int MODE>
+size_t update_smem() {
+  return sizeof(T) * (NB * TileCfg<T, MODE>::US + 2 * 64 * TileCfg<T, MODE>::AS) + RG;
+}
+
+__device__ __forceinline__ void cp_async_pair(void* smem, const void* gmem, int bytes, int valid) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  if (bytes == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(valid));
+}
+
+// sm[r][c] <- g[r*gld + c] for r < rows, c < cols of a nr x nc tile (zero
+// elsewhere); vec: element pairs (rows and base aligned to two elements).
+template <class T>
+__device__ __forceinline__ void async_tile(T* sm, int sld, const T* g, int64_t gld, int rows, int cols, int nr,
+                                           int nc, bool vec) {
+  if (vec) {
+    const int cpr = nc / 2;
 #pragma unroll 4
-    for (int idx = tid; idx < 64 * NB; idx += UT) {
-      const int i = idx >> 5, q = idx & 31;
-      const bool ok = r0 + i < n;
-      cp_async<sizeof(T)>(dstb + i * LS + q, ok ? L + (int64_t)(r0 + i) * n + k0 + q : L, ok);
+    for (int idx = threadIdx.x; idx < nr * cpr; idx += UT) {
+      const int r = idx / cpr, c = (idx % cpr) * 2;
+      const int ok = r < rows ? max(0, min(2, cols - c)) : 0;
+      cp_async_pair(sm + r * sld + c, ok ? g + (int64_t)r * gld + c : g, 2 * (int)sizeof(T), ok * (int)sizeof(T));
     }
-    cp_async_commit();
+  } else {
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < nr * nc; idx += UT) {
+      const int r = idx / nc, c = idx % nc;
+      const bool ok = r < rows && c < cols;
+      cp_async<sizeof(T)>(sm + r * sld + c, ok ? g + (int64_t)r * gld + c : g, ok);
+    }
+  }
+  cp_async_commit();
+}
+
+template <class T>
+__device__ __forceinline__ bool pair_aligned(const T* p, int64_t ld) {
+  return ((reinterpret_cast<uintptr_t>(p) % (2 * sizeof(T))) == 0) && (ld % 2 == 0);
+}
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(UT, 3)
+k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
+  using P2 = typename Pair<T>::type;
+  using Acc = typename AccSel<T, MODE>::type;
+  constexpr int AS = TileCfg<T, MODE>::AS, US = TileCfg<T, MODE>::US;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* Us = reinterpret_cast<T*>(smem_raw);  // U12, 32 x 64
+  T* As0 = Us + NB * US;                   // L21 tiles, 64 x 32, two buffers
+  T* As1 = As0 + 64 * AS;
+  unsigned char* moved = reinterpret_cast<unsigned char*>(As1 + 64 * AS);  // RG flags
+
+  const int tid = threadIdx.x;
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, k0, false);
+  if (it.kind == kSegLeft) return;
+  const SysDesc d = step_desc(sa, it.sys);
+  const StepScratchT<T>* sc = sa.scratch + d.pad_;
+  if (sc->info) return;
+  const int n = d.n;
+  const int rb = k0 + NB + (int)blockIdx.y * RG;
+  if (rb >= n) return;  // includes the last panel (nothing below it)
+  const int re = min(n, rb + RG), w = it.width, c0 = it.c0;
+  const Seg<T> s = segment(sa, d, it.kind, k0);
+  const int64_t ld = s.ld;
+  // step 0 out of place: rows holding a displaced row are already in dst
+  const bool first = s.ident || s.src != s.dst;
+  if (first) {
+    for (int i = tid; i < re - rb; i += UT) moved[i] = 0;
+    __syncthreads();
+    if (tid < sc->ndisp) {
+      const int r = k0 + sc->disp_dst[tid];
+      if (r >= rb && r < re) moved[r - rb] = 1;
+    }
+    __syncthreads();
+  }
+  const T* L = sa.LU + d.lu_off;
+  T* const dst = s.dst + c0;
+  const T* const src = s.src + c0;
+  const bool dvec = pair_aligned(dst, ld), svec = !s.ident && pair_aligned(src, ld);
+
+  async_tile<T>(Us, US, dst + (int64_t)k0 * ld, ld, NB, w, NB, 64, dvec);
+  auto prefetch_a = [&](T* buf, int r0) {
+    async_tile<T>(buf, AS, L + (int64_t)r0 * d.n + k0, d.n, re - r0, NB, 64, NB, pair_aligned(L + k0, d.n));
   };
-  auto load_c = [&](Acc64<T>& c, int r0) {
-    c.each([&](int rr, int cc, T& x) {
+  auto load_c = [&](Acc& c, int r0) {
+    c.pairs([&](int rr, int cc, T& v0, T& v1) {
       const int r = r0 + rr;
-      T v = T(0);
-      if (r < n && cc < w) {
-        const int dm = dmap[r - k0 - kb];
-        v = dm >= 0 ? D[dm * WS + cc] : seg_load(s, r, c0 + cc);
+      v0 = v1 = T(0);
+      if (r < re && cc < w) {
+        const bool two = cc + 1 < w;
+        const bool fromdst = !first || moved[r - rb];
+        if (!fromdst && s.ident) {
+          v0 = (r == c0 + cc) ? T(1) : T(0);
+          v1 = (two && r == c0 + cc + 1) ? T(1) : T(0);
+        } else {
+          const T* p = (fromdst ? dst : src) + (int64_t)r * ld + cc;
+          if (two && (fromdst ? dvec : svec)) {
+            const P2 t = *reinterpret_cast<const P2*>(p);
+            v0 = t.x;
+            v1 = t.y;
+          } else {
+            v0 = p[0];
+            if (two) v1 = p[1];
+          }
+        }
       }
-      x = v;
     });
   };
-  const int r_first = k0 + NB;
-  Acc64<T> cur, nxt;
-  prefetch_a(0, r_first);
-  load_c(cur, r_first);
-  int buf = 0;
-  for (int r0 = r_first; r0 < n; r0 += 64) {
-    const bool more = r0 + 64 < n;
+  Acc cur, nxt;
+  prefetch_a(As0, rb);
+  load_c(cur, rb);
+  bool b1 = false;
+  for (int r0 = rb; r0 < re; r0 += 64) {
+    const bool more = r0 + 64 < re;
     if (more) {
-      prefetch_a(buf ^ 1, r0 + 64);
+      prefetch_a(b1 ? As0 : As1, r0 + 64);
       load_c(nxt, r0 + 64);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    cur.sub_mma(buf ? Tm : As, Us);
-    cur.each([&](int rr, int cc, T& x) {
+    cur.template sub_mma<AS, US>(b1 ? As1 : As0, Us);
+    cur.pairs([&](int rr, int cc, T& v0, T& v1) {
       const int r = r0 + rr;
-      if (r < n && cc < w) s.dst[(int64_t)r * s.ld + c0 + cc] = x;
+      if (r < re && cc < w) {
+        T* p = dst + (int64_t)r * ld + cc;
+        if (cc + 1 < w && dvec) {
+          *reinterpret_cast<P2*>(p) = make_pair2<T>(v0, v1);
+        } else {
+          p[0] = v0;
+          if (cc + 1 < w) p[1] = v1;
+        }
+      }
     });
     if (more) cur = nxt;
-    buf ^= 1;
-    __syncthreads();  // buffer `buf` is refilled by the next iteration's prefetch
+    b1 = !b1;
+    __syncthreads();  // the buffer just read is refilled by the next iteration's prefetch
   }
 }
 
@@ -726,38 +964,80 @@ __device__ __forceinline__ T* strip_base(const StepArgsT<T>& sa, const StepItem&
   return (it.kind == kSegRhs) ? sa.X + d.b_off : sa.inv + d.inv_off;
 }
 
-// k_back: X = U^-1 Y on a 64-column strip inside one window, blocks from the bottom.
-template <class T>
-__global__ void __launch_bounds__(UT)
-k_back(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
-  __shared__ T Ub[NB * LS];
+// Solve rows [lo, hi) of one strip in place: back substitution with U (UPPER,
+// 32-row blocks from the bottom) or forward substitution with the unit-lower
+// L (blocks from the top). After each diagonal block, the rest of the window
+// is updated with the block just solved. Strips of up to 8 columns solve a
+// diagonal block with one warp per column (lane i holds row i, the solved
+// value is broadcast by shuffle) and update row by row from shared memory;
+// wider strips use one thread per column and DMMA tiles.
+template <class T, bool UPPER>
+__device__ __forceinline__ void window_solve(const T* __restrict__ M, int n, T* X, int ld, int c0, int w, int lo,
+                                             int hi) {
+  __shared__ T Db[NB * LS];
   __shared__ T Xb[NB * WS];
   __shared__ T As[64 * LS];
-  const int tid = threadIdx.x;
-  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
-  const SysDesc d = step_desc(sa, it.sys);
-  if (!sa.solve_only && sa.scratch[d.pad_].info) return;
-  const int n = d.n, w = it.width, c0 = it.c0;
-  int lo, hi, ld;
-  if (!back_window(n, pass, lo, hi)) return;
-  const T* U = sa.LU + d.lu_off;
-  T* X = strip_base(sa, it, d, ld);
-  for (int kb0 = ((hi - 1) / NB) * NB; kb0 >= lo; kb0 -= NB) {
-    const int bw = min(NB, n - kb0);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const bool narrow = w <= 8;
+  const int nblk = (hi - lo + NB - 1) / NB;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int kb0 = UPPER ? lo + (nblk - 1 - bi) * NB : lo + bi * NB;
+    const int bw = min(NB, hi - kb0);
     for (int idx = tid; idx < NB * NB; idx += UT) {
       const int i = idx >> 5, q = idx & 31;
-      Ub[i * LS + q] = (i < bw && q < bw) ? U[(int64_t)(kb0 + i) * n + kb0 + q] : T(0);
+      Db[i * LS + q] = (i < bw && q < bw) ? M[(int64_t)(kb0 + i) * n + kb0 + q] : (i == q ? T(1) : T(0));
     }
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
       Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : T(0);
     }
     __syncthreads();
-    if (tid < w) {
-      for (int i = bw - 1; i >= 0; --i) {
-        T x = Xb[i * WS + tid];
-        for (int q = i + 1; q < bw; ++q) x = fma(-Ub[i * LS + q], Xb[q * WS + tid], x);
-        Xb[i * WS + tid] = x / Ub[i * LS + i];
+    if (narrow) {
+      if (warp < min(w, 4)) {
+        T u[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) u[j] = Db[lane * LS + j];
+        const bool two = warp + 4 < w;
+        T x0 = Xb[lane * WS + warp], x1 = two ? Xb[lane * WS + warp + 4] : T(0);
+        if constexpr (UPPER) {
+#pragma unroll
+          for (int j = NB - 1; j >= 0; --j) {
+            if (lane == j) {
+              x0 = x0 / u[j];
+              x1 = x1 / u[j];
+            }
+            const T y0 = __shfl_sync(0xffffffffu, x0, j), y1 = __shfl_sync(0xffffffffu, x1, j);
+            if (lane < j) {
+              x0 = fma(-u[j], y0, x0);
+              x1 = fma(-u[j], y1, x1);
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NB; ++j) {
+            const T y0 = __shfl_sync(0xffffffffu, x0, j), y1 = __shfl_sync(0xffffffffu, x1, j);
+            if (lane > j) {
+              x0 = fma(-u[j], y0, x0);
+              x1 = fma(-u[j], y1, x1);
+            }
+          }
+        }
+        Xb[lane * WS + warp] = x0;
+        if (two) Xb[lane * WS + warp + 4] = x1;
+      }
+    } else if (tid < w) {
+      if constexpr (UPPER) {
+        for (int i = bw - 1; i >= 0; --i) {
+          T x = Xb[i * WS + tid];
+          for (int q = i + 1; q < bw; ++q) x = fma(-Db[i * LS + q], Xb[q * WS + tid], x);
+          Xb[i * WS + tid] = x / Db[i * LS + i];
+        }
+      } else {
+        for (int i = 1; i < bw; ++i) {
+          T x = Xb[i * WS + tid];
+          for (int q = 0; q < i; ++q) x = fma(-Db[i * LS + q], Xb[q * WS + tid], x);
+          Xb[i * WS + tid] = x;
+        }
       }
     }
     __syncthreads();
@@ -765,18 +1045,45 @@ k_back(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
       const int i = idx >> 6, c = idx & 63;
       if (i < bw && c < w) X[(int64_t)(kb0 + i) * ld + c0 + c] = Xb[i * WS + c];
     }
-    for (int r0 = lo; r0 < kb0; r0 += 64) {
+    // the rest of the window: above the block (UPPER) or below it
+    const int r_lo = UPPER ? lo : kb0 + bw, r_hi = UPPER ? kb0 : hi;
+    for (int r0 = r_lo; r0 < r_hi; r0 += 64) {
       for (int idx = tid; idx < 64 * NB; idx += UT) {
         const int i = idx >> 5, q = idx & 31;
-        As[i * LS + q] = (r0 + i < kb0 && q < bw) ? U[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
+        As[i * LS + q] = (r0 + i < r_hi && q < bw) ? M[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
       }
       __syncthreads();
-      tile_update<T>(
-          As, Xb, r0, kb0, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
-          [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
+      if (narrow) {
+        for (int p = tid; p < 64 * w; p += UT) {
+          const int r = p / w, c = p - r * w;
+          if (r0 + r < r_hi) {
+            T acc = T(0);
+#pragma unroll 8
+            for (int j = 0; j < NB; ++j) acc = fma(As[r * LS + j], Xb[j * WS + c], acc);
+            X[(int64_t)(r0 + r) * ld + c0 + c] -= acc;
+          }
+        }
+      } else {
+        tile_update<T>(
+            As, Xb, r0, r_hi, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
+            [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
+      }
       __syncthreads();
     }
   }
+}
+
+// k_back: X = U^-1 Y on a strip, the window of this pass.
+template <class T>
+__global__ void __launch_bounds__(UT)
+k_back(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
+  if (!sa.solve_only && sa.scratch[d.pad_].info) return;
+  int lo, hi, ld;
+  if (!back_window(d.n, pass, lo, hi)) return;
+  T* X = strip_base(sa, it, d, ld);
+  window_solve<T, true>(sa.LU + d.lu_off, d.n, X, ld, it.c0, it.width, lo, hi);
 }
 
 // X[r0 .. r0+63] -= M[r0 .. r0+63, lo:hi] X[lo:hi] on one strip (rows < rend):
@@ -787,6 +1094,47 @@ __device__ __forceinline__ void window_apply(const T* __restrict__ M, int n, T* 
   __shared__ T As[64 * LS];
   __shared__ T Bs[NB * WS];
   const int tid = threadIdx.x;
+  if (w <= 8) {
+    // few columns: one warp per row, the row of M read coalesced, the window's
+    // solved values from shared memory
+    const int lane = tid & 31, warp = tid >> 5, kw = hi - lo;
+    T* xs = As;  // kw x w  (kw <= SB: 256 x 8 <= 64 x LS elements)
+    for (int idx = tid; idx < kw * w; idx += UT) {
+      const int j = idx / w, c = idx - j * w;
+      xs[idx] = X[(int64_t)(lo + j) * ld + c0 + c];
+    }
+    __syncthreads();
+    for (int rr = warp; rr < 64; rr += UT / 32) {
+      const int r = r0 + rr;
+      if (r >= rend) break;
+      const T* mr = M + (int64_t)r * n + lo;
+      T acc[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) acc[c] = T(0);
+#pragma unroll
+      for (int j0 = 0; j0 < SB; j0 += 32) {
+        const int j = j0 + lane;
+        if (j < kw) {
+          const T m = mr[j];
+#pragma unroll
+          for (int c = 0; c < 8; ++c)
+            if (c < w) acc[c] = fma(m, xs[j * w + c], acc[c]);
+        }
+      }
+      T mine = T(0);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        if (c < w) {
+          T v = acc[c];
+#pragma unroll
+          for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == c) mine = v;
+        }
+      }
+      if (lane < w) X[(int64_t)r * ld + c0 + lane] -= mine;
+    }
+    return;
+  }
   Acc64<T> acc;
   acc.each([&](int r, int cc, T& x) { x = (r0 + r < rend && cc < w) ? X[(int64_t)(r0 + r) * ld + c0 + cc] : T(0); });
   for (int kc = lo; kc < hi; kc += NB) {
@@ -856,52 +1204,11 @@ k_permute(StepArgsT<T> sa, const StepItem* __restrict__ items) {
 template <class T>
 __global__ void __launch_bounds__(UT)
 k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
-  __shared__ T Lb[NB * LS];
-  __shared__ T Xb[NB * WS];
-  __shared__ T As[64 * LS];
-  const int tid = threadIdx.x;
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
-  const int n = d.n, w = it.width, c0 = it.c0, ld = d.nrhs;
   int lo, hi;
-  if (!forward_window(n, pass, lo, hi)) return;
-  const T* L = sa.LU + d.lu_off;
-  T* X = sa.X + d.b_off;
-  for (int kb0 = lo; kb0 < hi; kb0 += NB) {
-    const int bw = min(NB, n - kb0), kb1 = kb0 + bw;
-    for (int idx = tid; idx < NB * NB; idx += UT) {
-      const int i = idx >> 5, q = idx & 31;
-      Lb[i * LS + q] = (i < bw && q < bw) ? L[(int64_t)(kb0 + i) * n + kb0 + q] : T(0);
-    }
-    for (int idx = tid; idx < NB * 64; idx += UT) {
-      const int i = idx >> 6, c = idx & 63;
-      Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : T(0);
-    }
-    __syncthreads();
-    if (tid < w) {
-      for (int i = 1; i < bw; ++i) {
-        T x = Xb[i * WS + tid];
-        for (int q = 0; q < i; ++q) x = fma(-Lb[i * LS + q], Xb[q * WS + tid], x);
-        Xb[i * WS + tid] = x;
-      }
-    }
-    __syncthreads();
-    for (int idx = tid; idx < NB * 64; idx += UT) {
-      const int i = idx >> 6, c = idx & 63;
-      if (i < bw && c < w) X[(int64_t)(kb0 + i) * ld + c0 + c] = Xb[i * WS + c];
-    }
-    for (int r0 = kb1; r0 < hi; r0 += 64) {
-      for (int idx = tid; idx < 64 * NB; idx += UT) {
-        const int i = idx >> 5, q = idx & 31;
-        As[i * LS + q] = (r0 + i < hi && q < bw) ? L[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
-      }
-      __syncthreads();
-      tile_update<T>(
-          As, Xb, r0, hi, w, [&](int r, int cc) { return X[(int64_t)r * ld + c0 + cc]; },
-          [&](int r, int cc, T v) { X[(int64_t)r * ld + c0 + cc] = v; });
-      __syncthreads();
-    }
-  }
+  if (!forward_window(d.n, pass, lo, hi)) return;
+  window_solve<T, false>(sa.LU + d.lu_off, d.n, sa.X + d.b_off, d.nrhs, it.c0, it.width, lo, hi);
 }
 
 // Rows below the window of this pass: one CTA per (strip, 64-row tile = blockIdx.y).
@@ -917,14 +1224,10 @@ k_forward_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) 
   window_apply<T>(sa.LU + d.lu_off, d.n, sa.X + d.b_off, d.nrhs, it.c0, it.width, r0, d.n, lo, hi);
 }
 
-template <class T>
-size_t update_smem(int nmax) {
-  return sizeof(T) * (2 * NB * WS + 2 * 64 * LS) + sizeof(int) * (3 * NB + (size_t)nmax);
-}
-template <class T>
-cudaError_t prepare_t() {
-  return cudaFuncSetAttribute(k_update<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)update_smem<T>(kStepMaxN));
+template <class T, int MODE>
+cudaError_t prepare_update() {
+  return cudaFuncSetAttribute(k_update<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)update_smem<T, MODE>());
 }
 
 // Passes over windows of SB rows; between two windows, the solved one is
@@ -954,9 +1257,11 @@ cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, 
 }  // namespace
 
 cudaError_t step_prepare() {
-  cudaError_t e = prepare_t<double>();
-  if (e != cudaSuccess) return e;
-  return prepare_t<float>();
+  cudaError_t e = prepare_update<double, kUpdFp32>();
+  if (e == cudaSuccess) e = prepare_update<float, kUpdFp32>();
+  if (e == cudaSuccess) e = prepare_update<float, kUpdTf32>();
+  if (e == cudaSuccess) e = prepare_update<float, kUpdBf16>();
+  return e;
 }
 
 template <class T, int CS>
@@ -995,7 +1300,22 @@ template <class T>
 cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  k_update<T><<<nitems, UT, update_smem<T>(nmax), st>>>(sa, items, k0);
+  k_rows<T><<<nitems, UT, 0, st>>>(sa, items, k0);
+  cudaError_t e = cudaGetLastError();
+  const int below = nmax - k0 - NB;
+  if (e != cudaSuccess || below <= 0) return e;
+  const dim3 grid((unsigned)nitems, (unsigned)((below + RG - 1) / RG));
+  if constexpr (std::is_same_v<T, float>) {
+    if (sa.umode == kUpdTf32) {
+      k_update<T, kUpdTf32><<<grid, UT, update_smem<T, kUpdTf32>(), st>>>(sa, items, k0);
+      return cudaGetLastError();
+    }
+    if (sa.umode == kUpdBf16) {
+      k_update<T, kUpdBf16><<<grid, UT, update_smem<T, kUpdBf16>(), st>>>(sa, items, k0);
+      return cudaGetLastError();
+    }
+  }
+  k_update<T, kUpdFp32><<<grid, UT, update_smem<T, kUpdFp32>(), st>>>(sa, items, k0);
   return cudaGetLastError();
 }
 

@@ -4,7 +4,8 @@
 // src/linalg/linalg.cpp:92-103). For a uniform batch of order n:
 //  1. equilibrate: power-of-two row/column scales, the scaled matrix in FP32;
 //  2. factor in FP32 on the step-wise kernels (pivots and row moves kept),
-//     the first solution riding along as augmented columns;
+//     the first solution riding along as augmented columns; the trailing
+//     products in FP32, or on the tensor cores from TF32 / BF16 operands;
 //  3. refine in FP64: R = B - A X, eta = normwise backward error; systems with
 //     eta <= tol stop, systems whose eta no longer halves are marked stalled;
 //     the others solve A d = R with the FP32 factors and add d in FP64;
@@ -43,6 +44,11 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
           double* dFerr, int32_t* dIters, int32_t* dFallback, cudaStream_t st) {
   if (count64 < 0 || n < 0 || nrhs < 0 || max_iter < 0 || !(tol >= 0.0)) {
     set_error("negative count, order, nrhs or max_iter, or bad tolerance");
+    return NPPB_E_ARG;
+  }
+  if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16)) ||
+      ((flags & NPPB_MIXED_TF32) && (flags & NPPB_MIXED_BF16))) {
+    set_error("unknown mixed flag bits, or both TF32 and BF16");
     return NPPB_E_ARG;
   }
   if (n > kMixedMaxN || count64 > INT32_MAX) {
@@ -93,6 +99,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     sa.un = n;
     sa.unrhs = nrhs;
     sa.uleft = 1;
+    sa.umode = (flags & NPPB_MIXED_BF16) ? 2 : (flags & NPPB_MIXED_TF32) ? 1 : 0;
     NPPB_CUDA(run_step_uniform<float>(sa, count, st), "FP32 factorisation");
     NPPB_CUDA(mixed_mark_fp32_failures(info32.as<int32_t>(), S, count, st), "mark");
     NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 1, st), "apply");

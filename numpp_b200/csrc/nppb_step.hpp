@@ -60,6 +60,7 @@ struct StepArgsT {
   // scratch slot s; an inverse for every system when uinv != 0.
   int un, unrhs, uinv;
   int uleft;         // uniform batch keeps its factors: carry row moves left of each panel
+  int umode;         // FP32 factors: trailing product in FP32 (0), TF32 (1) or BF16 (2) tensor-core arithmetic
 };
 using StepArgs = StepArgsT<double>;
 

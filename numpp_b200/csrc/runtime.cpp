@@ -63,6 +63,14 @@ const Device* device() {
       d.cc_major = p.major;
       d.cc_minor = p.minor;
       t.probed[cur] = prepare_kernels() == cudaSuccess ? 1 : -1;
+      // workspaces come from this process's default stream-ordered pool: keep
+      // freed blocks in the pool instead of returning them at every synchronise
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, cur) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      cudaGetLastError();
     }
   }
   if (t.probed[cur] != 1) {

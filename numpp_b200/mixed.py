@@ -7,10 +7,15 @@ from . import _lib
 from .linalg import _check
 
 
+_FACTOR = {"fp32": 0, "tf32": _lib.MIXED_TF32, "bf16": _lib.MIXED_BF16}
+
+
 def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equilibrate: bool = True,
-                fallback: bool = True):
+                fallback: bool = True, factor: str = "fp32"):
     """X for a (count, n, n) / (count, n, nrhs) float64 batch; returns
-    (X, report) with report = dict(berr, ferr, iters, fallback, info) per system."""
+    (X, report) with report = dict(berr, ferr, iters, fallback, info) per system.
+    factor: arithmetic of the factorisation's trailing products ("fp32",
+    "tf32" or "bf16" tensor cores; FP32 panels and stored factors)."""
     L = _lib.load()
     A = np.ascontiguousarray(A, np.float64)
     B = np.ascontiguousarray(B, np.float64)
@@ -22,7 +27,8 @@ def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equil
     iters = np.zeros(cnt, np.int32)
     fb = np.zeros(cnt, np.int32)
     Xt = None if X_true is None else np.ascontiguousarray(X_true, np.float64)
-    flags = (0 if equilibrate else _lib.MIXED_NO_EQUILIBRATE) | (0 if fallback else _lib.MIXED_NO_FALLBACK)
+    flags = ((0 if equilibrate else _lib.MIXED_NO_EQUILIBRATE) | (0 if fallback else _lib.MIXED_NO_FALLBACK)
+             | _FACTOR[factor])
     P = _lib.ptr
     _check(L.nppb_solve_mixed_batched(cnt, n, k, P(A), P(B), P(X), P(Xt), tol, max_iter, flags, P(info),
                                       P(berr), P(ferr), P(iters), P(fb)))

@@ -72,3 +72,23 @@ def test_small_orders_take_the_fp64_kernel(lib, oracle):
     assert np.all(rep["fallback"] == 1) and np.all(rep["berr"] <= 1e-14)
     Xo, _ = oracle.solve(A, B)
     np.testing.assert_allclose(X, Xo, rtol=1e-12, atol=1e-13)
+
+
+@pytest.mark.parametrize("factor,kappa", [("tf32", 1e2), ("tf32", 1e3), ("bf16", 1e1)])
+def test_tensor_core_factors_refine(lib, oracle, factor, kappa):
+    """TF32 / BF16 trailing products: rougher factors, more corrections, same bar."""
+    A, B, Xt = workloads.conditioned_batch(seed=40 + int(np.log10(kappa)), count=6, n=256, kappa=kappa, nrhs=4)
+    X, rep = solve_mixed(A, B, X_true=Xt, factor=factor, max_iter=30)
+    assert np.all(rep["berr"] <= 1e-10), rep["berr"]
+    assert np.all(rep["fallback"] == 0), rep
+    Xo, _ = oracle.solve(A, B)
+    rel = np.abs(X - Xo).max(axis=(1, 2)) / np.abs(Xo).max(axis=(1, 2))
+    assert np.all(rel <= 10 * kappa * 1e-10 + kappa * 1e-13), rel
+
+
+def test_bf16_factors_fall_back_when_too_rough(lib):
+    """kappa * u_bf16 >> 1: refinement cannot contract; every system still meets the bar via FP64."""
+    A, B, Xt = workloads.conditioned_batch(seed=44, count=4, n=128, kappa=1e6, nrhs=1)
+    X, rep = solve_mixed(A, B, X_true=Xt, factor="bf16")
+    assert np.all(rep["berr"] <= 1e-10), rep["berr"]
+    assert np.all(rep["fallback"] == 1)
