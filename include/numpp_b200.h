@@ -151,15 +151,18 @@ int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const d
  * info (of the FP64 solve, when it ran). Orders <= 32 always take the FP64
  * warp kernel (fallback = 1). The device form synchronises `stream` (it reads
  * convergence counts back between corrections).
- * NPPB_MIXED_TF32 / NPPB_MIXED_BF16: the trailing products of the FP32
- * factorisation run on the tensor cores with operands rounded to TF32 / BF16
- * (FP32 accumulation); the panels, the stored factors and the correction
- * solves stay FP32. */
+ * Trailing products of the FP32 factorisation: by default on the tensor
+ * cores as error-compensated TF32 (each operand split into two TF32 parts,
+ * three products: close to FP32 accuracy); NPPB_MIXED_TF32 / NPPB_MIXED_BF16:
+ * one tensor-core product from operands rounded to TF32 / BF16;
+ * NPPB_MIXED_FP32_FMA: FP32 fused multiply-adds. FP32 accumulation in every
+ * case; the panels, the stored factors and the correction solves stay FP32. */
 enum {
   NPPB_MIXED_NO_EQUILIBRATE = 1,
   NPPB_MIXED_NO_FALLBACK = 2,
   NPPB_MIXED_TF32 = 4,
-  NPPB_MIXED_BF16 = 8
+  NPPB_MIXED_BF16 = 8,
+  NPPB_MIXED_FP32_FMA = 16
 };
 int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                const double* dB, double* dX, const double* dXtrue, double tol,

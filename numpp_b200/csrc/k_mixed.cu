@@ -152,19 +152,22 @@ k_apply(double* __restrict__ X, const float* __restrict__ Y, const double* __res
 }
 
 // One CTA per (system, kMixedRows rows of A): R = B - A X for those rows,
-// right-hand sides in chunks of RC, X staged through shared memory in blocks
-// of CB rows; each warp keeps kMixedRows / 8 rows' sums in registers and reads
-// its rows of A coalesced. max |R| (and, by the first CTA, max |X|) go to the
-// system's running maxima; k_refine_decide turns them into eta.
-constexpr int RC = 8;
-constexpr int CB = 512;
+// right-hand sides in chunks of RC (1, 2, 4 or 8: the smallest power of two
+// covering nrhs, at most 8), X staged through shared memory in blocks of
+// XS / RC rows; each warp keeps kMixedRows / 8 rows' sums in registers and
+// reads its rows of A coalesced. max |R| (and, by the first CTA, max |X|) go
+// to the system's running maxima; k_refine_decide turns them into eta. With
+// rpos, row i of the scaled residual is stored at row rpos[i] (pivoted order).
+constexpr int XS = 4096;                    // doubles of X staged per block
 constexpr int RW = kMixedRows / (MT / 32);  // rows per warp
 
+template <int RC>
 __global__ void __launch_bounds__(MT)
 k_residual(const double* __restrict__ A, const double* __restrict__ B, const double* __restrict__ X,
            int n, int nrhs, const double* __restrict__ rs, float* __restrict__ R32,
-           RefineState* __restrict__ st, int only_active) {
-  __shared__ double xs[CB * RC];
+           const int32_t* __restrict__ rpos, RefineState* __restrict__ st, int only_active) {
+  constexpr int CB = XS / RC;
+  __shared__ double xs[XS];
   __shared__ double red[MT / 32];
   __shared__ double ax_s[MT / 32][RW][RC];
   const int s = blockIdx.x, r0 = blockIdx.y * kMixedRows;
@@ -197,8 +200,10 @@ k_residual(const double* __restrict__ A, const double* __restrict__ B, const dou
       for (int q = 0; q < RW; ++q) {
         const int i = r0 + warp * RW + q;
         if (i < n) {
+          const double* ai = a + (int64_t)i * n + j0;
+#pragma unroll 4
           for (int j = lane; j < jn; j += 32) {
-            const double aij = a[(int64_t)i * n + j0 + j];
+            const double aij = ai[j];
 #pragma unroll
             for (int k = 0; k < RC; ++k) acc[q][k] = fma(aij, xs[j * RC + k], acc[q][k]);
           }
@@ -222,7 +227,10 @@ k_residual(const double* __restrict__ A, const double* __restrict__ B, const dou
       if (i < n && k < kc) {
         const double r = b[(int64_t)i * nrhs + k0 + k] - ax_s[warp][q][k];
         rmax = fmax(rmax, fabs(r));
-        if (R32) R32[(int64_t)s * nb + (int64_t)i * nrhs + k0 + k] = (float)(rs[(int64_t)s * n + i] * r);
+        if (R32) {
+          const int p = rpos ? rpos[(int64_t)s * n + i] : i;
+          R32[(int64_t)s * nb + (int64_t)p * nrhs + k0 + k] = (float)(rs[(int64_t)s * n + i] * r);
+        }
       }
     }
     __syncwarp();
@@ -278,6 +286,30 @@ k_ferr(const double* __restrict__ X, const double* __restrict__ Xt, int n, int n
   if (threadIdx.x == 0) ferr[s] = m > 0.0 ? d / m : d;
 }
 
+// Position of every row in the pivoted order (the inverse of the row
+// permutation a swap list applies), one CTA per system: the swaps are
+// replayed serially from shared memory.
+__global__ void __launch_bounds__(MT)
+k_row_positions(const int32_t* __restrict__ ipiv, int n, int32_t* __restrict__ rpos) {
+  extern __shared__ int prm[];  // perm, then the swap list
+  int* piv = prm + n;
+  const int s = blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += MT) {
+    prm[i] = i;
+    piv[i] = ipiv[(int64_t)s * n + i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < n; ++k) {
+      int p = piv[k];
+      if (p < k || p >= n) p = k;
+      const int t = prm[k]; prm[k] = prm[p]; prm[p] = t;
+    }
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < n; q += MT) rpos[(int64_t)s * n + prm[q]] = q;
+}
+
 __global__ void k_mark_fp32_failures(const int32_t* __restrict__ info32, RefineState* __restrict__ st, int count) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < count && info32[s]) st[s].status = kRefineStalled;
@@ -305,10 +337,13 @@ cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, 
   return cudaGetLastError();
 }
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
-                           const double* rs, float* R32, RefineState* st, double tol, int iter, int decide,
-                           int* active, cudaStream_t s) {
+                           const double* rs, float* R32, const int32_t* rpos, RefineState* st, double tol,
+                           int iter, int decide, int* active, cudaStream_t s) {
   const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
-  k_residual<<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, st, decide);
+  if (nrhs == 1) k_residual<1><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
+  else if (nrhs == 2) k_residual<2><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
+  else if (nrhs <= 4) k_residual<4><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
+  else k_residual<8><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_refine_decide<<<(count + 255) / 256, 256, 0, s>>>(st, count, tol, iter, decide, active);
@@ -317,6 +352,10 @@ cudaError_t mixed_residual(const double* A, const double* B, const double* X, in
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,
                        cudaStream_t s) {
   k_ferr<<<count, MT, 0, s>>>(X, Xt, n, nrhs, ferr);
+  return cudaGetLastError();
+}
+cudaError_t mixed_row_positions(const int32_t* ipiv, int count, int n, int32_t* rpos, cudaStream_t s) {
+  k_row_positions<<<count, MT, 2 * sizeof(int) * (size_t)n, s>>>(ipiv, n, rpos);
   return cudaGetLastError();
 }
 cudaError_t mixed_mark_fp32_failures(const int32_t* info32, RefineState* st, int count, cudaStream_t s) {

@@ -603,7 +603,12 @@ template <> struct Acc32<float> {  // 4 x 4 elements per thread
 // rounded to TF32 (mma.m16n8k8) or BF16 (mma.m16n8k16), FP32 accumulation.
 // Same 64 x 64 tile and 2 x 2 warp split as Acc64; a warp holds 2 x 4
 // m16n8 accumulators.
-enum : int { kUpdFp32 = 0, kUpdTf32 = 1, kUpdBf16 = 2 };
+// kUpd3xTf32: each FP32 operand split as x = hi + lo with hi = tf32(x) and
+// lo = tf32(x - hi), the product taken as hi*hi + hi*lo + lo*hi (three
+// tensor-core products, the lo*lo term dropped): close to FP32 accuracy at
+// tensor-core speed (the error-compensated TF32 scheme of Ootomo and Yokota,
+// 2022, and of CUTLASS's 3xTF32 kernels).
+enum : int { kUpdFp32 = 0, kUpdTf32 = 1, kUpdBf16 = 2, kUpd3xTf32 = 3 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
@@ -630,10 +635,52 @@ struct AccTC {
         f(wm + mi * 16 + g + 8, wn + ni * 8 + 2 * tq, v[mi][ni][2], v[mi][ni][3]);
       }
   }
+  __device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+  }
   template <int AST, int BST>
   __device__ __forceinline__ void sub_mma(const float* As, const float* Bs) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, g = lane >> 2, tq = lane & 3;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    if constexpr (MODE == kUpd3xTf32) {
+#pragma unroll
+      for (int kk = 0; kk < NB; kk += 8) {
+        uint32_t ah[2][4], al[2][4], bh[4][2], bl[4][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          const float* r0 = As + (wm + mi * 16 + g) * AST + kk + tq;
+          const float* r1 = r0 + 8 * AST;
+          const float x[4] = {-r0[0], -r1[0], -r0[4], -r1[4]};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            ah[mi][e] = to_tf32(x[e]);
+            al[mi][e] = to_tf32(x[e] - __uint_as_float(ah[mi][e]));
+          }
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          const float* c = Bs + (kk + tq) * BST + wn + ni * 8 + g;
+          const float y[2] = {c[0], c[4 * BST]};
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            bh[ni][e] = to_tf32(y[e]);
+            bl[ni][e] = to_tf32(y[e] - __uint_as_float(bh[ni][e]));
+          }
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) {
+            mma_tf32(v[mi][ni], al[mi], bh[ni]);  // small terms first
+            mma_tf32(v[mi][ni], ah[mi], bl[ni]);
+            mma_tf32(v[mi][ni], ah[mi], bh[ni]);
+          }
+      }
+    } else
     if constexpr (MODE == kUpdTf32) {
 #pragma unroll
       for (int kk = 0; kk < NB; kk += 8) {
@@ -703,6 +750,7 @@ struct AccTC {
 template <class T, int MODE> struct AccSel { using type = Acc64<T>; };
 template <> struct AccSel<float, kUpdTf32> { using type = AccTC<kUpdTf32>; };
 template <> struct AccSel<float, kUpdBf16> { using type = AccTC<kUpdBf16>; };
+template <> struct AccSel<float, kUpd3xTf32> { using type = AccTC<kUpd3xTf32>; };
 
 // C[rows r0.., 64 cols] -= As * Bs for rows [r0, rend), columns < w, one tile.
 template <class T, class Load, class Store>
@@ -792,6 +840,10 @@ template <> struct TileCfg<float, kUpdFp32> {
 template <> struct TileCfg<float, kUpdTf32> {
   static constexpr int AS = 36;  // banks 4g + tq
   static constexpr int US = 72;  // banks 8tq + g
+};
+template <> struct TileCfg<float, kUpd3xTf32> {
+  static constexpr int AS = 36;
+  static constexpr int US = 72;
 };
 template <> struct TileCfg<float, kUpdBf16> {
   static constexpr int AS = 40;  // 8-byte reads: banks 8g + 2tq
@@ -946,15 +998,15 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
 // substitution takes window jw = (n-1)/SB - pass (from the bottom), forward
 // substitution window jw = pass (from the top); a system without that window
 // skips the pass.
-__device__ __forceinline__ bool back_window(int n, int pass, int& lo, int& hi) {
-  const int jw = (n - 1) / SB - pass;
-  lo = jw * SB;
-  hi = min(n, lo + SB);
+__device__ __forceinline__ bool back_window(int n, int pass, int& lo, int& hi, int sb = SB) {
+  const int jw = (n - 1) / sb - pass;
+  lo = jw * sb;
+  hi = min(n, lo + sb);
   return jw >= 0;
 }
-__device__ __forceinline__ bool forward_window(int n, int pass, int& lo, int& hi) {
-  lo = pass * SB;
-  hi = min(n, lo + SB);
+__device__ __forceinline__ bool forward_window(int n, int pass, int& lo, int& hi, int sb = SB) {
+  lo = pass * sb;
+  hi = min(n, lo + sb);
   return lo < n;
 }
 
@@ -1095,43 +1147,47 @@ __device__ __forceinline__ void window_apply(const T* __restrict__ M, int n, T* 
   __shared__ T Bs[NB * WS];
   const int tid = threadIdx.x;
   if (w <= 8) {
-    // few columns: one warp per row, the row of M read coalesced, the window's
-    // solved values from shared memory
+    // few columns: a warp takes 4 rows at a time, each row of M read
+    // coalesced through the read-only path (all 4 rows' loads in flight
+    // together), the window's solved values from shared memory
+    constexpr int RPW = 4, JT = SB / 32;
     const int lane = tid & 31, warp = tid >> 5, kw = hi - lo;
-    T* xs = As;  // kw x w  (kw <= SB: 256 x 8 <= 64 x LS elements)
-    for (int idx = tid; idx < kw * w; idx += UT) {
+    T* xs = As;  // SB x w, zero past kw  (256 x 8 <= 64 x LS elements)
+    for (int idx = tid; idx < SB * w; idx += UT) {
       const int j = idx / w, c = idx - j * w;
-      xs[idx] = X[(int64_t)(lo + j) * ld + c0 + c];
+      xs[idx] = j < kw ? X[(int64_t)(lo + j) * ld + c0 + c] : T(0);
     }
     __syncthreads();
-    for (int rr = warp; rr < 64; rr += UT / 32) {
-      const int r = r0 + rr;
-      if (r >= rend) break;
-      const T* mr = M + (int64_t)r * n + lo;
-      T acc[8];
+    for (int g0 = warp * RPW; g0 < 64; g0 += (UT / 32) * RPW) {
+      if (r0 + g0 >= rend) break;
+      T m[RPW][JT];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) acc[c] = T(0);
+      for (int q = 0; q < RPW; ++q) {
+        const int r = r0 + g0 + q;
+        const T* mr = M + (int64_t)min(r, rend - 1) * n + lo;
 #pragma unroll
-      for (int j0 = 0; j0 < SB; j0 += 32) {
-        const int j = j0 + lane;
-        if (j < kw) {
-          const T m = mr[j];
-#pragma unroll
-          for (int c = 0; c < 8; ++c)
-            if (c < w) acc[c] = fma(m, xs[j * w + c], acc[c]);
+        for (int t = 0; t < JT; ++t) {
+          const int j = t * 32 + lane;
+          m[q][t] = (r < rend && j < kw) ? __ldg(mr + j) : T(0);
         }
       }
-      T mine = T(0);
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {
-        if (c < w) {
-          T v = acc[c];
+      for (int q = 0; q < RPW; ++q) {
+        T mine = T(0);
 #pragma unroll
-          for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          if (lane == c) mine = v;
+        for (int c = 0; c < 8; ++c) {
+          if (c < w) {
+            T v = T(0);
+#pragma unroll
+            for (int t = 0; t < JT; ++t) v = fma(m[q][t], xs[(t * 32 + lane) * w + c], v);
+#pragma unroll
+            for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == c) mine = v;
+          }
         }
+        const int r = r0 + g0 + q;
+        if (r < rend && lane < w) X[(int64_t)r * ld + c0 + lane] -= mine;
       }
-      if (lane < w) X[(int64_t)r * ld + c0 + lane] -= mine;
     }
     return;
   }
@@ -1159,12 +1215,12 @@ __device__ __forceinline__ void window_apply(const T* __restrict__ M, int n, T* 
 // Rows above the window of this pass: one CTA per (strip, 64-row tile = blockIdx.y).
 template <class T>
 __global__ void __launch_bounds__(UT)
-k_back_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+k_back_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass, int sb) {
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
   if (!sa.solve_only && sa.scratch[d.pad_].info) return;
   int lo, hi, ld;
-  if (!back_window(d.n, pass, lo, hi)) return;
+  if (!back_window(d.n, pass, lo, hi, sb)) return;
   const int r0 = (int)blockIdx.y * 64;
   if (r0 >= lo) return;
   T* X = strip_base(sa, it, d, ld);
@@ -1185,11 +1241,15 @@ k_permute(StepArgsT<T> sa, const StepItem* __restrict__ items) {
   const int32_t* ipiv = sa.ipiv + d.piv_off;
   const T* B = sa.B + d.b_off;
   T* X = sa.X + d.b_off;
-  for (int i = tid; i < n; i += UT) perm[i] = i;
+  int* piv = perm + n;
+  for (int i = tid; i < n; i += UT) {
+    perm[i] = i;
+    piv[i] = ipiv[i];
+  }
   __syncthreads();
   if (tid == 0) {
     for (int k = 0; k < n; ++k) {
-      int p = ipiv[k];
+      int p = piv[k];
       if (p < k || p >= n) p = k;  // a swap list only names rows >= k
       const int t = perm[k]; perm[k] = perm[p]; perm[p] = t;
     }
@@ -1211,14 +1271,119 @@ k_forward(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
   window_solve<T, false>(sa.LU + d.lu_off, d.n, sa.X + d.b_off, d.nrhs, it.c0, it.width, lo, hi);
 }
 
+// Strips of at most 8 columns (few right-hand sides): the whole window of M
+// (SBN x SBN) is staged into shared memory once, then the window is solved
+// from shared memory: each 32-row diagonal block by one warp per column
+// (lane i holds row i; the solved value is broadcast by shuffle), the rest of
+// the window by one warp per row. UPPER: back substitution with U from the
+// bottom; else forward substitution with the unit-lower L from the top.
+constexpr int SBN = 128;
+constexpr int MSN = SBN + 2;  // row stride of the staged window (16-byte rows)
+
+template <class T>
+size_t narrow_smem() {
+  return sizeof(T) * ((size_t)SBN * MSN + 8 * SBN);
+}
+
+template <class T, bool UPPER>
+__global__ void __launch_bounds__(UT)
+k_tri_narrow(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+  extern __shared__ __align__(16) unsigned char tri_raw[];
+  T* Ms = reinterpret_cast<T*>(tri_raw);  // window of M, stride MSN
+  T* xt = Ms + SBN * MSN;                 // window of X, column-major: xt[c * SBN + row]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
+  const SysDesc d = step_desc(sa, it.sys);
+  if (UPPER && !sa.solve_only && sa.scratch[d.pad_].info) return;
+  const int n = d.n;
+  int lo, hi;
+  if (!(UPPER ? back_window(n, pass, lo, hi, SBN) : forward_window(n, pass, lo, hi, SBN))) return;
+  int ld;
+  T* X;
+  if constexpr (UPPER) {
+    X = strip_base(sa, it, d, ld);
+  } else {
+    X = sa.X + d.b_off;
+    ld = d.nrhs;
+  }
+  const int kw = hi - lo, w = it.width, c0 = it.c0;
+  const T* M = sa.LU + d.lu_off + (int64_t)lo * n + lo;
+  async_tile<T>(Ms, MSN, M, n, kw, kw, SBN, SBN, pair_aligned(M, n));
+  for (int idx = tid; idx < 8 * SBN; idx += UT) {
+    const int c = idx / SBN, j = idx - c * SBN;
+    xt[idx] = (c < w && j < kw) ? X[(int64_t)(lo + j) * ld + c0 + c] : T(0);
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+  const int nblk = (kw + NB - 1) / NB;
+  for (int bi = 0; bi < nblk; ++bi) {
+    const int b0 = UPPER ? (nblk - 1 - bi) * NB : bi * NB;  // window-relative
+    const int bw = min(NB, kw - b0);
+    if (warp < min(w, 4)) {
+      const bool two = warp + 4 < w, in = lane < bw;
+      T u[NB];
+#pragma unroll
+      for (int j = 0; j < NB; ++j) u[j] = (in && j < bw) ? Ms[(b0 + lane) * MSN + b0 + j] : (lane == j ? T(1) : T(0));
+      T* x0p = xt + warp * SBN + b0;
+      T* x1p = xt + (warp + 4) * SBN + b0;
+      T x0 = in ? x0p[lane] : T(0), x1 = (in && two) ? x1p[lane] : T(0);
+      if constexpr (UPPER) {
+        // every lane takes the reciprocal of its own diagonal entry up front
+        const T rd = T(1) / (in ? Ms[(b0 + lane) * MSN + b0 + lane] : T(1));
+#pragma unroll
+        for (int j = NB - 1; j >= 0; --j) {
+          if (lane == j) {
+            x0 *= rd;
+            x1 *= rd;
+          }
+          const T y0 = __shfl_sync(0xffffffffu, x0, j), y1 = __shfl_sync(0xffffffffu, x1, j);
+          if (lane < j) {
+            x0 = fma(-u[j], y0, x0);
+            x1 = fma(-u[j], y1, x1);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+          const T y0 = __shfl_sync(0xffffffffu, x0, j), y1 = __shfl_sync(0xffffffffu, x1, j);
+          if (lane > j) {
+            x0 = fma(-u[j], y0, x0);
+            x1 = fma(-u[j], y1, x1);
+          }
+        }
+      }
+      if (in) {
+        x0p[lane] = x0;
+        if (two) x1p[lane] = x1;
+      }
+    }
+    __syncthreads();
+    const int r_lo = UPPER ? 0 : b0 + bw, r_hi = UPPER ? b0 : kw;
+    for (int r = r_lo + warp; r < r_hi; r += UT / 32) {
+      const T m = lane < bw ? Ms[r * MSN + b0 + lane] : T(0);
+      for (int c = 0; c < w; ++c) {
+        T v = m * xt[c * SBN + b0 + lane];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) xt[c * SBN + r] -= v;
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < w * SBN; idx += UT) {
+    const int c = idx / SBN, j = idx - c * SBN;
+    if (j < kw) X[(int64_t)(lo + j) * ld + c0 + c] = xt[idx];
+  }
+}
+
 // Rows below the window of this pass: one CTA per (strip, 64-row tile = blockIdx.y).
 template <class T>
 __global__ void __launch_bounds__(UT)
-k_forward_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
+k_forward_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass, int sb) {
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
   int lo, hi;
-  if (!forward_window(d.n, pass, lo, hi)) return;
+  if (!forward_window(d.n, pass, lo, hi, sb)) return;
   const int r0 = hi + (int)blockIdx.y * 64;
   if (r0 >= d.n) return;
   window_apply<T>(sa.LU + d.lu_off, d.n, sa.X + d.b_off, d.nrhs, it.c0, it.width, r0, d.n, lo, hi);
@@ -1230,23 +1395,31 @@ cudaError_t prepare_update() {
                               (int)update_smem<T, MODE>());
 }
 
-// Passes over windows of SB rows; between two windows, the solved one is
-// applied to the rows on the far side (tiles of 64 rows: blockIdx.y).
+// Passes over windows (SB rows, or SBN for strips of at most 8 columns);
+// between two windows, the solved one is applied to the rows on the far side
+// (tiles of 64 rows: blockIdx.y).
 template <class T>
-cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, bool forward,
+cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax, bool forward,
                      cudaStream_t st) {
-  const int passes = (nmax + SB - 1) / SB;
+  const bool narrow = wmax <= 8;
+  const int sb = narrow ? SBN : SB;
+  const int passes = (nmax + sb - 1) / sb;
   for (int p = 0; p < passes; ++p) {
-    if (forward) k_forward<T><<<nitems, UT, 0, st>>>(sa, items, p);
-    else k_back<T><<<nitems, UT, 0, st>>>(sa, items, p);
+    if (narrow) {
+      if (forward) k_tri_narrow<T, false><<<nitems, UT, narrow_smem<T>(), st>>>(sa, items, p);
+      else k_tri_narrow<T, true><<<nitems, UT, narrow_smem<T>(), st>>>(sa, items, p);
+    } else {
+      if (forward) k_forward<T><<<nitems, UT, 0, st>>>(sa, items, p);
+      else k_back<T><<<nitems, UT, 0, st>>>(sa, items, p);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // rows left on the far side of this pass's window, largest system first
-    const int far = forward ? nmax - (p + 1) * SB : ((nmax - 1) / SB - p) * SB;
+    const int far = forward ? nmax - (p + 1) * sb : ((nmax - 1) / sb - p) * sb;
     if (p + 1 < passes && far > 0) {
       const dim3 grid((unsigned)nitems, (unsigned)((far + 63) / 64));
-      if (forward) k_forward_update<T><<<grid, UT, 0, st>>>(sa, items, p);
-      else k_back_update<T><<<grid, UT, 0, st>>>(sa, items, p);
+      if (forward) k_forward_update<T><<<grid, UT, 0, st>>>(sa, items, p, sb);
+      else k_back_update<T><<<grid, UT, 0, st>>>(sa, items, p, sb);
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
     }
@@ -1256,11 +1429,23 @@ cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, 
 
 }  // namespace
 
+template <class T>
+cudaError_t prepare_narrow() {
+  cudaError_t e = cudaFuncSetAttribute(k_tri_narrow<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)narrow_smem<T>());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tri_narrow<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)narrow_smem<T>());
+}
+
 cudaError_t step_prepare() {
-  cudaError_t e = prepare_update<double, kUpdFp32>();
+  cudaError_t e = prepare_narrow<double>();
+  if (e == cudaSuccess) e = prepare_narrow<float>();
+  if (e == cudaSuccess) e = prepare_update<double, kUpdFp32>();
   if (e == cudaSuccess) e = prepare_update<float, kUpdFp32>();
   if (e == cudaSuccess) e = prepare_update<float, kUpdTf32>();
   if (e == cudaSuccess) e = prepare_update<float, kUpdBf16>();
+  if (e == cudaSuccess) e = prepare_update<float, kUpd3xTf32>();
   return e;
 }
 
@@ -1314,32 +1499,39 @@ cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nit
       k_update<T, kUpdBf16><<<grid, UT, update_smem<T, kUpdBf16>(), st>>>(sa, items, k0);
       return cudaGetLastError();
     }
+    if (sa.umode == kUpd3xTf32) {
+      k_update<T, kUpd3xTf32><<<grid, UT, update_smem<T, kUpd3xTf32>(), st>>>(sa, items, k0);
+      return cudaGetLastError();
+    }
   }
   k_update<T, kUpdFp32><<<grid, UT, update_smem<T, kUpdFp32>(), st>>>(sa, items, k0);
   return cudaGetLastError();
 }
 
 template <class T>
-cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, cudaStream_t st) {
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax,
+                        cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
-  return windowed<T>(sa, items, nitems, nmax, false, st);
+  return windowed<T>(sa, items, nitems, nmax, wmax, false, st);
 }
 
 template <class T>
-cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
-                           cudaStream_t st) {
+cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax,
+                           cudaStream_t st, bool permute) {
   if (nitems <= 0) return cudaSuccess;
-  k_permute<T><<<nitems, UT, sizeof(int) * (size_t)nmax, st>>>(sa, items);
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  return windowed<T>(sa, items, nitems, nmax, true, st);
+  if (permute) {
+    k_permute<T><<<nitems, UT, 2 * sizeof(int) * (size_t)nmax, st>>>(sa, items);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return windowed<T>(sa, items, nitems, nmax, wmax, true, st);
 }
 
 #define NPPB_STEP_INSTANTIATE(T)                                                                          \
   template cudaError_t launch_panel<T>(const StepArgsT<T>&, const int32_t*, int, int, int, cudaStream_t);     \
   template cudaError_t launch_update<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);   \
-  template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);          \
-  template cudaError_t launch_forward<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);
+  template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);          \
+  template cudaError_t launch_forward<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t, bool);
 NPPB_STEP_INSTANTIATE(double)
 NPPB_STEP_INSTANTIATE(float)
 #undef NPPB_STEP_INSTANTIATE

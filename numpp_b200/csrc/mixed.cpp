@@ -5,7 +5,8 @@
 //  1. equilibrate: power-of-two row/column scales, the scaled matrix in FP32;
 //  2. factor in FP32 on the step-wise kernels (pivots and row moves kept),
 //     the first solution riding along as augmented columns; the trailing
-//     products in FP32, or on the tensor cores from TF32 / BF16 operands;
+//     products on the tensor cores (error-compensated TF32 by default, or
+//     plain TF32 / BF16 operands) or in FP32 FMA;
 //  3. refine in FP64: R = B - A X, eta = normwise backward error; systems with
 //     eta <= tol stop, systems whose eta no longer halves are marked stalled;
 //     the others solve A d = R with the FP32 factors and add d in FP64;
@@ -46,9 +47,11 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     set_error("negative count, order, nrhs or max_iter, or bad tolerance");
     return NPPB_E_ARG;
   }
-  if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16)) ||
-      ((flags & NPPB_MIXED_TF32) && (flags & NPPB_MIXED_BF16))) {
-    set_error("unknown mixed flag bits, or both TF32 and BF16");
+  const int arith = flags & (NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA);
+  if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 |
+                 NPPB_MIXED_FP32_FMA)) ||
+      (arith & (arith - 1))) {
+    set_error("unknown mixed flag bits, or more than one of TF32 / BF16 / FP32_FMA");
     return NPPB_E_ARG;
   }
   if (n > kMixedMaxN || count64 > INT32_MAX) {
@@ -63,9 +66,10 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   if (!device()) return NPPB_E_NODEV;
   const int count = (int)count64;
   const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs, c = (size_t)count;
-  DevMem a32, piv, sc32, b32, y32, rsm, csm, cmx, stm, info32, act;
+  DevMem a32, piv, rpos, sc32, b32, y32, rsm, csm, cmx, stm, info32, act;
   NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
   NPPB_CUDA(piv.alloc(sizeof(int32_t) * c * n, st), "workspace");
+  NPPB_CUDA(rpos.alloc(sizeof(int32_t) * c * n, st), "workspace");
   NPPB_CUDA(sc32.alloc(sizeof(StepScratchT<float>) * c, st), "workspace");
   NPPB_CUDA(b32.alloc(sizeof(float) * c * nb, st), "workspace");
   NPPB_CUDA(y32.alloc(sizeof(float) * c * nb, st), "workspace");
@@ -99,23 +103,25 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     sa.un = n;
     sa.unrhs = nrhs;
     sa.uleft = 1;
-    sa.umode = (flags & NPPB_MIXED_BF16) ? 2 : (flags & NPPB_MIXED_TF32) ? 1 : 0;
+    sa.umode = (flags & NPPB_MIXED_BF16) ? 2 : (flags & NPPB_MIXED_TF32) ? 1 : (flags & NPPB_MIXED_FP32_FMA) ? 0 : 3;
     NPPB_CUDA(run_step_uniform<float>(sa, count, st), "FP32 factorisation");
     NPPB_CUDA(mixed_mark_fp32_failures(info32.as<int32_t>(), S, count, st), "mark");
+    NPPB_CUDA(mixed_row_positions(piv.as<int32_t>(), count, n, rpos.as<int32_t>(), st), "row positions");
     NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 1, st), "apply");
     int h_act = 0;
     for (int it = 0;; ++it) {
       NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
-      NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), S, tol, it, 1,
-                               act.as<int>(), st),
+      // the scaled residual lands in y32 already in pivoted row order
+      NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), y32.as<float>(), rpos.as<int32_t>(), S,
+                               tol, it, 1, act.as<int>(), st),
                 "residual");
       NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
       NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
       if (h_act == 0 || it >= max_iter) break;
-      StepArgsT<float> sb = sa;  // correction: solve with the stored FP32 factors
-      sb.B = b32.as<float>();
+      StepArgsT<float> sb = sa;  // correction: solve with the stored FP32 factors, in place on y32
+      sb.B = nullptr;
       sb.X = y32.as<float>();
-      NPPB_CUDA(run_step_solve_uniform<float>(sb, count, st), "FP32 correction solve");
+      NPPB_CUDA(run_step_solve_uniform<float>(sb, count, st, true), "FP32 correction solve");
       NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 0, st), "apply");
     }
     NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
@@ -165,7 +171,8 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     for (size_t q = 0; q < k; ++q) hinfo[idx[q]] = cinfo[q];
   }
   // final backward error of every system, whatever path produced it
-  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, S, tol, 0, 0, act.as<int>(), st),
+  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, 0, 0,
+                           act.as<int>(), st),
             "residual");
   if (dFerr && dXtrue) NPPB_CUDA(mixed_ferr(dX, dXtrue, count, n, nrhs, dFerr, st), "forward error");
   NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");

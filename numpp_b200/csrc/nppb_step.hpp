@@ -60,7 +60,7 @@ struct StepArgsT {
   // scratch slot s; an inverse for every system when uinv != 0.
   int un, unrhs, uinv;
   int uleft;         // uniform batch keeps its factors: carry row moves left of each panel
-  int umode;         // FP32 factors: trailing product in FP32 (0), TF32 (1) or BF16 (2) tensor-core arithmetic
+  int umode;         // FP32 factors: trailing product in FP32 FMA (0), TF32 (1), BF16 (2) or 3xTF32 (3) tensor-core arithmetic
 };
 using StepArgs = StepArgsT<double>;
 
@@ -87,11 +87,16 @@ cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, 
 template <class T>
 cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st);
-// Back substitution of each strip item (nmax >= n of any item).
+// Back substitution of each strip item (nmax >= n of any item, wmax >= the
+// width of any item: strips of at most 8 columns take the narrow kernels).
 template <class T>
-cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, cudaStream_t st);
+cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax,
+                        cudaStream_t st);
+// getrs from stored factors: launch_forward gathers X = P B (unless permute
+// is false: X already holds the permuted right-hand sides) and runs the
+// forward substitution; the caller then runs launch_back.
 template <class T>
-cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax,
-                           cudaStream_t st);
+cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax,
+                           cudaStream_t st, bool permute = true);
 
 }  // namespace nppb

@@ -40,11 +40,19 @@ int arg_error(const std::string& m) {
     if (e_ != cudaSuccess) return nppb::cuda_status(e_, what); \
   } while (0)
 
+// Device allocation of a plan: plain, or stream-ordered on `ord` (no device
+// synchronisation; used by plans built and dropped per batch).
+cudaError_t plan_alloc(void** p, size_t bytes, cudaStream_t ord) {
+  return ord ? cudaMallocAsync(p, bytes, ord) : cudaMalloc(p, bytes);
+}
+
 template <class T>
-int upload(T** d, const std::vector<T>& h) {
+int upload(T** d, const std::vector<T>& h, cudaStream_t ord) {
   if (h.empty()) return NPPB_OK;
-  NPPB_CUDA(cudaMalloc(d, sizeof(T) * h.size()), "plan allocation");
-  NPPB_CUDA(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "plan upload");
+  NPPB_CUDA(plan_alloc(reinterpret_cast<void**>(d), sizeof(T) * h.size(), ord), "plan allocation");
+  // from pageable memory: the call returns once the source has been staged
+  if (ord) NPPB_CUDA(cudaMemcpyAsync(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, ord), "plan upload");
+  else NPPB_CUDA(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice), "plan upload");
   return NPPB_OK;
 }
 
@@ -78,14 +86,22 @@ Plan::~Plan() {
   if (done) cudaEventDestroy(done);
   if (cap) cudaStreamDestroy(cap);
   for (void* p : {(void*)d_desc, (void*)d_order, (void*)d_lu, (void*)d_piv, (void*)d_scratch,
-                  (void*)d_step_list, (void*)d_items, (void*)d_back, (void*)hA, (void*)hB, (void*)hX,
-                  (void*)hInv, (void*)hDet, (void*)hSign, (void*)hLog, (void*)hInfo})
+                  (void*)d_step_list, (void*)d_items, (void*)d_back})
+    if (p) {
+      if (alloc_stream) cudaFreeAsync(p, alloc_stream);
+      else cudaFree(p);
+    }
+  for (void* p : {(void*)hA, (void*)hB, (void*)hX, (void*)hInv, (void*)hDet, (void*)hSign, (void*)hLog, (void*)hInfo})
     if (p) cudaFree(p);
   if (prev >= 0) cudaSetDevice(prev);
 }
 
 int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
-                const int64_t* b_off, const int64_t* inv_off, int fl, bool solve_only_, bool own_lu) {
+                const int64_t* b_off, const int64_t* inv_off, int fl, bool solve_only_, bool own_lu,
+                const int64_t* lu_off_ext, const int64_t* piv_off_ext) {
+  if ((lu_off_ext == nullptr) != (piv_off_ext == nullptr)) return arg_error("factor offsets come in pairs");
+  ext_factors = lu_off_ext != nullptr;
+  if (ext_factors) own_lu = false;
   if (cnt < 0 || cnt > INT32_MAX) return arg_error("bad system count");
   if (fl & ~(NPPB_WANT_LU | NPPB_WANT_SOLVE | NPPB_WANT_DET | NPPB_WANT_SLOGDET | NPPB_WANT_INV))
     return arg_error("unknown flag bits");
@@ -122,10 +138,10 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
     s.idx = (int32_t)i;
     s.pad_ = -1;
     s.a_off = a_off[i];
-    s.lu_off = own_lu ? lu : a_off[i];
+    s.lu_off = ext_factors ? lu_off_ext[i] : own_lu ? lu : a_off[i];
     s.b_off = solve ? b_off[i] : 0;
     s.inv_off = (want_inv && inv_off[i] >= 0) ? inv_off[i] : -1;
-    s.piv_off = piv;
+    s.piv_off = ext_factors ? piv_off_ext[i] : piv;
     lu += (int64_t)ni * ni;
     piv += ni;
     a_elems = std::max(a_elems, a_off[i] + (int64_t)ni * ni);
@@ -140,7 +156,7 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
     }
   }
   lu_elems = own_lu ? lu : 0;
-  piv_elems = piv;
+  piv_elems = ext_factors ? 0 : piv;
 
   // warp classes: longest first
   std::vector<int32_t> order;
@@ -223,14 +239,22 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
           ch.steps.push_back(st);
         }
       }
-      ch.back_first = (int64_t)back.size();
+      // substitution strips, narrow (<= 8 columns) and wide ones in separate
+      // launch sequences: each strip's arithmetic depends on its own width only
+      std::vector<StepItem> cb;
       for (int64_t r = 0; r < num; ++r) {
         const int32_t si = list[first + r];
         const SysDesc& s = desc[si];
         const double cols = (solve ? s.nrhs : 0) + ((s.inv_off >= 0 && !solve_only) ? s.n : 0);
         kind_flops[kKindBack] += (double)s.n * s.n * cols * (solve_only ? 2.0 : 1.0);
-        if (solve && s.nrhs) add_strips(back, si, kSegRhs, 0, s.nrhs);
-        if (s.inv_off >= 0 && !solve_only) add_strips(back, si, kSegInv, 0, s.n);
+        if (solve && s.nrhs) add_strips(cb, si, kSegRhs, 0, s.nrhs);
+        if (s.inv_off >= 0 && !solve_only) add_strips(cb, si, kSegInv, 0, s.n);
+      }
+      std::stable_partition(cb.begin(), cb.end(), [](const StepItem& it) { return it.width <= 8; });
+      ch.back_first = (int64_t)back.size();
+      for (const StepItem& it : cb) {
+        if (it.width <= 8) ++ch.narrow_count;
+        back.push_back(it);
       }
       ch.back_count = (int64_t)back.size() - ch.back_first;
       chains.push_back(ch);
@@ -239,15 +263,21 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
   }
   nback = (int64_t)back.size();
 
-  int rc = upload(&d_desc, desc);
-  if (rc == NPPB_OK) rc = upload(&d_order, order);
-  if (rc == NPPB_OK) rc = upload(&d_step_list, step_members);
-  if (rc == NPPB_OK) rc = upload(&d_items, items);
-  if (rc == NPPB_OK) rc = upload(&d_back, back);
+  int rc = upload(&d_desc, desc, alloc_stream);
+  if (rc == NPPB_OK) rc = upload(&d_order, order, alloc_stream);
+  if (rc == NPPB_OK) rc = upload(&d_step_list, step_members, alloc_stream);
+  if (rc == NPPB_OK) rc = upload(&d_items, items, alloc_stream);
+  if (rc == NPPB_OK) rc = upload(&d_back, back, alloc_stream);
   if (rc != NPPB_OK) return rc;
-  if (nstep_sys) NPPB_CUDA(cudaMalloc(&d_scratch, sizeof(StepScratch) * nstep_sys), "plan scratch");
-  if (lu_elems) NPPB_CUDA(cudaMalloc(&d_lu, sizeof(double) * lu_elems), "plan LU workspace");
-  if (piv) NPPB_CUDA(cudaMalloc(&d_piv, sizeof(int32_t) * piv), "plan pivot workspace");
+  if (nstep_sys)
+    NPPB_CUDA(plan_alloc(reinterpret_cast<void**>(&d_scratch), sizeof(StepScratch) * nstep_sys, alloc_stream),
+              "plan scratch");
+  if (lu_elems)
+    NPPB_CUDA(plan_alloc(reinterpret_cast<void**>(&d_lu), sizeof(double) * lu_elems, alloc_stream),
+              "plan LU workspace");
+  if (piv_elems)
+    NPPB_CUDA(plan_alloc(reinterpret_cast<void**>(&d_piv), sizeof(int32_t) * piv_elems, alloc_stream),
+              "plan pivot workspace");
   return NPPB_OK;
 }
 
@@ -312,11 +342,10 @@ cudaError_t Plan::launch_warp(const Ptrs& p, int cls, cudaStream_t st) const {
 cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
   const StepArgs sa = step_args(p);
   const Chain& ch = chains[c];
-  const StepItem* back = d_back + ch.back_first;
   if (solve_only) {
-    cudaError_t e = launch_forward(sa, back, (int)ch.back_count, ch.nmax, st);
+    cudaError_t e = substitute(sa, ch, st, true);
     if (e != cudaSuccess) return e;
-    return launch_back(sa, back, (int)ch.back_count, ch.nmax, st);
+    return substitute(sa, ch, st, false);
   }
   for (const Step& s : ch.steps) {
     for (const auto& pr : s.panels) {
@@ -326,7 +355,17 @@ cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
     cudaError_t e = launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st);
     if (e != cudaSuccess) return e;
   }
-  return launch_back(sa, back, (int)ch.back_count, ch.nmax, st);
+  return substitute(sa, ch, st, false);
+}
+
+cudaError_t Plan::substitute(const StepArgs& sa, const Chain& ch, cudaStream_t st, bool forward) const {
+  const StepItem* back = d_back + ch.back_first;
+  const int nn = (int)ch.narrow_count, nw = (int)(ch.back_count - ch.narrow_count);
+  cudaError_t e = cudaSuccess;
+  if (nn) e = forward ? launch_forward(sa, back, nn, ch.nmax, 8, st) : launch_back(sa, back, nn, ch.nmax, 8, st);
+  if (e == cudaSuccess && nw)
+    e = forward ? launch_forward(sa, back + nn, nw, ch.nmax, 64, st) : launch_back(sa, back + nn, nw, ch.nmax, 64, st);
+  return e;
 }
 
 int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
@@ -348,9 +387,8 @@ int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
   for (int c = 0; c < (int)warp_classes.size(); ++c) timed(kKindWarp, [&] { return launch_warp(p, c, st); });
   const StepArgs sa = step_args(p);
   for (const Chain& ch : chains) {
-    const StepItem* back = d_back + ch.back_first;
     if (solve_only) {
-      timed(kKindBack, [&] { return launch_forward(sa, back, (int)ch.back_count, ch.nmax, st); });
+      timed(kKindBack, [&] { return substitute(sa, ch, st, true); });
     } else {
       for (const Step& s : ch.steps) {
         for (const auto& pr : s.panels)
@@ -358,7 +396,7 @@ int Plan::time_kernels(const Ptrs& p, cudaStream_t st, double* ms) const {
         timed(kKindUpdate, [&] { return launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st); });
       }
     }
-    timed(kKindBack, [&] { return launch_back(sa, back, (int)ch.back_count, ch.nmax, st); });
+    timed(kKindBack, [&] { return substitute(sa, ch, st, false); });
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -382,7 +420,8 @@ int Plan::execute(const Ptrs& p, cudaStream_t st) {
   if ((flags & NPPB_WANT_DET) && !p.Det) return arg_error("det needs Det");
   if ((flags & NPPB_WANT_SLOGDET) && (!p.Sign || !p.Logabs)) return arg_error("slogdet needs Sign, Logabs");
   if ((lu_elems || !p.A) && !p.LU) return arg_error("plan workspace missing");
-  if (piv_elems && !p.ipiv) return arg_error("plan pivot workspace missing");
+  if ((piv_elems || ext_factors) && !p.ipiv) return arg_error("plan pivot workspace missing");
+  if (ext_factors && !p.LU) return arg_error("plan factor storage missing");
   int cur = -1;
   cudaGetDevice(&cur);
   if (cur != dev) return arg_error("plan used on a different device than it was created on");
@@ -443,14 +482,22 @@ int Plan::execute(const Ptrs& p, cudaStream_t st) {
 int Plan::num_kernel_groups() const { return (int)warp_classes.size() + (nstep_sys ? 1 : 0); }
 
 int Plan::launches_per_execute() const {
+  // mirrors launch_update (k_rows, plus k_update while rows remain below the
+  // panel) and the windowed substitutions (a solve and, between windows, an
+  // update launch per pass; k_permute first for getrs)
+  auto windows = [](int nmax, int narrow, bool forward) {
+    const int sb = narrow ? 128 : 256, passes = (nmax + sb - 1) / sb;
+    return 2 * passes - 1 + (forward ? 1 : 0);
+  };
   int l = (int)warp_classes.size();
   for (const Chain& ch : chains) {
-    if (solve_only) {
-      l += 2;
-      continue;
+    const int nn = (int)ch.narrow_count, nw = (int)(ch.back_count - ch.narrow_count);
+    for (int fwd = solve_only ? 1 : 0; fwd >= 0; --fwd) {
+      if (nn) l += windows(ch.nmax, 1, fwd);
+      if (nw) l += windows(ch.nmax, 0, fwd);
     }
-    for (const Step& s : ch.steps) l += (int)s.panels.size() + 1;
-    l += 1;
+    if (solve_only) continue;
+    for (const Step& s : ch.steps) l += (int)s.panels.size() + 1 + (s.nmax - s.k0 - kStepNB > 0 ? 1 : 0);
   }
   return l;
 }

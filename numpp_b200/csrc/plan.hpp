@@ -51,6 +51,7 @@ class Plan {
     std::vector<Step> steps;
     int64_t back_first = 0, back_count = 0;
     int nmax = 0;
+    int64_t narrow_count = 0;  // the first narrow_count substitution strips are <= 8 columns wide
   };
 
   Plan() = default;
@@ -60,8 +61,12 @@ class Plan {
 
   // own_lu: allocate an LU workspace (else the factors go where A is: in place).
   // solve_only: getrs from factors already in LU / ipiv.
+  // lu_off_ext / piv_off_ext: caller-placed factors (system i's LU at
+  // lu_off_ext[i] of Ptrs::LU, its pivots at piv_off_ext[i] of Ptrs::ipiv).
+  // Set alloc_stream before build for stream-ordered device allocations.
   int build(int64_t count, const int32_t* n, const int32_t* nrhs, const int64_t* a_off,
-            const int64_t* b_off, const int64_t* inv_off, int flags, bool solve_only, bool own_lu);
+            const int64_t* b_off, const int64_t* inv_off, int flags, bool solve_only, bool own_lu,
+            const int64_t* lu_off_ext = nullptr, const int64_t* piv_off_ext = nullptr);
   int execute(const Ptrs& p, cudaStream_t st);
   cudaError_t launch_warp(const Ptrs& p, int cls, cudaStream_t st) const;
   cudaError_t launch_chain(const Ptrs& p, int chain, cudaStream_t st) const;
@@ -81,6 +86,8 @@ class Plan {
   int flags = 0;
   bool solve_only = false;
   bool use_graph = true;
+  bool ext_factors = false;
+  cudaStream_t alloc_stream = nullptr;  // stream-ordered allocations (freed on it too)
   int64_t a_elems = 0, b_elems = 0, inv_elems = 0, lu_elems = 0, piv_elems = 0;
   std::vector<WarpClass> warp_classes;
   std::vector<Chain> chains;
@@ -105,6 +112,8 @@ class Plan {
 
  private:
   void add_cost(const SysDesc& s, double& fl, double& by) const;
+  // forward (getrs) or back substitution of one chain's strips
+  cudaError_t substitute(const StepArgs& sa, const Chain& ch, cudaStream_t st, bool forward) const;
   Batch warp_batch(const Ptrs& p) const;
   StepArgs step_args(const Ptrs& p) const;
 

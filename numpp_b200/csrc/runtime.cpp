@@ -2,6 +2,7 @@
 // order -> kernel choice for uniform batches. C++20.
 #include "runtime.hpp"
 
+#include <algorithm>
 #include <climits>
 #include <mutex>
 #include <string>
@@ -127,24 +128,24 @@ cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st)
   }
   const int64_t back = (int64_t)count * uniform_back_strips(n, sa.unrhs, sa.uinv);
   if (back > INT32_MAX) return cudaErrorInvalidValue;
-  return launch_back(sa, nullptr, (int)back, sa.un, st);
+  return launch_back(sa, nullptr, (int)back, sa.un, sa.uinv ? 64 : std::min(64, sa.unrhs), st);
 }
 template cudaError_t run_step_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
 template cudaError_t run_step_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
 
 template <class T>
-cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st) {
+cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st, bool prepermuted) {
   const int64_t items = (int64_t)count * uniform_back_strips(sa.un, sa.unrhs, 0);
   if (sa.un <= 32 || items > INT32_MAX || count <= 0) return cudaErrorInvalidValue;
   StepArgsT<T> s2 = sa;
   s2.solve_only = 1;
   s2.uinv = 0;
-  cudaError_t e = launch_forward(s2, nullptr, (int)items, sa.un, st);
+  cudaError_t e = launch_forward(s2, nullptr, (int)items, sa.un, std::min(64, sa.unrhs), st, !prepermuted);
   if (e != cudaSuccess) return e;
-  return launch_back(s2, nullptr, (int)items, s2.un, st);
+  return launch_back(s2, nullptr, (int)items, s2.un, std::min(64, s2.unrhs), st);
 }
-template cudaError_t run_step_solve_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
-template cudaError_t run_step_solve_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
+template cudaError_t run_step_solve_uniform<double>(const StepArgsT<double>&, int, cudaStream_t, bool);
+template cudaError_t run_step_solve_uniform<float>(const StepArgsT<float>&, int, cudaStream_t, bool);
 
 cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t st) {
   if (n > 32) return cudaErrorInvalidValue;

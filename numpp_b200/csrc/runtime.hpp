@@ -62,9 +62,10 @@ cudaError_t run_warp_uniform(const Batch& bt, int64_t count, int n, cudaStream_t
 // the LU workspace, the per-system scratch and un / unrhs / uinv.
 template <class T>
 cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st);
-// getrs on a uniform batch from factors (LU, ipiv) a uleft=1 factorisation left: B -> X.
+// getrs on a uniform batch from factors (LU, ipiv) a uleft=1 factorisation left: B -> X;
+// prepermuted: X already holds P B (B is not read).
 template <class T>
-cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st);
+cudaError_t run_step_solve_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st, bool prepermuted = false);
 
 // One-time kernel attribute setup (dynamic shared memory opt-in), done before
 // any stream capture.

@@ -7,15 +7,17 @@ from . import _lib
 from .linalg import _check
 
 
-_FACTOR = {"fp32": 0, "tf32": _lib.MIXED_TF32, "bf16": _lib.MIXED_BF16}
+_FACTOR = {"3xtf32": 0, "fp32": _lib.MIXED_FP32_FMA, "tf32": _lib.MIXED_TF32, "bf16": _lib.MIXED_BF16}
 
 
 def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equilibrate: bool = True,
-                fallback: bool = True, factor: str = "fp32"):
+                fallback: bool = True, factor: str = "3xtf32"):
     """X for a (count, n, n) / (count, n, nrhs) float64 batch; returns
     (X, report) with report = dict(berr, ferr, iters, fallback, info) per system.
-    factor: arithmetic of the factorisation's trailing products ("fp32",
-    "tf32" or "bf16" tensor cores; FP32 panels and stored factors)."""
+    factor: arithmetic of the factorisation's trailing products: "3xtf32"
+    (error-compensated TF32 tensor-core products, close to FP32), "tf32" or
+    "bf16" (one tensor-core product), "fp32" (FMA); FP32 panels and stored
+    factors in every case."""
     L = _lib.load()
     A = np.ascontiguousarray(A, np.float64)
     B = np.ascontiguousarray(B, np.float64)

@@ -74,7 +74,7 @@ def test_small_orders_take_the_fp64_kernel(lib, oracle):
     np.testing.assert_allclose(X, Xo, rtol=1e-12, atol=1e-13)
 
 
-@pytest.mark.parametrize("factor,kappa", [("tf32", 1e2), ("tf32", 1e3), ("bf16", 1e1)])
+@pytest.mark.parametrize("factor,kappa", [("tf32", 1e2), ("tf32", 1e3), ("bf16", 1e1), ("fp32", 1e4)])
 def test_tensor_core_factors_refine(lib, oracle, factor, kappa):
     """TF32 / BF16 trailing products: rougher factors, more corrections, same bar."""
     A, B, Xt = workloads.conditioned_batch(seed=40 + int(np.log10(kappa)), count=6, n=256, kappa=kappa, nrhs=4)
