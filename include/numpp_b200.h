@@ -173,6 +173,40 @@ int nppb_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const doubl
                              int32_t* info, double* berr, double* ferr, int32_t* iters,
                              int32_t* fallback);
 
+/* ---- serving loop ---------------------------------------------------------- */
+/* No counterpart in the reference (NumPP solves one call at a time on the
+ * caller's thread, src/linalg/linalg.cpp:368-385). A server owns one worker
+ * thread, one stream and a resident-factor arena carved out of budget_bytes
+ * of device memory (three quarters; the rest bounds each batch's inputs).
+ * Requests from any thread are batched continuously: a batch closes when its
+ * oldest request has waited window_us, or at max_batch requests. A request
+ * either factors A (n x n, row-major) and solves for B (n x nrhs) into X,
+ * optionally keeping the factors resident (*factor_out = their id), or
+ * re-solves new right-hand sides with a resident factor (A == NULL,
+ * factor_in = its id). A, B and X are read / written by the worker with
+ * cudaMemcpyAsync and must stay valid until nppb_server_wait returns for the
+ * request (pinned host memory takes the fast path). When a new factor does
+ * not fit, the least recently used resident factors not read by the current
+ * batch are evicted; a re-solve on an evicted factor completes with
+ * NPPB_E_RANGE. A singular factorisation completes with NPPB_OK and
+ * info = first zero pivot + 1 (the factor is then not kept). A request's
+ * result does not depend on which other requests share its batch. */
+typedef struct nppb_server nppb_server;
+int nppb_server_create(nppb_server** srv, int64_t budget_bytes, double window_us, int32_t max_batch);
+int nppb_server_submit(nppb_server* srv, int32_t n, int32_t nrhs, const double* A, const double* B, double* X,
+                       int64_t factor_in, int32_t keep_factor, int64_t* request_id, int64_t* factor_out);
+/* Waits up to timeout_s; NPPB_DECLINED if the request is still running then
+ * (wait again). Otherwise returns the request's status, once per request,
+ * with its info and its latency (submission to completion, seconds). */
+int nppb_server_wait(nppb_server* srv, int64_t request_id, double timeout_s, int32_t* info,
+                     double* latency_s);
+int nppb_server_release_factor(nppb_server* srv, int64_t factor_id);
+/* out6: requests completed, batches run, resident factors, arena bytes in
+ * use, evictions, requests queued. */
+int nppb_server_stats(nppb_server* srv, int64_t* out6);
+/* Drains the queue, stops the worker, frees the arena. */
+int nppb_server_destroy(nppb_server* srv);
+
 /* ---- uneven batches ------------------------------------------------------ */
 /* A plan packs `count` systems of different orders n[i] and right-hand-side
  * counts nrhs[i] into size classes, one persistent launch per class, and
