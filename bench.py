@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--count", type=int, default=8192)
     p.add_argument("--cpu-sample", type=int, default=512, help="systems in the bounded CPU sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the side measurements (mixed vs FP64, small batch, serving)")
+    p.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per serving rate")
     return p.parse_args()
 
 
@@ -141,6 +144,226 @@ def fp64_peak_tflops(torch, dev):
     del a, b
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
+
+# ---------------------------------------------------------------------------
+# Side measurements (rank 0, one GPU): the other workloads of the path, each
+# timed with CUDA events on the launching stream after warm-up.
+
+def _event_ms(torch, fn, reps=3, warm=2):
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    return float(np.median(ts))
+
+
+def _berr(torch, A, B, X):
+    """max over systems of ||B - A X||_inf / (||A||_inf ||X||_inf + ||B||_inf), on the device."""
+    R = B - A @ X
+    eta = R.abs().amax((1, 2)) / (A.abs().sum(2).amax(1) * X.abs().amax((1, 2)) + B.abs().amax((1, 2)))
+    return float(eta.max().item())
+
+
+def _orthogonal_pairs(torch, dev, count, n, seed):
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    q1 = torch.linalg.qr(torch.randn(count, n, n, dtype=torch.float64, device=dev, generator=g))[0]
+    q2 = torch.linalg.qr(torch.randn(count, n, n, dtype=torch.float64, device=dev, generator=g))[0]
+    xt = torch.randn(count, n, 1, dtype=torch.float64, device=dev, generator=g)
+    return q1, q2, xt, g
+
+
+def mixed_vs_fp64(torch, dev, L, _lib):
+    """C3 (64 x 1024 and 8 x 4096, kappa 1e2..1e8, mixed FP32 factors) and C4
+    (512 x 256, nrhs 4, rows scaled 10^U(-6,6), BF16 factors + equilibration):
+    batched solves/s of the refined mixed solve vs the FP64 LU, both to a
+    normwise backward error <= 1e-10."""
+    P = _lib.ptr
+    st = torch.cuda.current_stream().cuda_stream
+    out = []
+    cases = [(64, 1024, (1e2, 1e4, 1e6, 1e8), 1, 0.0, ("3xtf32",)),
+             (8, 4096, (1e2, 1e4, 1e6, 1e8), 1, 0.0, ("3xtf32",)),
+             (512, 256, (1e1, 1e3, 1e4), 4, 6.0, ("bf16", "3xtf32"))]
+    flag = {"3xtf32": 0, "fp32": _lib.MIXED_FP32_FMA, "tf32": _lib.MIXED_TF32, "bf16": _lib.MIXED_BF16}
+    for count, n, kappas, nrhs, decades, factors in cases:
+        q1, q2, xt1, g = _orthogonal_pairs(torch, dev, count, n, seed=n)
+        xt = xt1.expand(count, n, nrhs).contiguous() if nrhs == 1 else torch.randn(
+            count, n, nrhs, dtype=torch.float64, device=dev, generator=g)
+        scale = None
+        if decades:
+            scale = 10.0 ** (torch.rand(count, n, 1, dtype=torch.float64, device=dev, generator=g) * 2 * decades
+                             - decades)
+        for kappa in kappas:
+            sig = torch.logspace(0.0, float(np.log10(kappa)), n, dtype=torch.float64, device=dev)
+            A = (q1 * sig) @ q2.transpose(1, 2)
+            if scale is not None:
+                A = A * scale
+            A = A.contiguous()
+            B = (A @ xt).contiguous()
+            X64 = torch.zeros_like(B)
+            info = torch.zeros(count, dtype=torch.int32, device=dev)
+
+            def fp64():
+                rc = L.nppb_d_linalg_batched(count, n, nrhs, _lib.WANT_SOLVE, P(A), P(B), P(X64), None, None, None,
+                                             None, None, None, P(info), st)
+                assert rc == 0, _lib.last_error()
+
+            t64 = _event_ms(torch, fp64)
+            b64 = _berr(torch, A, B, X64)
+            for fac in factors:
+                X = torch.zeros_like(B)
+                be = torch.zeros(count, dtype=torch.float64, device=dev)
+                fe = torch.zeros_like(be)
+                it = torch.zeros(count, dtype=torch.int32, device=dev)
+                fb = torch.zeros_like(it)
+
+                def mixed():
+                    rc = L.nppb_d_solve_mixed_batched(count, n, nrhs, P(A), P(B), P(X), P(xt), 1e-10, 30, flag[fac],
+                                                      P(info), P(be), P(fe), P(it), P(fb), st)
+                    assert rc == 0, _lib.last_error()
+
+                tm = _event_ms(torch, mixed)
+                out.append({
+                    "count": count, "n": n, "nrhs": nrhs, "kappa": kappa, "row_scale_decades": decades,
+                    "fp64_solves_s": count / (t64 * 1e-3), "fp64_ms": t64, "fp64_max_berr": b64,
+                    "mixed_factor": fac, "mixed_solves_s": count / (tm * 1e-3), "mixed_ms": tm,
+                    "mixed_over_fp64": t64 / tm, "mixed_max_berr": float(be.max().item()),
+                    "mixed_mean_corrections": float(it.float().mean().item()),
+                    "mixed_fp64_fallbacks": int(fb.sum().item()), "mixed_max_ferr": float(fe.max().item())})
+            del A, B, X64
+        del q1, q2
+        torch.cuda.empty_cache()
+    return out
+
+
+def small_uniform(torch, dev, L, _lib, workloads):
+    """C1: (256, 32, 32) + 32 I, solve + det, one launch of the warp kernel."""
+    P = _lib.ptr
+    A, B = workloads.uniform_batch(seed=SEED)
+    dA, dB = torch.from_numpy(A).to(dev), torch.from_numpy(B).to(dev)
+    dX = torch.zeros_like(dB)
+    det = torch.zeros(256, dtype=torch.float64, device=dev)
+    info = torch.zeros(256, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        rc = L.nppb_d_linalg_batched(256, 32, 1, _lib.WANT_SOLVE | _lib.WANT_DET, P(dA), P(dB), P(dX), None, P(det),
+                                     None, None, None, None, P(info), st)
+        assert rc == 0
+
+    ms = _event_ms(torch, run, reps=50, warm=5)
+    hX, hdet, hinfo = np.zeros_like(B), np.zeros(256), np.zeros(256, np.int32)
+    for _ in range(5):
+        L.nppb_solve_det_batched(256, 32, 1, P(A), P(B), P(hX), P(hdet), P(hinfo))
+    t0 = time.perf_counter()
+    for _ in range(50):
+        L.nppb_solve_det_batched(256, 32, 1, P(A), P(B), P(hX), P(hdet), P(hinfo))
+    e2e_ms = (time.perf_counter() - t0) / 50 * 1e3
+    return {"workload": "256 x 32 x 32 + 32 I, solve + det", "device_us": ms * 1e3,
+            "solves_s": 256 / (ms * 1e-3), "e2e_us": e2e_ms * 1e3, "e2e_solves_s": 256 / (e2e_ms * 1e-3),
+            "e2e_path": "nppb_solve_det_batched (host buffers, pageable)"}
+
+
+def serving_run(torch, dev, seconds, rates):
+    """C5: Poisson arrivals at each rate against the serving loop; n log-uniform
+    [16, 2048] from a seeded pool of 48 matrices (kappa log-uniform [1e1, 1e10]),
+    nrhs U[1, 64], 30% of requests new right-hand sides on a resident factor.
+    A waiter thread collects completions so the arrival clock never blocks;
+    inputs and outputs live in pinned host memory. Returns p50 / p99 latency
+    (submission to completion) and completed solves/s per rate."""
+    import queue
+
+    from numpp_b200.serving import Server
+
+    rng = np.random.default_rng(SEED)
+    g = torch.Generator(device=dev)
+    g.manual_seed(SEED)
+    pool = []
+    for _ in range(48):
+        n = int(np.floor(np.exp(rng.uniform(np.log(16), np.log(2049)))))
+        kappa = 10.0 ** rng.uniform(1, 10)
+        q1 = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))[0]
+        q2 = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, device=dev, generator=g))[0]
+        sig = torch.logspace(0.0, float(np.log10(kappa)), n, dtype=torch.float64, device=dev)
+        pool.append(((q1 * sig) @ q2.T).cpu().pin_memory().numpy())
+    rhs = torch.randn(2048 * 64, dtype=torch.float64).pin_memory().numpy()
+    slots = 384
+    xring = torch.zeros(slots, 2048 * 64, dtype=torch.float64).pin_memory().numpy()
+    results = []
+    for rate in rates:
+        lat, statuses = [], []
+        q = queue.Queue()
+        free = threading.Semaphore(slots)
+        with Server(budget_bytes=64 << 30, window_us=500.0, max_batch=512) as srv:
+            for A in pool:  # warm-up: every pool entry once
+                n = A.shape[0]
+                rid, _, _ = srv.submit(A, rhs[:n].reshape(n, 1), X=xring[0, :n].reshape(n, 1))
+                srv.wait(rid)
+
+            def waiter():
+                while True:
+                    rid = q.get()
+                    if rid is None:
+                        return
+                    rc, info, l = srv.wait(rid, timeout_s=120.0)
+                    lat.append(l)
+                    statuses.append(rc)
+                    free.release()
+
+            th = threading.Thread(target=waiter)
+            th.start()
+            resident = []  # (factor id, n)
+            t_next = time.perf_counter()
+            t_end = t_next + seconds
+            n_req = 0
+            while True:
+                t_next += rng.exponential(1.0 / rate)
+                if t_next >= t_end:
+                    break
+                while True:
+                    d = t_next - time.perf_counter()
+                    if d <= 0:
+                        break
+                    if d > 2e-3:
+                        time.sleep(d - 1e-3)
+                k = int(rng.integers(1, 65))
+                free.acquire()
+                slot = n_req % slots
+                if resident and rng.random() < 0.3:
+                    fid, n = resident[int(rng.integers(len(resident)))]
+                    rid, _, _ = srv.submit(None, rhs[:n * k].reshape(n, k), X=xring[slot, :n * k].reshape(n, k),
+                                           factor=fid)
+                else:
+                    A = pool[int(rng.integers(len(pool)))]
+                    n = A.shape[0]
+                    keep = rng.random() < 0.3
+                    rid, _, fid = srv.submit(A, rhs[:n * k].reshape(n, k), X=xring[slot, :n * k].reshape(n, k),
+                                             keep=keep)
+                    if keep:
+                        resident.append((fid, n))
+                        if len(resident) > 64:
+                            srv.release(resident.pop(0)[0])
+                q.put(rid)
+                n_req += 1
+            q.put(None)
+            th.join()
+            st = srv.stats()
+        lat_ms = np.asarray(lat) * 1e3
+        ok = int(sum(1 for r in statuses if r == 0))
+        results.append({"rate_per_s": rate, "requests": n_req, "completed_ok": ok,
+                        "evicted_or_failed": n_req - ok, "solves_s": ok / seconds,
+                        "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
+                        "batches": st["batches"]})
+    return {"workload": "Poisson arrivals, n log-uniform [16,2048] pool of 48, kappa log-uniform [1e1,1e10], "
+                        "nrhs U[1,64], 30% re-solves on resident factors, 64 GB budget, FP64 LU",
+            "seconds_per_rate": seconds, "rates": results}
 
 def cpu_reference_sample(sys, sample: int, threads: int, seed: int = 1):
     """Time the reference's CPU path (oracle/_ref) on a bounded random sample of the
@@ -311,6 +534,20 @@ def run_b200(args):
         cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind, "sample": desc}
 
     flops_step = workloads.uneven_flops(sys_)
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        plan.close()
+        del bufs, dA, dB, dX, dInv
+        torch.cuda.empty_cache()
+        # a side measurement that fails is reported, not fatal to the headline line
+        for key, fn in (("small_batch", lambda: small_uniform(torch, dev, L, _lib, workloads)),
+                        ("mixed_vs_fp64", lambda: mixed_vs_fp64(torch, dev, L, _lib)),
+                        ("serving", lambda: serving_run(torch, dev, args.serve_seconds, (500, 2000, 5000)))):
+            try:
+                extras[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                extras[key] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -337,6 +574,7 @@ def run_b200(args):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "hbm_peak_gbs": measured_peaks().get("hbm_gbs"),
+            **extras,
         }
         print(json.dumps(line), flush=True)
     plan.close()

@@ -1308,7 +1308,7 @@ k_tri_narrow(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
   }
   const int kw = hi - lo, w = it.width, c0 = it.c0;
   const T* M = sa.LU + d.lu_off + (int64_t)lo * n + lo;
-  async_tile<T>(Ms, MSN, M, n, kw, kw, SBN, SBN, pair_aligned(M, n));
+  async_tile<T>(Ms, MSN, M, n, kw, kw, kw, (kw + 1) & ~1, pair_aligned(M, n));  // only the live window
   for (int idx = tid; idx < 8 * SBN; idx += UT) {
     const int c = idx / SBN, j = idx - c * SBN;
     xt[idx] = (c < w && j < kw) ? X[(int64_t)(lo + j) * ld + c0 + c] : T(0);
@@ -1395,13 +1395,15 @@ cudaError_t prepare_update() {
                               (int)update_smem<T, MODE>());
 }
 
-// Passes over windows (SB rows, or SBN for strips of at most 8 columns);
+// Passes over windows (SB rows, or SBN for strips of at most 8 columns of
+// systems above 2 * SB);
 // between two windows, the solved one is applied to the rows on the far side
 // (tiles of 64 rows: blockIdx.y).
 template <class T>
 cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax, bool forward,
                      cudaStream_t st) {
-  const bool narrow = wmax <= 8;
+  // the narrow kernels pay off once a system needs more than two wide windows
+  const bool narrow = wmax <= 8 && nmax > 2 * SB;
   const int sb = narrow ? SBN : SB;
   const int passes = (nmax + sb - 1) / sb;
   for (int p = 0; p < passes; ++p) {

@@ -239,8 +239,9 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
           ch.steps.push_back(st);
         }
       }
-      // substitution strips, narrow (<= 8 columns) and wide ones in separate
-      // launch sequences: each strip's arithmetic depends on its own width only
+      // substitution strips, narrow (<= 8 columns of an order above 512) and
+      // the others in separate launch sequences: each strip's arithmetic
+      // depends on its own width and its system's order only
       std::vector<StepItem> cb;
       for (int64_t r = 0; r < num; ++r) {
         const int32_t si = list[first + r];
@@ -250,12 +251,18 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
         if (solve && s.nrhs) add_strips(cb, si, kSegRhs, 0, s.nrhs);
         if (s.inv_off >= 0 && !solve_only) add_strips(cb, si, kSegInv, 0, s.n);
       }
-      std::stable_partition(cb.begin(), cb.end(), [](const StepItem& it) { return it.width <= 8; });
+      auto narrow = [&](const StepItem& it) { return it.width <= 8 && desc[it.sys].n > 512; };
+      std::stable_partition(cb.begin(), cb.end(), narrow);
       ch.back_first = (int64_t)back.size();
+      int narrow_nmax = 0;
       for (const StepItem& it : cb) {
-        if (it.width <= 8) ++ch.narrow_count;
+        if (narrow(it)) {
+          ++ch.narrow_count;
+          narrow_nmax = std::max(narrow_nmax, desc[it.sys].n);
+        }
         back.push_back(it);
       }
+      ch.narrow_nmax = narrow_nmax;
       ch.back_count = (int64_t)back.size() - ch.back_first;
       chains.push_back(ch);
     }
@@ -362,7 +369,8 @@ cudaError_t Plan::substitute(const StepArgs& sa, const Chain& ch, cudaStream_t s
   const StepItem* back = d_back + ch.back_first;
   const int nn = (int)ch.narrow_count, nw = (int)(ch.back_count - ch.narrow_count);
   cudaError_t e = cudaSuccess;
-  if (nn) e = forward ? launch_forward(sa, back, nn, ch.nmax, 8, st) : launch_back(sa, back, nn, ch.nmax, 8, st);
+  if (nn)
+    e = forward ? launch_forward(sa, back, nn, ch.narrow_nmax, 8, st) : launch_back(sa, back, nn, ch.narrow_nmax, 8, st);
   if (e == cudaSuccess && nw)
     e = forward ? launch_forward(sa, back + nn, nw, ch.nmax, 64, st) : launch_back(sa, back + nn, nw, ch.nmax, 64, st);
   return e;
@@ -489,11 +497,12 @@ int Plan::launches_per_execute() const {
     const int sb = narrow ? 128 : 256, passes = (nmax + sb - 1) / sb;
     return 2 * passes - 1 + (forward ? 1 : 0);
   };
+  // wide strips: the chain's largest order bounds the passes
   int l = (int)warp_classes.size();
   for (const Chain& ch : chains) {
     const int nn = (int)ch.narrow_count, nw = (int)(ch.back_count - ch.narrow_count);
     for (int fwd = solve_only ? 1 : 0; fwd >= 0; --fwd) {
-      if (nn) l += windows(ch.nmax, 1, fwd);
+      if (nn) l += windows(ch.narrow_nmax, 1, fwd);
       if (nw) l += windows(ch.nmax, 0, fwd);
     }
     if (solve_only) continue;

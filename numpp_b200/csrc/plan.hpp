@@ -51,7 +51,8 @@ class Plan {
     std::vector<Step> steps;
     int64_t back_first = 0, back_count = 0;
     int nmax = 0;
-    int64_t narrow_count = 0;  // the first narrow_count substitution strips are <= 8 columns wide
+    int64_t narrow_count = 0;  // the first narrow_count substitution strips: <= 8 columns, order > 512
+    int narrow_nmax = 0;       // largest order among them
   };
 
   Plan() = default;

@@ -12,10 +12,16 @@
 //  * re-solve requests (new right-hand sides on a resident factor) run as one
 //    solve-only plan after the factor plan, so a re-solve may follow its
 //    factor request in the same batch;
+//  * requests go to one of three lanes by order (<= 128, <= 512, larger),
+//    each with its own queue, worker thread and stream, so small requests
+//    never queue behind a large factorisation; a re-solve takes its
+//    factor's lane, after the factor request;
 //  * the factor arena is carved out of the memory budget at creation; when a
 //    new factor does not fit, the least recently used resident factors that
-//    this batch does not read are evicted (a later re-solve on an evicted
-//    factor completes with NPPB_E_RANGE).
+//    this batch does not read are evicted, those no queued request reads
+//    first (a later re-solve on an evicted factor completes with
+//    NPPB_E_RANGE); a released factor is freed once no queued request reads
+//    it.
 // Inputs are read and outputs written with cudaMemcpyAsync straight from / to
 // the client's buffers (pinned buffers take the fast DMA path); the client
 // must keep them alive until its request completes. Latency = completion time
@@ -117,7 +123,25 @@ struct Factor {
   bool resident = false;  // holds arena slots
   bool released = false;  // the client let go of it
   int pins = 0;           // read or written by the batch in flight
+  int refs = 0;           // queued re-solve requests that read it
   std::list<int64_t>::iterator lru;
+};
+
+// One batch on its lane's stream: copies in, the factor plan, the re-solve
+// plan, copies out.
+struct Sub {
+  cudaStream_t st = nullptr;
+  std::vector<Req*> F, R;
+  std::vector<int64_t> f_lu, f_piv, r_lu, r_piv;
+  std::vector<int32_t> finfo;
+  std::vector<int64_t> transient_lu, transient_piv;  // factor slots freed after the batch
+  std::vector<int32_t> transient_n;
+  std::vector<int64_t> pinned;
+  DevMem dA, dB, dX, dI;
+  std::unique_ptr<Plan> pf, pr;
+  int rc = NPPB_OK;
+  bool ok = true;
+  std::string err;
 };
 
 }  // namespace
@@ -142,13 +166,15 @@ class Server {
     lu_cap_ = std::max<int64_t>(arena_bytes / 16 * 15 / (int64_t)sizeof(double) / 32 * 32, 32);
     piv_cap_ = std::max<int64_t>(arena_bytes / 16 / (int64_t)sizeof(int32_t) / 32 * 32, 32 * 128);
     batch_bytes_ = std::max<int64_t>(budget - arena_bytes, 64 << 20);
-    cudaError_t e = cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking);
+    cudaError_t e = cudaSuccess;
+    for (Lane& ln : lanes_)
+      if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ln.st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&lu_arena_, sizeof(double) * (size_t)lu_cap_);
     if (e == cudaSuccess) e = cudaMalloc(&piv_arena_, sizeof(int32_t) * (size_t)piv_cap_);
     if (e != cudaSuccess) return cuda_status(e, "server arena");
     lu_alloc_.reset(lu_cap_);
     piv_alloc_.reset(piv_cap_);
-    worker_ = std::thread([this] { loop(); });
+    for (int i = 0; i < kLanes; ++i) lanes_[i].worker = std::thread([this, i] { loop(i); });
     return NPPB_OK;
   }
 
@@ -185,6 +211,7 @@ class Server {
         set_error("order differs from the factor's");
         return NPPB_E_ARG;
       }
+      ++it->second.refs;
     }
     r->id = next_req_++;
     if (r->keep) {
@@ -196,9 +223,10 @@ class Server {
     if (req_id) *req_id = r->id;
     if (factor_out) *factor_out = r->factor_out;
     r->t_submit = Clock::now();
-    queue_.push_back(r.get());
+    Lane& ln = lanes_[lane_of(n)];
+    ln.queue.push_back(r.get());
     reqs_[r->id] = std::move(r);
-    cv_work_.notify_one();
+    ln.cv.notify_one();
     return NPPB_OK;
   }
 
@@ -245,7 +273,8 @@ class Server {
     out[2] = resident;
     out[3] = lu_alloc_.used() * (int64_t)sizeof(double);
     out[4] = evictions_;
-    out[5] = (int64_t)queue_.size();
+    out[5] = 0;
+    for (const Lane& ln : lanes_) out[5] += (int64_t)ln.queue.size();
   }
 
   void shutdown() {
@@ -253,16 +282,20 @@ class Server {
       std::lock_guard<std::mutex> lk(mu_);
       stop_ = true;
     }
-    cv_work_.notify_all();
-    if (worker_.joinable()) worker_.join();
+    for (Lane& ln : lanes_) ln.cv.notify_all();
+    for (Lane& ln : lanes_)
+      if (ln.worker.joinable()) ln.worker.join();
     if (dev_ >= 0) cudaSetDevice(dev_);
-    if (st_) cudaStreamSynchronize(st_);
+    for (Lane& ln : lanes_)
+      if (ln.st) cudaStreamSynchronize(ln.st);
     if (lu_arena_) cudaFree(lu_arena_);
     if (piv_arena_) cudaFree(piv_arena_);
-    if (st_) cudaStreamDestroy(st_);
+    for (Lane& ln : lanes_) {
+      if (ln.st) cudaStreamDestroy(ln.st);
+      ln.st = nullptr;
+    }
     lu_arena_ = nullptr;
     piv_arena_ = nullptr;
-    st_ = nullptr;
   }
 
  private:
@@ -279,7 +312,7 @@ class Server {
     auto it = factors_.find(fid);
     if (it == factors_.end()) return;
     Factor& f = it->second;
-    if (f.released && f.pins == 0) {
+    if (f.released && f.pins == 0 && f.refs == 0) {
       free_slots(f);
       factors_.erase(it);
     }
@@ -293,11 +326,13 @@ class Server {
       if (lu_off >= 0 && piv_off >= 0) return true;
       if (lu_off >= 0) lu_alloc_.release(lu_off, (int64_t)n * n);
       int64_t victim = -1;
-      for (auto it = lru_.rbegin(); it != lru_.rend(); ++it) {
-        const Factor& f = factors_[*it];
-        if (f.pins == 0 && f.ready) {
-          victim = *it;
-          break;
+      for (int pass = 0; pass < 2 && victim < 0; ++pass) {
+        for (auto it = lru_.rbegin(); it != lru_.rend(); ++it) {
+          const Factor& f = factors_[*it];
+          if (f.pins == 0 && f.ready && (pass == 1 || f.refs == 0)) {
+            victim = *it;
+            break;
+          }
         }
       }
       if (victim < 0) return false;
@@ -310,28 +345,31 @@ class Server {
     r->error = msg;
   }
 
-  void loop() {
+  static int lane_of(int32_t n) { return n <= 128 ? 0 : n <= 512 ? 1 : 2; }
+
+  void loop(int li) {
     cudaSetDevice(dev_);
+    Lane& ln = lanes_[li];
     for (;;) {
       std::vector<Req*> batch;
       {
         std::unique_lock<std::mutex> lk(mu_);
-        cv_work_.wait(lk, [&] { return stop_ || !queue_.empty(); });
-        if (queue_.empty()) return;  // stopping, nothing left
-        const auto deadline = queue_.front()->t_submit + window_;
-        cv_work_.wait_until(lk, deadline, [&] { return stop_ || (int)queue_.size() >= max_batch_; });
+        ln.cv.wait(lk, [&] { return stop_ || !ln.queue.empty(); });
+        if (ln.queue.empty()) return;  // stopping, nothing left
+        const auto deadline = ln.queue.front()->t_submit + window_;
+        ln.cv.wait_until(lk, deadline, [&] { return stop_ || (int)ln.queue.size() >= max_batch_; });
         int64_t bytes = 0;
-        while (!queue_.empty() && (int)batch.size() < max_batch_) {
-          Req* r = queue_.front();
+        while (!ln.queue.empty() && (int)batch.size() < max_batch_) {
+          Req* r = ln.queue.front();
           const int64_t rb = 8 * ((r->A ? (int64_t)r->n * r->n : 0) + 2 * (int64_t)r->n * r->nrhs);
           if (!batch.empty() && bytes + rb > batch_bytes_) break;
           bytes += rb;
           batch.push_back(r);
-          queue_.pop_front();
+          ln.queue.pop_front();
         }
       }
       try {
-        run_batch(batch);
+        run_batch(batch, ln.st);
       } catch (const std::exception& e) {
         std::lock_guard<std::mutex> lk(mu_);
         for (Req* r : batch) {
@@ -346,12 +384,9 @@ class Server {
     }
   }
 
-  void run_batch(std::vector<Req*>& batch) {
-    std::vector<Req*> F, R;
-    std::vector<int64_t> f_lu, f_piv, r_lu, r_piv;
-    std::vector<int64_t> transient_lu, transient_piv;  // freed after the batch
-    std::vector<int32_t> transient_n;
-    std::vector<int64_t> pinned;
+  void run_batch(std::vector<Req*>& batch, cudaStream_t st) {
+    Sub p;
+    p.st = st;
     {
       std::lock_guard<std::mutex> lk(mu_);
       // factor requests first: a re-solve in the same batch may read them
@@ -363,9 +398,9 @@ class Server {
           if (r->keep) factors_.erase(r->factor_out);
           continue;
         }
-        F.push_back(r);
-        f_lu.push_back(lu);
-        f_piv.push_back(pv);
+        p.F.push_back(r);
+        p.f_lu.push_back(lu);
+        p.f_piv.push_back(pv);
         if (r->keep) {
           Factor& f = factors_[r->factor_out];
           f.lu_off = lu;
@@ -374,55 +409,56 @@ class Server {
           f.pins = 1;
           lru_.push_front(r->factor_out);
           f.lru = lru_.begin();
-          pinned.push_back(r->factor_out);
+          p.pinned.push_back(r->factor_out);
         } else {
-          transient_lu.push_back(lu);
-          transient_piv.push_back(pv);
-          transient_n.push_back(r->n);
+          p.transient_lu.push_back(lu);
+          p.transient_piv.push_back(pv);
+          p.transient_n.push_back(r->n);
         }
       }
       for (Req* r : batch) {
         if (r->factor_in < 0) continue;
         auto it = factors_.find(r->factor_in);
+        if (it != factors_.end()) --it->second.refs;
         if (it == factors_.end() || !it->second.resident) {
           fail(r, NPPB_E_RANGE, "factor not resident (evicted, failed or released)");
+          if (it != factors_.end()) maybe_free(r->factor_in);
           continue;
         }
         Factor& f = it->second;
         ++f.pins;
-        pinned.push_back(r->factor_in);
+        p.pinned.push_back(r->factor_in);
         lru_.splice(lru_.begin(), lru_, f.lru);
-        R.push_back(r);
-        r_lu.push_back(f.lu_off);
-        r_piv.push_back(f.piv_off);
+        p.R.push_back(r);
+        p.r_lu.push_back(f.lu_off);
+        p.r_piv.push_back(f.piv_off);
       }
     }
-
-    std::string err;
-    int rc = NPPB_OK;
-    std::vector<int32_t> finfo(F.size(), 0);
-    if (!F.empty() || !R.empty()) rc = execute(F, R, f_lu, f_piv, r_lu, r_piv, finfo, err);
-
+    launch(p);
+    if (!p.F.empty() || !p.R.empty()) {
+      if (!check(p, cudaStreamSynchronize(p.st), "batch")) p.ok = false;
+      if (p.rc == NPPB_OK && !p.ok) p.rc = NPPB_E_CUDA;
+    }
     const auto t_done = Clock::now();
     {
       std::lock_guard<std::mutex> lk(mu_);
-      for (size_t i = 0; i < F.size(); ++i) {
-        Req* r = F[i];
-        if (rc != NPPB_OK) fail(r, rc, err);
-        r->info = finfo[i];
+      for (size_t i = 0; i < p.F.size(); ++i) {
+        Req* r = p.F[i];
+        if (p.rc != NPPB_OK) fail(r, p.rc, p.err);
+        r->info = p.rc == NPPB_OK ? p.finfo[i] : 0;
         if (r->keep) {
           Factor& f = factors_[r->factor_out];
-          f.ready = rc == NPPB_OK && finfo[i] == 0;
+          f.ready = p.rc == NPPB_OK && r->info == 0;
           if (!f.ready) f.released = true;  // a failed or singular factorisation is not kept
         }
       }
-      for (Req* r : R)
-        if (rc != NPPB_OK) fail(r, rc, err);
-      for (size_t i = 0; i < transient_lu.size(); ++i) {
-        lu_alloc_.release(transient_lu[i], (int64_t)transient_n[i] * transient_n[i]);
-        piv_alloc_.release(transient_piv[i], transient_n[i]);
+      for (Req* r : p.R)
+        if (p.rc != NPPB_OK) fail(r, p.rc, p.err);
+      for (size_t i = 0; i < p.transient_lu.size(); ++i) {
+        lu_alloc_.release(p.transient_lu[i], (int64_t)p.transient_n[i] * p.transient_n[i]);
+        piv_alloc_.release(p.transient_piv[i], p.transient_n[i]);
       }
-      for (int64_t fid : pinned) {
+      for (int64_t fid : p.pinned) {
         auto it = factors_.find(fid);
         if (it != factors_.end()) {
           --it->second.pins;
@@ -439,19 +475,23 @@ class Server {
     cv_done_.notify_all();
   }
 
-  // One batch on the server stream: copies in, the factor plan, the re-solve
-  // plan, copies out; returns after the stream has drained.
-  int execute(const std::vector<Req*>& F, const std::vector<Req*>& R, const std::vector<int64_t>& f_lu,
-              const std::vector<int64_t>& f_piv, const std::vector<int64_t>& r_lu, const std::vector<int64_t>& r_piv,
-              std::vector<int32_t>& finfo, std::string& err) {
+  static bool check(Sub& p, cudaError_t e, const char* what) {
+    if (e != cudaSuccess && p.err.empty()) p.err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaSuccess;
+  }
+
+  // Enqueues one part on its stream; device memory is released
+  // stream-ordered, so the part is complete once its stream has drained.
+  void launch(Sub& p) {
+    const size_t nf = p.F.size(), nr = p.R.size();
+    if (!nf && !nr) return;
     // packed layout: A of the factor requests, then B / X of all requests
-    const size_t nf = F.size(), nr = R.size();
     std::vector<int32_t> fn(nf), fk(nf), rn(nr), rk(nr);
     std::vector<int64_t> fa(nf), fb(nf), rb(nr), fi(nf, -1), ri(nr, -1);
     int64_t a_elems = 0, b_elems = 0;
     for (size_t i = 0; i < nf; ++i) {
-      fn[i] = F[i]->n;
-      fk[i] = F[i]->nrhs;
+      fn[i] = p.F[i]->n;
+      fk[i] = p.F[i]->nrhs;
       fa[i] = a_elems;
       a_elems += (int64_t)fn[i] * fn[i];
       fb[i] = b_elems;
@@ -459,89 +499,88 @@ class Server {
     }
     const int64_t r_base = b_elems;
     for (size_t i = 0; i < nr; ++i) {
-      rn[i] = R[i]->n;
-      rk[i] = R[i]->nrhs;
+      rn[i] = p.R[i]->n;
+      rk[i] = p.R[i]->nrhs;
       rb[i] = b_elems - r_base;
       b_elems += (int64_t)rn[i] * rk[i];
     }
-    DevMem dA, dB, dX, dI;
-    auto cuda = [&](cudaError_t e, const char* what) {
-      if (e != cudaSuccess && err.empty()) err = std::string(what) + ": " + cudaGetErrorString(e);
-      return e == cudaSuccess;
-    };
-    bool ok = true;
-    if (a_elems) ok = ok && cuda(dA.alloc(sizeof(double) * a_elems, st_), "batch A");
-    ok = ok && cuda(dB.alloc(sizeof(double) * b_elems, st_), "batch B");
-    ok = ok && cuda(dX.alloc(sizeof(double) * b_elems, st_), "batch X");
-    if (nf) ok = ok && cuda(dI.alloc(sizeof(int32_t) * nf, st_), "batch info");
+    p.finfo.assign(nf, 0);
+    cudaStream_t st = p.st;
+    bool& ok = p.ok;
+    if (a_elems) ok = ok && check(p, p.dA.alloc(sizeof(double) * a_elems, st), "batch A");
+    ok = ok && check(p, p.dB.alloc(sizeof(double) * b_elems, st), "batch B");
+    ok = ok && check(p, p.dX.alloc(sizeof(double) * b_elems, st), "batch X");
+    if (nf) ok = ok && check(p, p.dI.alloc(sizeof(int32_t) * nf, st), "batch info");
     for (size_t i = 0; ok && i < nf; ++i) {
-      ok = cuda(cudaMemcpyAsync(dA.as<double>() + fa[i], F[i]->A, sizeof(double) * fn[i] * fn[i],
-                                cudaMemcpyHostToDevice, st_), "copy A") &&
-           cuda(cudaMemcpyAsync(dB.as<double>() + fb[i], F[i]->B, sizeof(double) * fn[i] * fk[i],
-                                cudaMemcpyHostToDevice, st_), "copy B");
+      ok = check(p, cudaMemcpyAsync(p.dA.as<double>() + fa[i], p.F[i]->A, sizeof(double) * fn[i] * fn[i],
+                                    cudaMemcpyHostToDevice, st), "copy A") &&
+           check(p, cudaMemcpyAsync(p.dB.as<double>() + fb[i], p.F[i]->B, sizeof(double) * fn[i] * fk[i],
+                                    cudaMemcpyHostToDevice, st), "copy B");
     }
     for (size_t i = 0; ok && i < nr; ++i)
-      ok = cuda(cudaMemcpyAsync(dB.as<double>() + r_base + rb[i], R[i]->B, sizeof(double) * rn[i] * rk[i],
-                                cudaMemcpyHostToDevice, st_), "copy B");
-    int rc = NPPB_OK;
-    std::unique_ptr<Plan> pf, pr;
+      ok = check(p, cudaMemcpyAsync(p.dB.as<double>() + r_base + rb[i], p.R[i]->B, sizeof(double) * rn[i] * rk[i],
+                                    cudaMemcpyHostToDevice, st), "copy B");
+    int& rc = p.rc;
     if (ok && nf) {
-      pf = std::make_unique<Plan>();
-      pf->use_graph = false;
-      pf->alloc_stream = st_;
-      rc = pf->build((int64_t)nf, fn.data(), fk.data(), fa.data(), fb.data(), fi.data(),
-                     NPPB_WANT_SOLVE | NPPB_WANT_LU, false, false, f_lu.data(), f_piv.data());
+      p.pf = std::make_unique<Plan>();
+      p.pf->use_graph = false;
+      p.pf->alloc_stream = st;
+      rc = p.pf->build((int64_t)nf, fn.data(), fk.data(), fa.data(), fb.data(), fi.data(),
+                       NPPB_WANT_SOLVE | NPPB_WANT_LU, false, false, p.f_lu.data(), p.f_piv.data());
       if (rc == NPPB_OK) {
-        Plan::Ptrs p{};
-        p.A = dA.as<double>();
-        p.B = dB.as<double>();
-        p.X = dX.as<double>();
-        p.info = dI.as<int32_t>();
-        p.LU = lu_arena_;
-        p.ipiv = piv_arena_;
-        rc = pf->execute(p, st_);
+        Plan::Ptrs q{};
+        q.A = p.dA.as<double>();
+        q.B = p.dB.as<double>();
+        q.X = p.dX.as<double>();
+        q.info = p.dI.as<int32_t>();
+        q.LU = lu_arena_;
+        q.ipiv = piv_arena_;
+        rc = p.pf->execute(q, st);
       }
     }
     if (ok && rc == NPPB_OK && nr) {
-      pr = std::make_unique<Plan>();
-      pr->use_graph = false;
-      pr->alloc_stream = st_;
+      p.pr = std::make_unique<Plan>();
+      p.pr->use_graph = false;
+      p.pr->alloc_stream = st;
       // a_off is not read in solve-only mode: the factor offsets stand in
-      rc = pr->build((int64_t)nr, rn.data(), rk.data(), r_lu.data(), rb.data(), ri.data(), NPPB_WANT_SOLVE, true,
-                     false, r_lu.data(), r_piv.data());
+      rc = p.pr->build((int64_t)nr, rn.data(), rk.data(), p.r_lu.data(), rb.data(), ri.data(), NPPB_WANT_SOLVE,
+                       true, false, p.r_lu.data(), p.r_piv.data());
       if (rc == NPPB_OK) {
-        Plan::Ptrs p{};
-        p.B = dB.as<double>() + r_base;
-        p.X = dX.as<double>() + r_base;
-        p.LU = lu_arena_;
-        p.ipiv = piv_arena_;
-        rc = pr->execute(p, st_);
+        Plan::Ptrs q{};
+        q.B = p.dB.as<double>() + r_base;
+        q.X = p.dX.as<double>() + r_base;
+        q.LU = lu_arena_;
+        q.ipiv = piv_arena_;
+        rc = p.pr->execute(q, st);
       }
     }
-    if (rc != NPPB_OK && err.empty()) err = last_error();
+    if (rc != NPPB_OK && p.err.empty()) p.err = last_error();
     for (size_t i = 0; ok && rc == NPPB_OK && i < nf; ++i)
-      ok = cuda(cudaMemcpyAsync(F[i]->X, dX.as<double>() + fb[i], sizeof(double) * fn[i] * fk[i],
-                                cudaMemcpyDeviceToHost, st_), "copy X");
+      ok = check(p, cudaMemcpyAsync(p.F[i]->X, p.dX.as<double>() + fb[i], sizeof(double) * fn[i] * fk[i],
+                                    cudaMemcpyDeviceToHost, st), "copy X");
     for (size_t i = 0; ok && rc == NPPB_OK && i < nr; ++i)
-      ok = cuda(cudaMemcpyAsync(R[i]->X, dX.as<double>() + r_base + rb[i], sizeof(double) * rn[i] * rk[i],
-                                cudaMemcpyDeviceToHost, st_), "copy X");
+      ok = check(p, cudaMemcpyAsync(p.R[i]->X, p.dX.as<double>() + r_base + rb[i], sizeof(double) * rn[i] * rk[i],
+                                    cudaMemcpyDeviceToHost, st), "copy X");
     if (ok && rc == NPPB_OK && nf)
-      ok = cuda(cudaMemcpyAsync(finfo.data(), dI.as<int32_t>(), sizeof(int32_t) * nf, cudaMemcpyDeviceToHost, st_),
-                "copy info");
-    // plans and staging free their device memory stream-ordered; then wait for the batch
-    pf.reset();
-    pr.reset();
-    dA.release();
-    dB.release();
-    dX.release();
-    dI.release();
-    ok = cuda(cudaStreamSynchronize(st_), "batch") && ok;
-    if (rc != NPPB_OK) return rc;
-    return ok ? NPPB_OK : NPPB_E_CUDA;
+      ok = check(p, cudaMemcpyAsync(p.finfo.data(), p.dI.as<int32_t>(), sizeof(int32_t) * nf,
+                                    cudaMemcpyDeviceToHost, st), "copy info");
+    p.pf.reset();
+    p.pr.reset();
+    p.dA.release();
+    p.dB.release();
+    p.dX.release();
+    p.dI.release();
   }
 
   int dev_ = -1;
-  cudaStream_t st_ = nullptr;
+  static constexpr int kLanes = 3;
+  struct Lane {
+    std::deque<Req*> queue;
+    std::condition_variable cv;
+    std::thread worker;
+    cudaStream_t st = nullptr;
+  };
+  Lane lanes_[kLanes];
   double* lu_arena_ = nullptr;
   int32_t* piv_arena_ = nullptr;
   int64_t lu_cap_ = 0, piv_cap_ = 0, batch_bytes_ = 0;
@@ -549,8 +588,7 @@ class Server {
   int max_batch_ = 1;
 
   std::mutex mu_;
-  std::condition_variable cv_work_, cv_done_;
-  std::deque<Req*> queue_;
+  std::condition_variable cv_done_;
   std::unordered_map<int64_t, std::unique_ptr<Req>> reqs_;
   std::unordered_map<int64_t, Factor> factors_;
   std::list<int64_t> lru_;  // most recently used first
@@ -558,7 +596,6 @@ class Server {
   int64_t next_req_ = 0, next_factor_ = 0;
   int64_t completed_ = 0, batches_ = 0, evictions_ = 0;
   bool stop_ = false;
-  std::thread worker_;
 };
 
 }  // namespace nppb

@@ -56,7 +56,8 @@ def test_same_result_alone_and_in_a_mixed_batch(lib):
     with Server(budget_bytes=1 << 30, window_us=100.0) as srv:
         rid, X_alone, _ = srv.submit(A, B)
         assert srv.wait(rid)[0] == 0
-    others = [_system(rng, n, k, shift=False) for n, k in [(40, 2), (700, 1), (12, 4), (300, 64), (513, 9), (90, 1)]]
+    # orders 129..512 share a lane: the request runs in one batch with 200 and 300
+    others = [_system(rng, n, k, shift=False) for n, k in [(40, 2), (700, 1), (12, 4), (300, 64), (200, 9), (90, 1)]]
     with Server(budget_bytes=1 << 30, window_us=50000.0) as srv:
         ids = [srv.submit(Ao, Bo)[0] for Ao, Bo in others[:3]]
         rid, X_mix, _ = srv.submit(A, B)
@@ -64,7 +65,7 @@ def test_same_result_alone_and_in_a_mixed_batch(lib):
         assert srv.wait(rid)[0] == 0
         for i in ids:
             assert srv.wait(i)[0] == 0
-        assert srv.stats()["batches"] == 1
+        assert srv.stats()["batches"] == 3  # one per lane
     assert np.array_equal(X_alone, X_mix)
 
 
