@@ -421,7 +421,7 @@ def run_b200(args):
     import torch
     import torch.distributed as dist
 
-    from numpp_b200 import _lib, workloads
+    from numpp_b200 import _lib, replicas, workloads
     from numpp_b200.grouped import Plan
 
     rank, world, local = dist_env()
@@ -470,9 +470,7 @@ def run_b200(args):
     per_step = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
     total_ms = ev[0].elapsed_time(ev[-1])
     if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+        total_ms = replicas.max_over_ranks(total_ms, device=dev)
         dist.barrier()
     ms_step = total_ms / args.steps
     value = world * cnt / (ms_step * 1e-3)
@@ -522,9 +520,7 @@ def run_b200(args):
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_step = float(np.mean(e2e_ms))
     if world > 1:
-        t = torch.tensor([e2e_step], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t.item())
+        e2e_step = replicas.max_over_ranks(e2e_step, device=dev)
     h2d = 8 * (plan.a_elems + plan.b_elems)
     d2h = 8 * (plan.b_elems + plan.inv_elems + 3 * cnt) + 4 * cnt
 
