@@ -156,13 +156,18 @@ int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const d
  * three products: close to FP32 accuracy); NPPB_MIXED_TF32 / NPPB_MIXED_BF16:
  * one tensor-core product from operands rounded to TF32 / BF16;
  * NPPB_MIXED_FP32_FMA: FP32 fused multiply-adds. FP32 accumulation in every
- * case; the panels, the stored factors and the correction solves stay FP32. */
+ * case; the panels, the stored factors and the correction solves stay FP32.
+ * The TF32 products run on the warp-level mma.sync instructions, or with
+ * NPPB_MIXED_TCGEN05 on tcgen05 with TMEM accumulators (same products; the
+ * mma.sync form measured faster here: the update is bound by memory, not by
+ * the tensor core). BF16 always uses mma.sync. */
 enum {
   NPPB_MIXED_NO_EQUILIBRATE = 1,
   NPPB_MIXED_NO_FALLBACK = 2,
   NPPB_MIXED_TF32 = 4,
   NPPB_MIXED_BF16 = 8,
-  NPPB_MIXED_FP32_FMA = 16
+  NPPB_MIXED_FP32_FMA = 16,
+  NPPB_MIXED_TCGEN05 = 32
 };
 int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                const double* dB, double* dX, const double* dXtrue, double tol,
@@ -226,6 +231,15 @@ int nppb_plan_sizes(const nppb_plan* plan, int64_t* a_elems, int64_t* b_elems,
 int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, double* dX,
                       double* dInv, double* dDet, double* dSign, double* dLogabs,
                       int32_t* dinfo, void* stream);
+/* Autotuner (no reference counterpart): times the plan with 1, 2, 3, 4 and 6
+ * independent step chains (graph branches whose panels overlap each other's
+ * updates) on these device buffers, a warm-up and two replays each, and keeps
+ * the fastest; *chains_out = the chain count kept, *ms_out = its time per
+ * execution. The outputs are written as by nppb_plan_execute; synchronises
+ * `stream`. */
+int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,
+                       double* dDet, double* dSign, double* dLogabs, int32_t* dinfo, void* stream,
+                       int32_t* chains_out, float* ms_out);
 /* Host buffers: copies in, runs, copies out, synchronises. Inputs in pinned
  * memory take the fast DMA path. */
 int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X,

@@ -15,7 +15,7 @@ OK, DECLINED = 0, 1
 E_ARG, E_NODEV, E_CUDA, E_NOMEM, E_RANGE = -1, -2, -3, -4, -5
 DT_FLOAT32, DT_FLOAT64 = 10, 11
 WANT_LU, WANT_SOLVE, WANT_DET, WANT_SLOGDET, WANT_INV = 1, 2, 4, 8, 16
-MIXED_NO_EQUILIBRATE, MIXED_NO_FALLBACK, MIXED_TF32, MIXED_BF16, MIXED_FP32_FMA = 1, 2, 4, 8, 16
+MIXED_NO_EQUILIBRATE, MIXED_NO_FALLBACK, MIXED_TF32, MIXED_BF16, MIXED_FP32_FMA, MIXED_TCGEN05 = 1, 2, 4, 8, 16, 32
 
 _vp = C.c_void_p
 _i32 = C.c_int32
@@ -58,6 +58,7 @@ SIGNATURES = {
     "nppb_plan_class_info": (_int, [_vp, _int, C.POINTER(_int), C.POINTER(_int), C.POINTER(_i64),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_plan_time_classes": (_int, [_vp] * 10 + [_int, C.POINTER(C.c_float)]),
+    "nppb_plan_autotune": (_int, [_vp] * 10 + [C.POINTER(_i32), C.POINTER(C.c_float)]),
     "nppb_plan_time_kernels": (_int, [_vp] * 10 + [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_solve_grouped": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _int] + [_vp] * 8),
     "nppb_server_create": (_int, [C.POINTER(_vp), _i64, C.c_double, _i32]),

@@ -608,7 +608,9 @@ template <> struct Acc32<float> {  // 4 x 4 elements per thread
 // tensor-core products, the lo*lo term dropped): close to FP32 accuracy at
 // tensor-core speed (the error-compensated TF32 scheme of Ootomo and Yokota,
 // 2022, and of CUTLASS's 3xTF32 kernels).
-enum : int { kUpdFp32 = 0, kUpdTf32 = 1, kUpdBf16 = 2, kUpd3xTf32 = 3 };
+// kUpdTcTf32 / kUpdTc3xTf32: the same TF32 / 3xTF32 products on the
+// tcgen05 tensor cores with TMEM accumulators (k_update_tc).
+enum : int { kUpdFp32 = 0, kUpdTf32 = 1, kUpdBf16 = 2, kUpd3xTf32 = 3, kUpdTcTf32 = 4, kUpdTc3xTf32 = 5 };
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
@@ -764,6 +766,30 @@ __device__ __forceinline__ void tile_update(const T* As, const T* Bs, int r0, in
   });
 }
 
+// The work item of an update CTA. Uniform batches can split one step's update
+// for look-ahead: part 1 = only the first matrix strip of every system (it
+// holds the next panel's columns; grid.x = systems), part 2 = every other
+// strip, part 0 = all. Returns false for a CTA with nothing to do.
+template <class T>
+__device__ __forceinline__ bool update_item(const StepArgsT<T>& sa, const StepItem* items, int k0, int part,
+                                            StepItem& it) {
+  if (items) {
+    it = items[blockIdx.x];
+    return true;
+  }
+  if (part == 0) {
+    it = uniform_item(sa, blockIdx.x, k0, false);
+    return true;
+  }
+  const int per = uniform_update_strips(sa.un, sa.unrhs, sa.uinv, k0, sa.uleft);
+  if (part == 1) {
+    it = uniform_item(sa, (int)blockIdx.x * per, k0, false);
+    return it.kind == kSegMatrix;
+  }
+  it = uniform_item(sa, blockIdx.x, k0, false);
+  return !((int)blockIdx.x % per == 0 && it.kind == kSegMatrix);
+}
+
 // ---------------------------------------------------------------------------
 // k_rows: one CTA per strip item of step k0. Applies the panel's row moves to
 // the strip (top rows from their sources, displaced old top rows to their new
@@ -894,7 +920,7 @@ __device__ __forceinline__ bool pair_aligned(const T* p, int64_t ld) {
 
 template <class T, int MODE>
 __global__ void __launch_bounds__(UT, 3)
-k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
+k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) {
   using P2 = typename Pair<T>::type;
   using Acc = typename AccSel<T, MODE>::type;
   constexpr int AS = TileCfg<T, MODE>::AS, US = TileCfg<T, MODE>::US;
@@ -905,7 +931,8 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
   unsigned char* moved = reinterpret_cast<unsigned char*>(As1 + 64 * AS);  // RG flags
 
   const int tid = threadIdx.x;
-  const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, k0, false);
+  StepItem it;
+  if (!update_item(sa, items, k0, part, it)) return;
   if (it.kind == kSegLeft) return;
   const SysDesc d = step_desc(sa, it.sys);
   const StepScratchT<T>* sc = sa.scratch + d.pad_;
@@ -990,6 +1017,305 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     if (more) cur = nxt;
     b1 = !b1;
     __syncthreads();  // the buffer just read is refilled by the next iteration's prefetch
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_update_tc: the FP32 factors' trailing update on the 5th-generation tensor
+// cores. One CTA per (strip, 512 rows below the panel), 128-row tiles:
+//  * U12^T (64 x 32) and each L21 tile (128 x 32) are staged in shared memory
+//    in the canonical K-major layout without swizzle: 8-row x 16-byte core
+//    matrices, K-adjacent cores 128 bytes apart (leading byte offset), 8-row
+//    groups 1024 bytes apart (stride byte offset);
+//  * one thread issues tcgen05.mma.kind::tf32 (M = 128, N = 64, K = 8, four
+//    per tile; three per K slice for 3xTF32: lo*hi + hi*lo + hi*hi on split
+//    copies) into a 64-column TMEM accumulator and commits to an mbarrier;
+//  * while the tensor core runs, the C tile (128 x 64) streams into shared
+//    memory in 16-byte pieces, piece c of row r stored at piece c ^ (r & 15)
+//    (conflict-free both for the coalesced copies and for one thread reading
+//    a whole row), and the next L21 tile behind it; then tcgen05.ld brings P
+//    back (thread = row), each thread subtracts its row in shared memory, and
+//    the tile is stored coalesced.
+// The mbarrier wait is bounded: past the limit the kernel records a timeout
+// in g_tc_timeouts, skips its stores, frees its TMEM and returns.
+constexpr int TC_M = 128;
+constexpr int TC_LBO = 128;   // bytes between K-adjacent core matrices
+constexpr int TC_SBO = 1024;  // bytes between 8-row groups (8 K-cores of 128 bytes)
+constexpr int TC_TILE_A = TC_M * NB * 4;  // 16 KB: one 128 x 32 FP32 operand
+constexpr int TC_TILE_B = 64 * NB * 4;    //  8 KB: U12^T
+constexpr uint32_t TC_COLS = 64;          // TMEM columns (FP32 accumulator, N = 64)
+__device__ __forceinline__ int tc_csw(int row, int piece) {  // float offset of a staged C piece
+  return row * 64 + ((piece ^ (row & 15)) << 2);
+}
+
+__device__ int g_tc_timeouts = 0;
+
+// byte offset of element (row, k) in a core-matrix K-major operand
+__device__ __forceinline__ int tc_off(int row, int k) {
+  return (row >> 3) * TC_SBO + (k >> 2) * TC_LBO + (row & 7) * 16 + (k & 3) * 4;
+}
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((TC_LBO >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((TC_SBO >> 4) & 0x3FFF) << 32) | (1ull << 46);  // descriptor version 1, no swizzle
+}
+
+// kind::tf32 instruction descriptor: FP32 accumulator, TF32 A and B, both
+// K-major, N = 64, M = 128
+constexpr uint32_t TC_IDESC =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((64u >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(TC_IDESC), "r"(acc));
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+template <int MODE>
+size_t update_tc_smem() {
+  // alignment slack, A raw x2 (prefetch), [A lo], B hi, [B lo], mbarrier +
+  // TMEM slot + abort flag, row flags
+  const int splits = MODE == kUpd3xTf32 ? 1 : 0;
+  return 1024 + (size_t)(2 + splits) * TC_TILE_A + (size_t)(1 + splits) * TC_TILE_B + 64 + RG +
+         sizeof(float) * TC_M * 64;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(UT)
+k_update_tc(StepArgsT<float> sa, const StepItem* __restrict__ items, int k0, int part) {
+  constexpr bool SPLIT = MODE == kUpd3xTf32;
+  extern __shared__ __align__(1024) unsigned char tc_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  unsigned char* Araw[2] = {base, base + TC_TILE_A};
+  unsigned char* Alo = base + 2 * TC_TILE_A;
+  unsigned char* Bhi = Alo + (SPLIT ? TC_TILE_A : 0);
+  unsigned char* Blo = Bhi + TC_TILE_B;
+  unsigned char* tail = Blo + (SPLIT ? TC_TILE_B : 0);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tail);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(tail + 8);
+  int* abort_flag = reinterpret_cast<int*>(tail + 16);
+  unsigned char* moved = tail + 64;
+  float* Cs = reinterpret_cast<float*>(moved + RG);  // staged C tile, TC_M x 64, swizzled pieces
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  StepItem it;
+  if (!update_item(sa, items, k0, part, it)) return;
+  if (it.kind == kSegLeft) return;
+  const SysDesc d = step_desc(sa, it.sys);
+  const StepScratchT<float>* sc = sa.scratch + d.pad_;
+  if (sc->info) return;
+  const int n = d.n;
+  const int rb = k0 + NB + (int)blockIdx.y * RG;
+  if (rb >= n) return;  // includes the last panel (nothing below it)
+  const int re = min(n, rb + RG), w = it.width, c0 = it.c0;
+  const Seg<float> s = segment(sa, d, it.kind, k0);
+  const int64_t ld = s.ld;
+  // step 0 out of place: rows holding a displaced row are already in dst
+  const bool first = s.ident || s.src != s.dst;
+  if (tid == 0) *abort_flag = 0;
+  if (first) {
+    for (int i = tid; i < re - rb; i += UT) moved[i] = 0;
+    __syncthreads();
+    if (tid < sc->ndisp) {
+      const int r = k0 + sc->disp_dst[tid];
+      if (r >= rb && r < re) moved[r - rb] = 1;
+    }
+  }
+  float* const dst = s.dst + c0;
+  const float* const src = s.src + c0;
+  const float* L = sa.LU + d.lu_off;
+  const bool lvec = ((reinterpret_cast<uintptr_t>(L + k0) & 15) == 0) && (n % 4 == 0);
+  // C rows in 16-byte pieces (both the source and the destination of every row)
+  const bool cvec = ld % 4 == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0 &&
+                    (s.ident || (reinterpret_cast<uintptr_t>(src) & 15) == 0);
+
+  // TMEM accumulator (one warp allocates) and the completion barrier
+  if (warp == 0) {
+    const uint32_t slot = static_cast<uint32_t>(__cvta_generic_to_shared(tslot));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(slot), "r"(TC_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  const uint32_t mbar_addr = static_cast<uint32_t>(__cvta_generic_to_shared(mbar));
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(mbar_addr));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+  }
+
+  // A tile: rows r0 .. r0+127 of L21 (zero past re) into the core layout
+  auto stage_a = [&](unsigned char* buf, int r0) {
+    if (lvec) {
+      for (int idx = tid; idx < TC_M * (NB / 4); idx += UT) {
+        const int r = idx >> 3, q = (idx & 7) * 4;
+        const bool ok = r0 + r < re;
+        cp_async_pair(buf + tc_off(r, q), ok ? L + (int64_t)(r0 + r) * n + k0 + q : L + k0, 16, ok ? 16 : 0);
+      }
+    } else {
+      for (int idx = tid; idx < TC_M * NB; idx += UT) {
+        const int r = idx >> 5, q = idx & 31;
+        const bool ok = r0 + r < re;
+        cp_async<4>(buf + tc_off(r, q), ok ? L + (int64_t)(r0 + r) * n + k0 + q : L, ok);
+      }
+    }
+    cp_async_commit();
+  };
+  // U12^T (64 x 32, K-major) from the strip's top rows, split for 3xTF32
+  for (int idx = tid; idx < 64 * NB; idx += UT) {
+    const int c = idx >> 5, q = idx & 31;  // column of the strip, row of U12
+    const float u = c < w ? dst[(int64_t)(k0 + q) * ld + c] : 0.f;
+    if constexpr (SPLIT) {
+      const float hi = __uint_as_float(to_tf32(u));
+      *reinterpret_cast<float*>(Bhi + tc_off(c, q)) = hi;
+      *reinterpret_cast<float*>(Blo + tc_off(c, q)) = __uint_as_float(to_tf32(u - hi));
+    } else {
+      *reinterpret_cast<float*>(Bhi + tc_off(c, q)) = u;
+    }
+  }
+  stage_a(Araw[0], rb);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tslot;
+  const uint32_t a_s[2] = {static_cast<uint32_t>(__cvta_generic_to_shared(Araw[0])),
+                           static_cast<uint32_t>(__cvta_generic_to_shared(Araw[1]))};
+  const uint32_t alo_s = static_cast<uint32_t>(__cvta_generic_to_shared(Alo));
+  const uint32_t bhi_s = static_cast<uint32_t>(__cvta_generic_to_shared(Bhi));
+  const uint32_t blo_s = static_cast<uint32_t>(__cvta_generic_to_shared(Blo));
+
+  int t = 0;
+  for (int r0 = rb; r0 < re; r0 += TC_M, ++t) {
+    const int cur = t & 1;
+    cp_async_wait<0>();
+    __syncthreads();
+    if constexpr (SPLIT) {
+      for (int idx = tid; idx < TC_M * NB; idx += UT) {
+        const int off = tc_off(idx >> 5, idx & 31);
+        float* x = reinterpret_cast<float*>(Araw[cur] + off);
+        const float v = *x;
+        const float hi = __uint_as_float(to_tf32(v));
+        *x = hi;
+        *reinterpret_cast<float*>(Alo + off) = __uint_as_float(to_tf32(v - hi));
+      }
+    }
+    // shared-memory writes of the generic proxy become visible to the tensor core
+    asm volatile("fence.proxy.async.shared::cta;\n" ::);
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+#pragma unroll
+      for (int kk = 0; kk < NB; kk += 8) {
+        const uint32_t koff = (uint32_t)(kk / 4) * TC_LBO;
+        if constexpr (SPLIT) {
+          tc_mma(tmem, tc_desc(alo_s + koff), tc_desc(bhi_s + koff), kk > 0);  // small terms first
+          tc_mma(tmem, tc_desc(a_s[cur] + koff), tc_desc(blo_s + koff), 1);
+          tc_mma(tmem, tc_desc(a_s[cur] + koff), tc_desc(bhi_s + koff), 1);
+        } else {
+          tc_mma(tmem, tc_desc(a_s[cur] + koff), tc_desc(bhi_s + koff), kk > 0);
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(mbar_addr));
+    }
+    // C tile into shared memory (one commit group), then the next A tile
+    // behind it (its buffer was read by the previous tile's products)
+    for (int idx = tid; idx < TC_M * 16; idx += UT) {
+      const int rr = idx >> 4, pc = idx & 15, j = pc * 4, r = r0 + rr;
+      float* cs = Cs + tc_csw(rr, pc);
+      const int valid = (r < re) ? max(0, min(4, w - j)) : 0;
+      const bool fromdst = valid && (!first || moved[r - rb]);
+      if (valid && !fromdst && s.ident) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) cs[e] = (e < valid && r == c0 + j + e) ? 1.f : 0.f;
+      } else if (cvec) {
+        const float* g = valid ? (fromdst ? dst : src) + (int64_t)r * ld + j : dst;
+        cp_async_pair(cs, g, 16, valid * 4);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          if (e < valid) cp_async<4>(cs + e, (fromdst ? dst : src) + (int64_t)r * ld + j + e, true);
+          else cs[e] = 0.f;
+        }
+      }
+    }
+    cp_async_commit();
+    if (r0 + TC_M < re) stage_a(Araw[cur ^ 1], r0 + TC_M);
+    else cp_async_commit();  // keep one group behind the C tile either way
+    const int row = warp * 32 + lane;  // TMEM lane = tile row
+    const int r = r0 + row;
+    const bool live = r < re;
+
+    // wait for the products, bounded
+    uint32_t done = 0;
+    for (int spin = 0; spin < (1 << 22) && !done; ++spin) {
+      asm volatile(
+          "{\n\t.reg .pred q;\n\t"
+          "mbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\n\t"
+          "selp.u32 %0, 1, 0, q;\n\t}\n"
+          : "=r"(done)
+          : "r"(mbar_addr), "r"((uint32_t)(t & 1))
+          : "memory");
+    }
+    if (!done) {
+      *abort_flag = 1;
+      atomicAdd(&g_tc_timeouts, 1);
+    }
+    cp_async_wait<1>();  // the C tile has landed (the next A tile may still be in flight)
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    __syncthreads();
+    if (*abort_flag) break;
+    {
+      float pv[64];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+      for (int j = 0; j < 64; j += 16) tc_ld16(taddr + (uint32_t)j, pv + j);
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+      if (live) {
+#pragma unroll
+        for (int pc = 0; pc < 16; ++pc) {
+          float4* q = reinterpret_cast<float4*>(Cs + tc_csw(row, pc));
+          float4 v = *q;
+          v.x -= pv[4 * pc];
+          v.y -= pv[4 * pc + 1];
+          v.z -= pv[4 * pc + 2];
+          v.w -= pv[4 * pc + 3];
+          *q = v;
+        }
+      }
+    }
+    __syncthreads();
+    for (int idx = tid; idx < TC_M * 16; idx += UT) {
+      const int rr = idx >> 4, pc = idx & 15, j = pc * 4, rg = r0 + rr;
+      if (rg >= re || j >= w) continue;
+      const float4 v = *reinterpret_cast<const float4*>(Cs + tc_csw(rr, pc));
+      float* o = dst + (int64_t)rg * ld + j;
+      if (cvec && j + 4 <= w) {
+        *reinterpret_cast<float4*>(o) = v;
+      } else {
+        const float e4[4] = {v.x, v.y, v.z, v.w};
+        for (int e = 0; e < 4 && j + e < w; ++e) o[e] = e4[e];
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+    __syncthreads();  // TMEM read and A lo consumed before the next tile's products
+  }
+  cp_async_wait<0>();
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TC_COLS));
   }
 }
 
@@ -1431,6 +1757,16 @@ cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, 
 
 }  // namespace
 
+int tc_timeouts_take() {
+  int h = 0;
+  if (cudaMemcpyFromSymbol(&h, g_tc_timeouts, sizeof(int)) != cudaSuccess) return -1;
+  if (h) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_tc_timeouts, &z, sizeof(int));
+  }
+  return h;
+}
+
 template <class T>
 cudaError_t prepare_narrow() {
   cudaError_t e = cudaFuncSetAttribute(k_tri_narrow<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1448,6 +1784,12 @@ cudaError_t step_prepare() {
   if (e == cudaSuccess) e = prepare_update<float, kUpdTf32>();
   if (e == cudaSuccess) e = prepare_update<float, kUpdBf16>();
   if (e == cudaSuccess) e = prepare_update<float, kUpd3xTf32>();
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_tc<kUpdTf32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)update_tc_smem<kUpdTf32>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_update_tc<kUpd3xTf32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)update_tc_smem<kUpd3xTf32>());
   return e;
 }
 
@@ -1484,30 +1826,49 @@ cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, 
 }
 
 template <class T>
-cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
-                          cudaStream_t st) {
+cudaError_t launch_rows(const StepArgsT<T>& sa, const StepItem* items, int nitems, int k0, cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
   k_rows<T><<<nitems, UT, 0, st>>>(sa, items, k0);
-  cudaError_t e = cudaGetLastError();
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_trailing(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0, int part,
+                            cudaStream_t st) {
   const int below = nmax - k0 - NB;
-  if (e != cudaSuccess || below <= 0) return e;
+  if (nitems <= 0 || below <= 0) return cudaSuccess;
   const dim3 grid((unsigned)nitems, (unsigned)((below + RG - 1) / RG));
   if constexpr (std::is_same_v<T, float>) {
-    if (sa.umode == kUpdTf32) {
-      k_update<T, kUpdTf32><<<grid, UT, update_smem<T, kUpdTf32>(), st>>>(sa, items, k0);
-      return cudaGetLastError();
-    }
-    if (sa.umode == kUpdBf16) {
-      k_update<T, kUpdBf16><<<grid, UT, update_smem<T, kUpdBf16>(), st>>>(sa, items, k0);
-      return cudaGetLastError();
-    }
-    if (sa.umode == kUpd3xTf32) {
-      k_update<T, kUpd3xTf32><<<grid, UT, update_smem<T, kUpd3xTf32>(), st>>>(sa, items, k0);
-      return cudaGetLastError();
+    switch (sa.umode) {
+      case kUpdTf32:
+        k_update<T, kUpdTf32><<<grid, UT, update_smem<T, kUpdTf32>(), st>>>(sa, items, k0, part);
+        return cudaGetLastError();
+      case kUpdBf16:
+        k_update<T, kUpdBf16><<<grid, UT, update_smem<T, kUpdBf16>(), st>>>(sa, items, k0, part);
+        return cudaGetLastError();
+      case kUpd3xTf32:
+        k_update<T, kUpd3xTf32><<<grid, UT, update_smem<T, kUpd3xTf32>(), st>>>(sa, items, k0, part);
+        return cudaGetLastError();
+      case kUpdTcTf32:
+        k_update_tc<kUpdTf32><<<grid, UT, update_tc_smem<kUpdTf32>(), st>>>(sa, items, k0, part);
+        return cudaGetLastError();
+      case kUpdTc3xTf32:
+        k_update_tc<kUpd3xTf32><<<grid, UT, update_tc_smem<kUpd3xTf32>(), st>>>(sa, items, k0, part);
+        return cudaGetLastError();
+      default:
+        break;
     }
   }
-  k_update<T, kUpdFp32><<<grid, UT, update_smem<T, kUpdFp32>(), st>>>(sa, items, k0);
+  k_update<T, kUpdFp32><<<grid, UT, update_smem<T, kUpdFp32>(), st>>>(sa, items, k0, part);
   return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
+                          cudaStream_t st) {
+  cudaError_t e = launch_rows(sa, items, nitems, k0, st);
+  if (e != cudaSuccess) return e;
+  return launch_trailing(sa, items, nitems, nmax, k0, 0, st);
 }
 
 template <class T>
@@ -1532,6 +1893,9 @@ cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int ni
 #define NPPB_STEP_INSTANTIATE(T)                                                                          \
   template cudaError_t launch_panel<T>(const StepArgsT<T>&, const int32_t*, int, int, int, cudaStream_t);     \
   template cudaError_t launch_update<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);   \
+  template cudaError_t launch_rows<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);          \
+  template cudaError_t launch_trailing<T>(const StepArgsT<T>&, const StepItem*, int, int, int, int,          \
+                                          cudaStream_t);                                                     \
   template cudaError_t launch_back<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);          \
   template cudaError_t launch_forward<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t, bool);
 NPPB_STEP_INSTANTIATE(double)

@@ -49,7 +49,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   }
   const int arith = flags & (NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA);
   if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 |
-                 NPPB_MIXED_FP32_FMA)) ||
+                 NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05)) ||
       (arith & (arith - 1))) {
     set_error("unknown mixed flag bits, or more than one of TF32 / BF16 / FP32_FMA");
     return NPPB_E_ARG;
@@ -103,8 +103,19 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     sa.un = n;
     sa.unrhs = nrhs;
     sa.uleft = 1;
-    sa.umode = (flags & NPPB_MIXED_BF16) ? 2 : (flags & NPPB_MIXED_TF32) ? 1 : (flags & NPPB_MIXED_FP32_FMA) ? 0 : 3;
+    const bool tc = (flags & NPPB_MIXED_TCGEN05) != 0;
+    sa.umode = (flags & NPPB_MIXED_BF16) ? 2
+               : (flags & NPPB_MIXED_TF32) ? (tc ? 4 : 1)
+               : (flags & NPPB_MIXED_FP32_FMA) ? 0
+               : (tc ? 5 : 3);
     NPPB_CUDA(run_step_uniform<float>(sa, count, st), "FP32 factorisation");
+    if (tc && (sa.umode == 4 || sa.umode == 5)) {
+      NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+      if (tc_timeouts_take() != 0) {
+        set_error("tensor-core trailing update: a completion wait ran out");
+        return NPPB_E_CUDA;
+      }
+    }
     NPPB_CUDA(mixed_mark_fp32_failures(info32.as<int32_t>(), S, count, st), "mark");
     NPPB_CUDA(mixed_row_positions(piv.as<int32_t>(), count, n, rpos.as<int32_t>(), st), "row positions");
     NPPB_CUDA(mixed_apply(dX, y32.as<float>(), csm.as<double>(), count, n, nrhs, S, 1, st), "apply");

@@ -60,7 +60,8 @@ struct StepArgsT {
   // scratch slot s; an inverse for every system when uinv != 0.
   int un, unrhs, uinv;
   int uleft;         // uniform batch keeps its factors: carry row moves left of each panel
-  int umode;         // FP32 factors: trailing product in FP32 FMA (0), TF32 (1), BF16 (2) or 3xTF32 (3) tensor-core arithmetic
+  int umode;         // FP32 factors: trailing product in FP32 FMA (0), TF32 (1), BF16 (2), 3xTF32 (3) on mma.sync,
+                     // or TF32 (4) / 3xTF32 (5) on tcgen05 with TMEM accumulators
 };
 using StepArgs = StepArgsT<double>;
 
@@ -76,6 +77,9 @@ __host__ __device__ inline int uniform_back_strips(int n, int nrhs, int inv) {
 }
 
 cudaError_t step_prepare();
+// Bounded waits of the tensor-core update that ran out since the last call
+// (each such CTA skipped its stores); the counter is reset. -1: unreadable.
+int tc_timeouts_take();
 // Panel of every listed system at column k0; mmax = largest n - k0 among them.
 // list == nullptr: systems 0..nsys-1 of a uniform batch. Likewise items ==
 // nullptr below means the uniform-batch items, derived from the block index.
@@ -84,6 +88,15 @@ template <class T>
 cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st);
 // Row moves + U12 + trailing update for each strip item of step k0 (nmax >= n of any item).
+// launch_update = launch_rows, then launch_trailing with part 0. A uniform
+// batch (items == nullptr) can split the trailing update for look-ahead:
+// part 1 launches only the first matrix strip of every system (nitems =
+// systems), part 2 every other strip (nitems = all strips).
+template <class T>
+cudaError_t launch_rows(const StepArgsT<T>& sa, const StepItem* items, int nitems, int k0, cudaStream_t st);
+template <class T>
+cudaError_t launch_trailing(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0, int part,
+                            cudaStream_t st);
 template <class T>
 cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int k0,
                           cudaStream_t st);

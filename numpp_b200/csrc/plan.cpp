@@ -187,7 +187,6 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
   std::vector<StepItem> items, back;
   step_flops = step_bytes = 0.0;
   for (int32_t i : step_members) add_cost(desc[i], step_flops, step_bytes);
-  if (const char* e = std::getenv("NPPB_CHAINS")) nchains = std::max(1, std::atoi(e));
   if (nstep_sys) {
     step_nmax = desc[step_members[0]].n;
     const int G = (int)std::min<int64_t>(nchains, nstep_sys);
@@ -553,7 +552,7 @@ std::shared_ptr<Plan> uniform_plan(int64_t count, int32_t n, int32_t nrhs, int f
 using nppb::Plan;
 
 struct nppb_plan {
-  Plan p;
+  std::unique_ptr<Plan> pp = std::make_unique<Plan>();
   // Host-buffer execution pipelined over chunks of systems: the copy of chunk
   // c+1 runs while chunk c computes (needs a packed layout: offsets ascending).
   struct Chunk {
@@ -627,7 +626,8 @@ int nppb_plan_create(nppb_plan** plan, int64_t count, const int32_t* n, const in
     }
     *plan = nullptr;
     auto* pl = new nppb_plan();
-    const int rc = pl->p.build(count, n, nrhs, a_off, b_off, inv_off, flags & ~NPPB_WANT_LU, false, true);
+    if (const char* e = std::getenv("NPPB_CHAINS")) pl->pp->nchains = std::max(1, std::atoi(e));
+    const int rc = pl->pp->build(count, n, nrhs, a_off, b_off, inv_off, flags & ~NPPB_WANT_LU, false, true);
     if (rc != NPPB_OK) {
       delete pl;
       return rc;
@@ -668,9 +668,9 @@ int nppb_plan_sizes(const nppb_plan* plan, int64_t* a_elems, int64_t* b_elems, i
     nppb::set_error("plan is null");
     return NPPB_E_ARG;
   }
-  if (a_elems) *a_elems = plan->p.a_elems;
-  if (b_elems) *b_elems = plan->p.b_elems;
-  if (inv_elems) *inv_elems = plan->p.inv_elems;
+  if (a_elems) *a_elems = plan->pp->a_elems;
+  if (b_elems) *b_elems = plan->pp->b_elems;
+  if (inv_elems) *inv_elems = plan->pp->inv_elems;
   return NPPB_OK;
 }
 
@@ -681,11 +681,11 @@ int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, doubl
       nppb::set_error("plan is null");
       return NPPB_E_ARG;
     }
-    if (plan->p.a_elems && !dA) {
+    if (plan->pp->a_elems && !dA) {
       nppb::set_error("A is null");
       return NPPB_E_ARG;
     }
-    return plan->p.execute(dev_ptrs(plan->p, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo),
+    return plan->pp->execute(dev_ptrs(*plan->pp, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo),
                            static_cast<cudaStream_t>(stream));
   });
 }
@@ -698,7 +698,7 @@ int build_chunks(nppb_plan& P) {
   if (!P.chunks.empty()) return NPPB_OK;
   int K = 4;
   if (const char* e = std::getenv("NPPB_HOST_CHUNKS")) K = std::max(1, std::atoi(e));
-  const int64_t count = P.p.count;
+  const int64_t count = P.pp->count;
   K = (int)std::min<int64_t>(K, std::max<int64_t>(1, count / 256));
   for (int c = 0; c < K; ++c) {
     nppb_plan::Chunk ch;
@@ -745,6 +745,67 @@ int build_chunks(nppb_plan& P) {
 
 }  // namespace
 
+int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,
+                       double* dDet, double* dSign, double* dLogabs, int32_t* dinfo, void* stream,
+                       int32_t* chains_out, float* ms_out) {
+  return guarded([&]() -> int {
+    if (!plan) {
+      nppb::set_error("plan is null");
+      return NPPB_E_ARG;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+      return nppb::cuda_status(cudaGetLastError(), "event");
+    struct Events {
+      cudaEvent_t a, b;
+      ~Events() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+      }
+    } ev{e0, e1};
+    // candidates are built fresh; the plan's own Plan stays in place until a
+    // timed candidate replaces it
+    const int64_t count = (int64_t)plan->n.size();
+    const int64_t nstep = plan->pp->nstep_sys;
+    std::unique_ptr<Plan> best;
+    float best_ms = 0.f;
+    int rc = NPPB_OK;
+    for (int c : {1, 2, 3, 4, 6}) {
+      if (c > 1 && c > nstep) break;  // more chains than step-wise systems change nothing
+      auto cand = std::make_unique<Plan>();
+      cand->nchains = c;
+      rc = cand->build(count, plan->n.data(), plan->nrhs.data(), plan->a_off.data(), plan->b_off.data(),
+                       plan->inv_off.data(), plan->flags, false, true);
+      if (rc != NPPB_OK) break;
+      const Plan::Ptrs p = dev_ptrs(*cand, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo);
+      rc = cand->execute(p, st);  // warm-up (and graph capture)
+      if (rc == NPPB_OK && cudaEventRecord(e0, st) != cudaSuccess) rc = NPPB_E_CUDA;
+      for (int r = 0; r < 2 && rc == NPPB_OK; ++r) rc = cand->execute(p, st);
+      float ms = 0.f;
+      if (rc == NPPB_OK) {
+        cudaError_t x = cudaEventRecord(e1, st);
+        if (x == cudaSuccess) x = cudaEventSynchronize(e1);
+        if (x == cudaSuccess) x = cudaEventElapsedTime(&ms, e0, e1);
+        if (x != cudaSuccess) rc = nppb::cuda_status(x, "autotune timing");
+      }
+      if (rc != NPPB_OK) break;
+      ms /= 2.f;
+      if (!best || ms < best_ms) {
+        best_ms = ms;
+        best = std::move(cand);
+      }
+    }
+    // a failed candidate may still be in flight on `st`: drain before it is freed
+    cudaStreamSynchronize(st);
+    if (best) plan->pp = std::move(best);
+    if (rc != NPPB_OK) return rc;
+    if (chains_out) *chains_out = plan->pp->nchains;
+    if (ms_out) *ms_out = best_ms;
+    return NPPB_OK;
+  });
+}
+
 int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X, double* Inv,
                            double* Det, double* Sign, double* Logabs, int32_t* info) {
   return guarded([&]() -> int {
@@ -752,7 +813,7 @@ int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, do
       nppb::set_error("plan is null");
       return NPPB_E_ARG;
     }
-    Plan& pl = plan->p;
+    Plan& pl = *plan->pp;
     const int f = pl.flags;
     const size_t c = (size_t)pl.count;
     int rc = ensure((void**)&pl.hA, sizeof(double) * pl.a_elems);
@@ -847,17 +908,17 @@ int nppb_plan_destroy(nppb_plan* plan) {
   return NPPB_OK;
 }
 
-int nppb_plan_num_classes(const nppb_plan* plan) { return plan ? plan->p.num_kernel_groups() : 0; }
+int nppb_plan_num_classes(const nppb_plan* plan) { return plan ? plan->pp->num_kernel_groups() : 0; }
 
-int nppb_plan_num_launches(const nppb_plan* plan) { return plan ? plan->p.launches_per_execute() : 0; }
+int nppb_plan_num_launches(const nppb_plan* plan) { return plan ? plan->pp->launches_per_execute() : 0; }
 
 int nppb_plan_class_info(const nppb_plan* plan, int c, int* is_warp, int* bound, int64_t* systems,
                          double* flops, double* bytes) {
-  if (!plan || c < 0 || c >= plan->p.num_kernel_groups()) {
+  if (!plan || c < 0 || c >= plan->pp->num_kernel_groups()) {
     nppb::set_error("bad plan or class index");
     return NPPB_E_ARG;
   }
-  const Plan& pl = plan->p;
+  const Plan& pl = *plan->pp;
   if (c < (int)pl.warp_classes.size()) {
     const auto& w = pl.warp_classes[c];
     if (is_warp) *is_warp = 1;
@@ -883,7 +944,7 @@ int nppb_plan_time_classes(nppb_plan* plan, const double* dA, const double* dB, 
       nppb::set_error("bad plan, reps or ms_out");
       return NPPB_E_ARG;
     }
-    Plan& pl = plan->p;
+    Plan& pl = *plan->pp;
     const Plan::Ptrs p = dev_ptrs(pl, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaEvent_t e0, e1;
@@ -916,7 +977,7 @@ int nppb_plan_time_kernels(nppb_plan* plan, const double* dA, const double* dB, 
       nppb::set_error("bad plan or ms_out");
       return NPPB_E_ARG;
     }
-    Plan& pl = plan->p;
+    Plan& pl = *plan->pp;
     if (flops_out)
       for (int k = 0; k < Plan::kKinds; ++k) flops_out[k] = pl.kind_flops[k];
     return pl.time_kernels(dev_ptrs(pl, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo),
@@ -931,7 +992,7 @@ int nppb_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, con
   nppb_plan* pl = nullptr;
   int rc = nppb_plan_create(&pl, count, n, nrhs, a_off, b_off, inv_off, flags);
   if (rc != NPPB_OK) return rc;
-  pl->p.use_graph = false;  // a one-shot call gains nothing from capture
+  pl->pp->use_graph = false;  // a one-shot call gains nothing from capture
   rc = nppb_plan_execute_host(pl, A, B, X, Inv, Det, Sign, Logabs, info);
   nppb_plan_destroy(pl);
   return rc;

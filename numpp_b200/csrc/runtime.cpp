@@ -114,18 +114,78 @@ void DevMem::release() {
 
 cudaError_t prepare_kernels() { return step_prepare(); }
 
+namespace {
+
+// A side stream and two events per device for the look-ahead of the current
+// thread's uniform factorisations (created on first use, kept for the thread).
+struct Lookahead {
+  cudaStream_t side = nullptr;
+  cudaEvent_t first = nullptr, rest = nullptr;
+};
+
+Lookahead* lookahead_for_device() {
+  struct Holder {
+    std::vector<Lookahead> per_dev;
+    ~Holder() {
+      for (auto& l : per_dev) {
+        if (l.side) cudaStreamDestroy(l.side);
+        if (l.first) cudaEventDestroy(l.first);
+        if (l.rest) cudaEventDestroy(l.rest);
+      }
+    }
+  };
+  thread_local Holder h;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  if ((int)h.per_dev.size() <= dev) h.per_dev.resize(dev + 1);
+  Lookahead& l = h.per_dev[dev];
+  if (!l.side) {
+    if (cudaStreamCreateWithFlags(&l.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&l.first, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&l.rest, cudaEventDisableTiming) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  return &l;
+}
+
+}  // namespace
+
+// Uniform factorisation with look-ahead: after the row moves of step k, the
+// strip that holds the next panel's columns is updated first; the next panel
+// then runs on `st` while the other strips update on a side stream, and the
+// next step's row moves wait for both. Every element sees the same
+// operations in the same order as without look-ahead. Step 0 keeps the plain
+// order: its out-of-place update reads the panel's row-move lists, which the
+// next panel overwrites.
 template <class T>
 cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st) {
   const int n = sa.un;
   if (n <= 32 || n > kStepMaxN || count <= 0) return cudaErrorInvalidValue;
-  for (int k0 = 0; k0 < n; k0 += kStepNB) {
-    cudaError_t e = launch_panel(sa, nullptr, count, n - k0, k0, st);
-    if (e != cudaSuccess) return e;
+  Lookahead* la = lookahead_for_device();
+  cudaError_t e = launch_panel(sa, nullptr, count, n, 0, st);
+  for (int k0 = 0; k0 < n && e == cudaSuccess; k0 += kStepNB) {
     const int64_t items = (int64_t)count * uniform_update_strips(n, sa.unrhs, sa.uinv, k0, sa.uleft);
     if (items > INT32_MAX) return cudaErrorInvalidValue;
-    e = launch_update(sa, nullptr, (int)items, n, k0, st);
-    if (e != cudaSuccess) return e;
+    const bool next = k0 + kStepNB < n;
+    e = launch_rows(sa, nullptr, (int)items, k0, st);
+    if (e != cudaSuccess) break;
+    if (!next) break;  // last panel: nothing below it
+    if (k0 == 0 || !la) {
+      e = launch_trailing(sa, nullptr, (int)items, n, k0, 0, st);
+      if (e == cudaSuccess) e = launch_panel(sa, nullptr, count, n - k0 - kStepNB, k0 + kStepNB, st);
+      continue;
+    }
+    e = launch_trailing(sa, nullptr, count, n, k0, 1, st);
+    if (e == cudaSuccess) e = cudaEventRecord(la->first, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(la->side, la->first, 0);
+    if (e == cudaSuccess) e = launch_trailing(sa, nullptr, (int)items, n, k0, 2, la->side);
+    if (e == cudaSuccess) e = cudaEventRecord(la->rest, la->side);
+    if (e == cudaSuccess) e = launch_panel(sa, nullptr, count, n - k0 - kStepNB, k0 + kStepNB, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, la->rest, 0);
   }
+  if (e != cudaSuccess) return e;
   const int64_t back = (int64_t)count * uniform_back_strips(n, sa.unrhs, sa.uinv);
   if (back > INT32_MAX) return cudaErrorInvalidValue;
   return launch_back(sa, nullptr, (int)back, sa.un, sa.uinv ? 64 : std::min(64, sa.unrhs), st);

@@ -84,6 +84,30 @@ def test_plan_device_buffers_torch(lib, oracle):
     plan.close()
 
 
+def test_plan_autotune_keeps_a_working_plan(lib, oracle):
+    """The autotuner times chain counts on the caller's buffers and keeps the
+    fastest; the plan it keeps gives the reference's results."""
+    torch = pytest.importorskip("torch")
+    sys = workloads.uneven_batch(seed=14, count=300, n_lo=2, n_hi=300)
+    plan = Plan(sys, FLAGS)
+    dev = torch.device("cuda:0")
+    cnt = len(sys["n"])
+    dA = torch.from_numpy(sys["A"]).to(dev)
+    dB = torch.from_numpy(sys["B"]).to(dev)
+    dX = torch.zeros_like(dB)
+    dInv = torch.zeros(max(plan.inv_elems, 1), dtype=torch.float64, device=dev)
+    d = [torch.zeros(cnt, dtype=torch.float64, device=dev) for _ in range(3)]
+    dinfo = torch.zeros(cnt, dtype=torch.int32, device=dev)
+    chains, ms = plan.autotune(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
+    assert chains in (1, 2, 3, 4, 6) and ms > 0
+    dX.zero_()
+    plan.execute(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
+    torch.cuda.synchronize()
+    check_vs_oracle(sys, dX.cpu().numpy(), dInv.cpu().numpy(), d[0].cpu().numpy(), d[1].cpu().numpy(),
+                    d[2].cpu().numpy(), dinfo.cpu().numpy(), oracle)
+    plan.close()
+
+
 def test_full_uneven_batch_properties(lib):
     """8192 systems, n log-uniform in [4, 512], nrhs in {1, 8, 32}, inverse for 10%."""
     sys = workloads.uneven_batch(seed=2025)

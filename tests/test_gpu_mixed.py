@@ -92,3 +92,22 @@ def test_bf16_factors_fall_back_when_too_rough(lib):
     X, rep = solve_mixed(A, B, X_true=Xt, factor="bf16")
     assert np.all(rep["berr"] <= 1e-10), rep["berr"]
     assert np.all(rep["fallback"] == 1)
+
+
+@pytest.mark.parametrize("factor", ["3xtf32", "tf32"])
+@pytest.mark.parametrize("n", [96, 301, 1030])
+def test_tcgen05_update_matches_mma_sync(lib, factor, n):
+    """The tcgen05 (TMEM accumulator) trailing update and the mma.sync one give
+    factors of the same quality: same corrections, no fallback, close solutions.
+    n = 301 takes the 4-byte staging path (rows not 16-byte aligned), 1030 several
+    128-row tiles and 512-row groups."""
+    kappa = 1e2 if factor == "tf32" else 1e4
+    A, B, Xt = workloads.conditioned_batch(seed=60 + n, count=3, n=n, kappa=kappa, nrhs=2)
+    Xa, ra = solve_mixed(A, B, X_true=Xt, factor=factor, max_iter=30, tcgen05=True)
+    Xb, rb = solve_mixed(A, B, X_true=Xt, factor=factor, max_iter=30)
+    for rep in (ra, rb):
+        assert np.all(rep["berr"] <= 1e-10), rep["berr"]
+        assert np.all(rep["fallback"] == 0), rep
+    assert np.all(np.abs(ra["iters"] - rb["iters"]) <= 1), (ra["iters"], rb["iters"])
+    rel = np.abs(Xa - Xb).max(axis=(1, 2)) / np.abs(Xb).max(axis=(1, 2))
+    assert np.all(rel <= 10 * kappa * 1e-10), rel
