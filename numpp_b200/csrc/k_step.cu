@@ -851,6 +851,7 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
 // rows stream into shared memory (cp.async, 16-byte pieces when aligned) and
 // its accumulator inputs into registers (paired loads when aligned).
 constexpr int RG = 512;
+constexpr int RG1 = 128;  // rows per CTA of the look-ahead strip (part 1): short critical path
 
 // Shared row strides (elements) for bank-conflict-free fragment reads; every
 // row starts on a 16-byte boundary.
@@ -938,9 +939,10 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) 
   const StepScratchT<T>* sc = sa.scratch + d.pad_;
   if (sc->info) return;
   const int n = d.n;
-  const int rb = k0 + NB + (int)blockIdx.y * RG;
+  const int rg = part == 1 ? RG1 : RG;  // rows per CTA
+  const int rb = k0 + NB + (int)blockIdx.y * rg;
   if (rb >= n) return;  // includes the last panel (nothing below it)
-  const int re = min(n, rb + RG), w = it.width, c0 = it.c0;
+  const int re = min(n, rb + rg), w = it.width, c0 = it.c0;
   const Seg<T> s = segment(sa, d, it.kind, k0);
   const int64_t ld = s.ld;
   // step 0 out of place: rows holding a displaced row are already in dst
@@ -1119,9 +1121,10 @@ k_update_tc(StepArgsT<float> sa, const StepItem* __restrict__ items, int k0, int
   const StepScratchT<float>* sc = sa.scratch + d.pad_;
   if (sc->info) return;
   const int n = d.n;
-  const int rb = k0 + NB + (int)blockIdx.y * RG;
+  const int rg = part == 1 ? RG1 : RG;  // rows per CTA
+  const int rb = k0 + NB + (int)blockIdx.y * rg;
   if (rb >= n) return;  // includes the last panel (nothing below it)
-  const int re = min(n, rb + RG), w = it.width, c0 = it.c0;
+  const int re = min(n, rb + rg), w = it.width, c0 = it.c0;
   const Seg<float> s = segment(sa, d, it.kind, k0);
   const int64_t ld = s.ld;
   // step 0 out of place: rows holding a displaced row are already in dst
@@ -1837,7 +1840,8 @@ cudaError_t launch_trailing(const StepArgsT<T>& sa, const StepItem* items, int n
                             cudaStream_t st) {
   const int below = nmax - k0 - NB;
   if (nitems <= 0 || below <= 0) return cudaSuccess;
-  const dim3 grid((unsigned)nitems, (unsigned)((below + RG - 1) / RG));
+  const int rg = part == 1 ? RG1 : RG;
+  const dim3 grid((unsigned)nitems, (unsigned)((below + rg - 1) / rg));
   if constexpr (std::is_same_v<T, float>) {
     switch (sa.umode) {
       case kUpdTf32:

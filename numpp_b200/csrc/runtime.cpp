@@ -119,8 +119,10 @@ namespace {
 // A side stream and two events per device for the look-ahead of the current
 // thread's uniform factorisations (created on first use, kept for the thread).
 struct Lookahead {
-  cudaStream_t side = nullptr;
-  cudaEvent_t first = nullptr, rest = nullptr;
+  cudaStream_t side = nullptr;   // the rest of the trailing update
+  cudaStream_t panel = nullptr;  // the next panel, at the highest stream priority: its
+                                 // clusters take SMs ahead of the update's CTAs
+  cudaEvent_t first = nullptr, rest = nullptr, next = nullptr;
 };
 
 Lookahead* lookahead_for_device() {
@@ -128,9 +130,10 @@ Lookahead* lookahead_for_device() {
     std::vector<Lookahead> per_dev;
     ~Holder() {
       for (auto& l : per_dev) {
-        if (l.side) cudaStreamDestroy(l.side);
-        if (l.first) cudaEventDestroy(l.first);
-        if (l.rest) cudaEventDestroy(l.rest);
+        for (cudaStream_t t : {l.side, l.panel})
+          if (t) cudaStreamDestroy(t);
+        for (cudaEvent_t e : {l.first, l.rest, l.next})
+          if (e) cudaEventDestroy(e);
       }
     }
   };
@@ -140,9 +143,13 @@ Lookahead* lookahead_for_device() {
   if ((int)h.per_dev.size() <= dev) h.per_dev.resize(dev + 1);
   Lookahead& l = h.per_dev[dev];
   if (!l.side) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (cudaStreamCreateWithFlags(&l.side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&l.panel, cudaStreamNonBlocking, greatest) != cudaSuccess ||
         cudaEventCreateWithFlags(&l.first, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&l.rest, cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreateWithFlags(&l.rest, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&l.next, cudaEventDisableTiming) != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -154,8 +161,8 @@ Lookahead* lookahead_for_device() {
 
 // Uniform factorisation with look-ahead: after the row moves of step k, the
 // strip that holds the next panel's columns is updated first; the next panel
-// then runs on `st` while the other strips update on a side stream, and the
-// next step's row moves wait for both. Every element sees the same
+// then runs on a high-priority stream while the other strips update on a side
+// stream, and the next step's row moves (on `st`) wait for both. Every element sees the same
 // operations in the same order as without look-ahead. Step 0 keeps the plain
 // order: its out-of-place update reads the panel's row-move lists, which the
 // next panel overwrites.
@@ -179,10 +186,13 @@ cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st)
     }
     e = launch_trailing(sa, nullptr, count, n, k0, 1, st);
     if (e == cudaSuccess) e = cudaEventRecord(la->first, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(la->panel, la->first, 0);
+    if (e == cudaSuccess) e = launch_panel(sa, nullptr, count, n - k0 - kStepNB, k0 + kStepNB, la->panel);
+    if (e == cudaSuccess) e = cudaEventRecord(la->next, la->panel);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(la->side, la->first, 0);
     if (e == cudaSuccess) e = launch_trailing(sa, nullptr, (int)items, n, k0, 2, la->side);
     if (e == cudaSuccess) e = cudaEventRecord(la->rest, la->side);
-    if (e == cudaSuccess) e = launch_panel(sa, nullptr, count, n - k0 - kStepNB, k0 + kStepNB, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, la->next, 0);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(st, la->rest, 0);
   }
   if (e != cudaSuccess) return e;
