@@ -450,7 +450,7 @@ def run_b200(args):
     bufs = (dA, dB, dX, dInv, dDet, dSign, dLog, dInfo)
     stream = torch.cuda.Stream()
     # the plan's chain count, tuned on these buffers before anything is timed
-    chains, _ = plan.autotune(*bufs, stream=stream)
+    chains, lookahead, _ = plan.autotune(*bufs, stream=stream)
     nlaunch = plan.launches()
 
     def step():
@@ -559,7 +559,7 @@ def run_b200(args):
             "data": "synthetic (PCG64 default_rng, seed %d + rank)" % SEED,
             "config": {"workload": WORKLOAD, "count": cnt, "parallelism": f"replicas{world}",
                        "l2": "inputs (%.2f GB of A) larger than L2; no flush" % (8 * plan.a_elems / 1e9),
-                       "graph": True, "autotuned_chains": chains,
+                       "graph": True, "autotuned_chains": chains, "autotuned_lookahead": lookahead,
                        "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls]},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "gflops": flops_step * world / (ms_step * 1e-3) / 1e9,

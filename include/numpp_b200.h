@@ -233,8 +233,10 @@ int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, doubl
                       int32_t* dinfo, void* stream);
 /* Autotuner (no reference counterpart): times the plan with 1, 2, 3, 4 and 6
  * independent step chains (graph branches whose panels overlap each other's
- * updates) on these device buffers, a warm-up and two replays each, and keeps
- * the fastest; *chains_out = the chain count kept, *ms_out = its time per
+ * updates), each with and without look-ahead (the next panels overlapping
+ * the current trailing update inside a chain), on these device buffers, a
+ * warm-up and two replays each, and keeps the fastest; *chains_out = the
+ * chain count kept, negated when look-ahead is on; *ms_out = its time per
  * execution. The outputs are written as by nppb_plan_execute; synchronises
  * `stream`. */
 int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,

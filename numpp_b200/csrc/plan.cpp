@@ -81,6 +81,9 @@ Plan::~Plan() {
   if (exec) cudaGraphExecDestroy(exec);
   if (graph) cudaGraphDestroy(graph);
   for (auto s : side) cudaStreamDestroy(s);
+  for (auto s : la_side) cudaStreamDestroy(s);
+  for (auto e : la_first) cudaEventDestroy(e);
+  for (auto e : la_rest) cudaEventDestroy(e);
   for (auto e : join) cudaEventDestroy(e);
   if (fork) cudaEventDestroy(fork);
   if (done) cudaEventDestroy(done);
@@ -220,6 +223,9 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
           }
           st.item_first = (int64_t)items.size();
           st.nmax = ch.nmax;
+          // the first matrix strip of every system (it holds the next panel's
+          // columns) ahead of the other strips, for look-ahead
+          std::vector<StepItem> rest;
           for (int64_t r = 0; r < act; ++r) {
             const int32_t si = list[first + r];
             const SysDesc& s = desc[si];
@@ -229,11 +235,18 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
               for (int j = 0; j < (int)kb; ++j) kind_flops[kKindPanel] += (m - j - 1) * (1.0 + 2.0 * (kb - j - 1));
               kind_flops[kKindUpdate] += kb * kb * w + 2.0 * (m - kb) * kb * w;
             }
-            add_strips(items, si, kSegMatrix, k0 + kStepNB, s.n);
-            if (solve && s.nrhs) add_strips(items, si, kSegRhs, 0, s.nrhs);
-            if (s.inv_off >= 0) add_strips(items, si, kSegInv, 0, s.n);
-            if ((fl & NPPB_WANT_LU) && k0 > 0) add_strips(items, si, kSegLeft, 0, k0);
+            std::vector<StepItem> mat;
+            add_strips(mat, si, kSegMatrix, k0 + kStepNB, s.n);
+            if (!mat.empty()) {
+              items.push_back(mat[0]);
+              rest.insert(rest.end(), mat.begin() + 1, mat.end());
+            }
+            if (solve && s.nrhs) add_strips(rest, si, kSegRhs, 0, s.nrhs);
+            if (s.inv_off >= 0) add_strips(rest, si, kSegInv, 0, s.n);
+            if ((fl & NPPB_WANT_LU) && k0 > 0) add_strips(rest, si, kSegLeft, 0, k0);
           }
+          st.nfirst = (int64_t)items.size() - st.item_first;
+          items.insert(items.end(), rest.begin(), rest.end());
           st.item_count = (int64_t)items.size() - st.item_first;
           ch.steps.push_back(st);
         }
@@ -267,6 +280,10 @@ int Plan::build(int64_t cnt, const int32_t* n, const int32_t* nrhs, const int64_
     }
     step_members.swap(list);
   }
+  // look-ahead pays when panels are long (orders above 512); many small
+  // systems already fill the GPU in every launch
+  if (lookahead_mode < 0) lookahead = step_nmax > 512;
+  else lookahead = lookahead_mode != 0;
   nback = (int64_t)back.size();
 
   int rc = upload(&d_desc, desc, alloc_stream);
@@ -353,15 +370,62 @@ cudaError_t Plan::launch_chain(const Ptrs& p, int c, cudaStream_t st) const {
     if (e != cudaSuccess) return e;
     return substitute(sa, ch, st, false);
   }
-  for (const Step& s : ch.steps) {
+  // Look-ahead (from step 1 on: step 0's out-of-place update reads the row-move
+  // lists the next panel overwrites): after the row moves of step s, the first
+  // strip of every system is updated, the panels of step s+1 run on `st`
+  // while the other strips update on the chain's side stream, and step s+1's
+  // row moves wait for both. Same operations per element, in the same order.
+  const bool la = c < (int)la_side.size() && la_side[c];
+  auto panels = [&](const Step& s) -> cudaError_t {
     for (const auto& pr : s.panels) {
       cudaError_t e = launch_panel(sa, d_step_list + pr.first, (int)pr.num, pr.mmax, s.k0, st);
       if (e != cudaSuccess) return e;
     }
-    cudaError_t e = launch_update(sa, d_items + s.item_first, (int)s.item_count, s.nmax, s.k0, st);
+    return cudaSuccess;
+  };
+  if (!ch.steps.empty()) {
+    cudaError_t e = panels(ch.steps[0]);
+    if (e != cudaSuccess) return e;
+  }
+  for (size_t k = 0; k < ch.steps.size(); ++k) {
+    const Step& s = ch.steps[k];
+    const StepItem* items = d_items + s.item_first;
+    cudaError_t e = launch_rows(sa, items, (int)s.item_count, s.k0, st);
+    if (e != cudaSuccess) return e;
+    const bool next = k + 1 < ch.steps.size();
+    if (!la || k == 0 || !next || s.nfirst == 0) {
+      e = launch_trailing(sa, items, (int)s.item_count, s.nmax, s.k0, 0, st);
+      if (e == cudaSuccess && next) e = panels(ch.steps[k + 1]);
+      if (e != cudaSuccess) return e;
+      continue;
+    }
+    e = launch_trailing(sa, items, (int)s.nfirst, s.nmax, s.k0, 1, st);
+    if (e == cudaSuccess) e = cudaEventRecord(la_first[c], st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(la_side[c], la_first[c], 0);
+    if (e == cudaSuccess)
+      e = launch_trailing(sa, items + s.nfirst, (int)(s.item_count - s.nfirst), s.nmax, s.k0, 0, la_side[c]);
+    if (e == cudaSuccess) e = cudaEventRecord(la_rest[c], la_side[c]);
+    if (e == cudaSuccess) e = panels(ch.steps[k + 1]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, la_rest[c], 0);
     if (e != cudaSuccess) return e;
   }
   return substitute(sa, ch, st, false);
+}
+
+cudaError_t Plan::ensure_lookahead() {
+  if (solve_only || !lookahead) return cudaSuccess;
+  while (la_side.size() < chains.size()) {
+    cudaStream_t s;
+    cudaEvent_t a, b;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    la_side.push_back(s);
+    if ((e = cudaEventCreateWithFlags(&a, cudaEventDisableTiming)) != cudaSuccess) return e;
+    la_first.push_back(a);
+    if ((e = cudaEventCreateWithFlags(&b, cudaEventDisableTiming)) != cudaSuccess) return e;
+    la_rest.push_back(b);
+  }
+  return cudaSuccess;
 }
 
 cudaError_t Plan::substitute(const StepArgs& sa, const Chain& ch, cudaStream_t st, bool forward) const {
@@ -433,6 +497,7 @@ int Plan::execute(const Ptrs& p, cudaStream_t st) {
   cudaGetDevice(&cur);
   if (cur != dev) return arg_error("plan used on a different device than it was created on");
   std::lock_guard<std::mutex> lk(mu);
+  NPPB_CUDA(ensure_lookahead(), "look-ahead streams");
   const int nwarp = (int)warp_classes.size();
   const int branches = nwarp + (int)chains.size();
   // executions share the plan's workspace: each one starts after the previous
@@ -505,7 +570,11 @@ int Plan::launches_per_execute() const {
       if (nw) l += windows(ch.nmax, 0, fwd);
     }
     if (solve_only) continue;
-    for (const Step& s : ch.steps) l += (int)s.panels.size() + 1 + (s.nmax - s.k0 - kStepNB > 0 ? 1 : 0);
+    for (size_t k = 0; k < ch.steps.size(); ++k) {
+      const Step& s = ch.steps[k];
+      l += (int)s.panels.size() + 1 + (s.nmax - s.k0 - kStepNB > 0 ? 1 : 0);
+      if (lookahead && k > 0 && k + 1 < ch.steps.size() && s.nfirst > 0) ++l;  // the look-ahead strip
+    }
   }
   return l;
 }
@@ -771,10 +840,13 @@ int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, doub
     std::unique_ptr<Plan> best;
     float best_ms = 0.f;
     int rc = NPPB_OK;
-    for (int c : {1, 2, 3, 4, 6}) {
+    static const int kChainCounts[5] = {1, 2, 3, 4, 6};
+    for (int cfg = 0; cfg < 10; ++cfg) {
+      const int c = kChainCounts[cfg / 2], la = cfg % 2;
       if (c > 1 && c > nstep) break;  // more chains than step-wise systems change nothing
       auto cand = std::make_unique<Plan>();
       cand->nchains = c;
+      cand->lookahead_mode = la;
       rc = cand->build(count, plan->n.data(), plan->nrhs.data(), plan->a_off.data(), plan->b_off.data(),
                        plan->inv_off.data(), plan->flags, false, true);
       if (rc != NPPB_OK) break;
@@ -800,7 +872,7 @@ int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, doub
     cudaStreamSynchronize(st);
     if (best) plan->pp = std::move(best);
     if (rc != NPPB_OK) return rc;
-    if (chains_out) *chains_out = plan->pp->nchains;
+    if (chains_out) *chains_out = plan->pp->nchains * (plan->pp->lookahead ? -1 : 1);
     if (ms_out) *ms_out = best_ms;
     return NPPB_OK;
   });

@@ -42,6 +42,7 @@ class Plan {
     int k0 = 0;
     std::vector<PanelRange> panels;
     int64_t item_first = 0, item_count = 0;
+    int64_t nfirst = 0;  // the first nfirst items: each system's first matrix strip (look-ahead)
     int nmax = 0;
   };
   // An independent sequence of steps over a subset of the step-wise systems;
@@ -88,6 +89,8 @@ class Plan {
   bool solve_only = false;
   bool use_graph = true;
   bool ext_factors = false;
+  bool lookahead = false;  // overlap the next panels with the current update (from step 1 on)
+  int lookahead_mode = -1;  // set before build: -1 automatic (orders above 512), 0 off, 1 on
   cudaStream_t alloc_stream = nullptr;  // stream-ordered allocations (freed on it too)
   int64_t a_elems = 0, b_elems = 0, inv_elems = 0, lu_elems = 0, piv_elems = 0;
   std::vector<WarpClass> warp_classes;
@@ -113,6 +116,7 @@ class Plan {
 
  private:
   void add_cost(const SysDesc& s, double& fl, double& by) const;
+  cudaError_t ensure_lookahead();  // a side stream and two events per chain
   // forward (getrs) or back substitution of one chain's strips
   cudaError_t substitute(const StepArgs& sa, const Chain& ch, cudaStream_t st, bool forward) const;
   Batch warp_batch(const Ptrs& p) const;
@@ -127,6 +131,8 @@ class Plan {
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
   cudaEvent_t done = nullptr;  // end of the last execution: the next one waits for it
+  std::vector<cudaStream_t> la_side;  // per chain: the look-ahead's other strips
+  std::vector<cudaEvent_t> la_first, la_rest;
 };
 
 // A cached plan for `count` systems of order n (uniform layout), for the

@@ -37,12 +37,13 @@ class Plan:
         _check(self.L.nppb_plan_execute(self.h, *args, st))
 
     def autotune(self, A, B, X, Inv, Det, Sign, Logabs, info, stream=None):
-        """Keep the fastest chain count for these device buffers; returns (chains, ms per execution)."""
+        """Keep the fastest chain count and look-ahead setting for these device
+        buffers; returns (chains, look-ahead on, ms per execution)."""
         st = stream if isinstance(stream, int) or stream is None else stream.cuda_stream
         ch, ms = C.c_int32(0), C.c_float(0.0)
         _check(self.L.nppb_plan_autotune(self.h, *(_lib.ptr(x) for x in (A, B, X, Inv, Det, Sign, Logabs, info)),
                                          st, C.byref(ch), C.byref(ms)))
-        return ch.value, ms.value
+        return abs(ch.value), ch.value < 0, ms.value
 
     def execute_host(self, A, B, X=None, Inv=None, Det=None, Sign=None, Logabs=None, info=None):
         """Host buffers (numpy); returns once the outputs are back."""

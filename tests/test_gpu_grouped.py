@@ -98,7 +98,7 @@ def test_plan_autotune_keeps_a_working_plan(lib, oracle):
     dInv = torch.zeros(max(plan.inv_elems, 1), dtype=torch.float64, device=dev)
     d = [torch.zeros(cnt, dtype=torch.float64, device=dev) for _ in range(3)]
     dinfo = torch.zeros(cnt, dtype=torch.int32, device=dev)
-    chains, ms = plan.autotune(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
+    chains, lookahead, ms = plan.autotune(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
     assert chains in (1, 2, 3, 4, 6) and ms > 0
     dX.zero_()
     plan.execute(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
