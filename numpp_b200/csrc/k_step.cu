@@ -1455,8 +1455,10 @@ __device__ __forceinline__ void window_solve(const T* __restrict__ M, int n, T* 
 }
 
 // k_back: X = U^-1 Y on a strip, the window of this pass.
+// four CTAs per SM: the substitution is a latency chain per strip, and the
+// uneven batches launch thousands of strips
 template <class T>
-__global__ void __launch_bounds__(UT)
+__global__ void __launch_bounds__(UT, 4)
 k_back(StepArgsT<T> sa, const StepItem* __restrict__ items, int pass) {
   const StepItem it = items ? items[blockIdx.x] : uniform_item(sa, blockIdx.x, 0, true);
   const SysDesc d = step_desc(sa, it.sys);
