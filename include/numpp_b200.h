@@ -76,6 +76,20 @@ int nppb_gemm(int dtype, int64_t m, int64_t n, int64_t k, const void* A, const v
 int nppb_d_gemm(int dtype, int64_t m, int64_t n, int64_t k, const void* dA, const void* dB,
                 void* dC, void* stream);
 
+/* Stacked matmul: `batch` contiguous row-major FP64 products C[z] = A[z] B[z]
+ * (m x k times k x n) on the DMMA GEMM, one launch for the whole stack. The
+ * reference's matmul is 2-D only (src/backend/backend.cpp:121-177 rejects
+ * ndim > 2); this is the einsum 'bij,bjk->bik' its callers fall back to. */
+int nppb_d_gemm_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const double* dA, const double* dB,
+                        double* dC, void* stream);
+int nppb_gemm_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const double* A, const double* B,
+                      double* C);
+/* matrix_power over a (count, n, n) FP64 stack (src/linalg/batched.cpp:83-84
+ * mapping src/linalg/linalg.cpp:443-455): binary exponentiation with the
+ * batched GEMM, the batched inverse first when p < 0 (info[i] != 0: system i
+ * is singular, its R is then undefined), the identity for p = 0. */
+int nppb_matrix_power_batched(int64_t count, int32_t n, int64_t p, const double* A, double* R, int32_t* info);
+
 /* ---- uniform batches: count systems of order n (host buffers) ----------- */
 /* getrf: LU with partial pivoting in place (src/linalg/linalg.cpp:48-71),
  * A (count,n,n) overwritten by the unit-lower L and U in pivoted row order. */

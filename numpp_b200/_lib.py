@@ -61,6 +61,9 @@ SIGNATURES = {
     "nppb_plan_autotune": (_int, [_vp] * 10 + [C.POINTER(_i32), C.POINTER(C.c_float)]),
     "nppb_plan_time_kernels": (_int, [_vp] * 10 + [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_solve_grouped": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _int] + [_vp] * 8),
+    "nppb_d_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
+    "nppb_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp]),
+    "nppb_matrix_power_batched": (_int, [_i64, _i32, _i64, _vp, _vp, _vp]),
     "nppb_server_create": (_int, [C.POINTER(_vp), _i64, C.c_double, _i32]),
     "nppb_server_submit": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, C.POINTER(_i64), C.POINTER(_i64)]),
     "nppb_server_wait": (_int, [_vp, _i64, C.c_double, C.POINTER(_i32), C.POINTER(C.c_double)]),

@@ -6,6 +6,8 @@
 // register round trip), so the next slab lands while the tensor pipe works on
 // the current one.
 // FP32: SIMT 64x64 tile, 4x4 outputs per thread (the float32 form of the slot).
+#include <algorithm>
+
 #include "dmma.cuh"
 #include "nppb_internal.hpp"
 
@@ -26,11 +28,19 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+// blockIdx.z walks a strided batch (sA, sB, sC elements apart; 0 for one GEMM)
 __global__ void __launch_bounds__(NT)
 k_gemm_f64(int64_t M, int64_t N, int64_t K, const double* __restrict__ A, int64_t lda,
-           const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc) {
+           const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc, int64_t sA,
+           int64_t sB, int64_t sC, int64_t z0) {
   __shared__ double As[2][BM * AS];
   __shared__ double Bs[2][BK * BS];
+  {
+    const int64_t z = z0 + blockIdx.z;
+    A += z * sA;
+    B += z * sB;
+    C += z * sC;
+  }
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, tq = lane & 3;
   const int64_t bm = (int64_t)blockIdx.y * BM, bn = (int64_t)blockIdx.x * BN;
@@ -152,8 +162,21 @@ cudaError_t launch_gemm_f64(int64_t m, int64_t n, int64_t k, const double* A, in
                             cudaStream_t st) {
   if (m <= 0 || n <= 0) return cudaSuccess;
   dim3 grid((unsigned)((n + BN - 1) / BN), (unsigned)((m + BM - 1) / BM));
-  k_gemm_f64<<<grid, NT, 0, st>>>(m, n, k, A, lda, B, ldb, C, ldc);
+  k_gemm_f64<<<grid, NT, 0, st>>>(m, n, k, A, lda, B, ldb, C, ldc, 0, 0, 0, 0);
   return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_f64_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const double* A,
+                                    const double* B, double* C, cudaStream_t st) {
+  if (m <= 0 || n <= 0 || batch <= 0) return cudaSuccess;
+  const unsigned gx = (unsigned)((n + BN - 1) / BN), gy = (unsigned)((m + BM - 1) / BM);
+  for (int64_t z0 = 0; z0 < batch; z0 += 65535) {
+    const dim3 grid(gx, gy, (unsigned)std::min<int64_t>(65535, batch - z0));
+    k_gemm_f64<<<grid, NT, 0, st>>>(m, n, k, A, k, B, n, C, n, m * k, k * n, m * n, z0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_gemm_f32(int64_t m, int64_t n, int64_t k, const float* A, const float* B,

@@ -101,6 +101,9 @@ cudaError_t launch_gemm_f64(int64_t m, int64_t n, int64_t k, const double* A, in
                             const double* B, int64_t ldb, double* C, int64_t ldc,
                             cudaStream_t st);
 
+// `batch` contiguous row-major FP64 GEMMs: C[z] = A[z] B[z] (m x k, k x n, m x n).
+cudaError_t launch_gemm_f64_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const double* A,
+                                    const double* B, double* C, cudaStream_t st);
 // Row-major FP32 GEMM (SIMT), used for the gemm slot's float32 form.
 cudaError_t launch_gemm_f32(int64_t m, int64_t n, int64_t k, const float* A, const float* B,
                             float* C, cudaStream_t st);

@@ -9,6 +9,16 @@ on numpy arrays:
   (NumPP keeps NumPy 1.x's rule), else a stack of (n, k) matrices.
 * ``inv(a)``, ``det(a)``, ``slogdet(a)`` -- linalg.cpp:386-439, batched.cpp:75-108.
 * ``matmul(a, b)`` -- backend.cpp:121-177 with the GPU forced (2-D only).
+* ``matmul_batched(a, b)`` -- equal-batch (..., m, k) @ (..., k, n) on the
+  batched DMMA GEMM. The reference has no stacked matmul (backend.cpp:122
+  rejects ndim != 2); this is the product its stacked ``matrix_power`` runs per
+  matrix, offered as one call. Leading axes broadcast as in numpy.matmul.
+* ``matrix_power(a, n)`` -- linalg.cpp:443-455, stacks batched.cpp:83-84.
+* ``tensorsolve(a, b, axes)``, ``tensorinv(a, ind)`` -- tensor_solve.cpp:10-49.
+* ``cond(a, p)`` -- tensor.cpp:359-393 for p in {1, -1, inf, -inf, "fro"}:
+  norm(a, p) * norm(inv(a), p), inf when a is singular. The 2-norm forms
+  (p None, 2, -2) need singular values, which this path does not compute:
+  they raise ``Declined``.
 
 dtype policy (``la_kind``, linalg.cpp:20-26): the computation is float64;
 float32 results come back as float32, every other real dtype as float64.
@@ -98,6 +108,21 @@ class NativeBackend:
         dt = _lib.DT_FLOAT64 if A.dtype == np.float64 else _lib.DT_FLOAT32
         _check(self.L.nppb_gemm(dt, m, n, k, _lib.ptr(A), _lib.ptr(B), _lib.ptr(Cm)))
         return Cm
+
+
+    def gemm_batched(self, A, B):
+        cnt, m, k = A.shape
+        n = B.shape[-1]
+        Cm = np.empty((cnt, m, n))
+        _check(self.L.nppb_gemm_batched(cnt, m, n, k, _lib.ptr(A), _lib.ptr(B), _lib.ptr(Cm)))
+        return Cm
+
+    def matrix_power(self, A, p):
+        cnt, n = A.shape[0], A.shape[-1]
+        R = np.empty_like(A)
+        info = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_matrix_power_batched(cnt, n, p, _lib.ptr(A), _lib.ptr(R), _lib.ptr(info)))
+        return R, info
 
 
 _default = None
@@ -233,3 +258,133 @@ def matmul(a, b, backend=None):
     if a.shape[0] == 0 or b.shape[1] == 0:
         return np.zeros((a.shape[0], b.shape[1]), dt)
     return be.gemm(np.ascontiguousarray(a, dt), np.ascontiguousarray(b, dt))
+
+
+def matmul_batched(a, b, backend=None):
+    """Stacked float64 product (..., m, k) @ (..., k, n); leading axes broadcast.
+
+    2-D operands are numpp::matmul itself (backend.cpp:121-177). Float32 and
+    every other real dtype compute in float64 and return float64 (float32 stays
+    float32), like the linalg front-end's dtype policy."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.ndim < 2 or b.ndim < 2:
+        raise ValueError("matmul requires at least 2-D arrays")
+    if a.shape[-1] != b.shape[-2]:
+        raise ValueError("matmul: shape mismatch")
+    out = _la_out(np.result_type(a.dtype, b.dtype))
+    lead = np.broadcast_shapes(a.shape[:-2], b.shape[:-2])
+    m, k, n = a.shape[-2], a.shape[-1], b.shape[-1]
+    cnt = int(np.prod(lead)) if lead else 1
+    if cnt == 0 or m == 0 or n == 0:
+        return np.zeros(lead + (m, n), out)
+    A3 = np.ascontiguousarray(np.broadcast_to(a, lead + (m, k)), np.float64).reshape(cnt, m, k)
+    B3 = np.ascontiguousarray(np.broadcast_to(b, lead + (k, n)), np.float64).reshape(cnt, k, n)
+    return be.gemm_batched(A3, B3).reshape(lead + (m, n)).astype(out, copy=False)
+
+
+def matrix_power(a, n, backend=None):
+    """numpp::linalg::matrix_power (linalg.cpp:443-455; stacks batched.cpp:83-84).
+
+    n = 0 gives the identity, n < 0 inverts first (``LinAlgError("Singular
+    matrix")`` when a matrix of the stack is singular), then binary
+    exponentiation: the same sequence of products as the reference."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    out = _la_out(a.dtype)
+    if a.ndim < 2:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+    n = int(n)
+    if not -(1 << 63) <= n < (1 << 63):
+        raise OverflowError("matrix_power exponent out of int64 range")
+    lead, cnt, d, A3 = _stack(a)
+    if cnt == 0 or d == 0:
+        return np.zeros(a.shape, out)
+    R, info = be.matrix_power(A3, n)
+    if n < 0 and info.any():
+        raise LinAlgError("Singular matrix")
+    return R.reshape(a.shape).astype(out, copy=False)
+
+
+def tensorsolve(a, b, axes=None, backend=None):
+    """numpy/NumPP tensorsolve (tensor_solve.cpp:10-34): the named axes of a move
+    to the end, the trailing a.ndim - b.ndim axes form the unknown's shape, and
+    the square reshape of a is solved against b.ravel()."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    an = a.ndim
+    if axes:
+        allaxes = list(range(an))
+        for k in axes:
+            if k not in allaxes:
+                raise ValueError(f"tensorsolve: axis {k} is not an axis of a")
+            allaxes.remove(k)
+            allaxes.append(k)
+        a = a.transpose(allaxes)
+    bn = b.ndim
+    if an < bn:
+        raise LinAlgError("tensorsolve: a.ndim must be >= b.ndim")
+    oldshape = a.shape[bn:]
+    prod = int(np.prod(oldshape)) if oldshape else 1
+    if a.size != prod * prod:
+        raise LinAlgError("tensorsolve: prod(a.shape[b.ndim:]) must equal prod(a.shape[:b.ndim])")
+    if b.size != prod:
+        raise ValueError("tensorsolve: b does not reshape to the unknown's size")
+    x = solve(a.reshape(prod, prod), b.reshape(prod), backend=backend)
+    return x.reshape(oldshape)
+
+
+def tensorinv(a, ind=2, backend=None):
+    """numpy/NumPP tensorinv (tensor_solve.cpp:36-49): inv of a reshaped to
+    (prod(a.shape[ind:]), prod(a.shape[:ind])), result shape a.shape[ind:] + a.shape[:ind]."""
+    a = np.asarray(a)
+    nd = a.ndim
+    ind = int(ind)
+    if ind <= 0 or ind > nd:
+        raise ValueError("Invalid ind argument")
+    sh = a.shape
+    prod = int(np.prod(sh[ind:])) if sh[ind:] else 1
+    lead = int(np.prod(sh[:ind]))
+    return inv(a.reshape(prod, lead), backend=backend).reshape(sh[ind:] + sh[:ind])
+
+
+def _matrix_norm(x, p):
+    ax = np.abs(x)
+    if p == "fro":
+        return np.sqrt((x * x).sum(axis=(-2, -1)))
+    if p in (1, -1):
+        col = ax.sum(axis=-2)
+        return col.max(axis=-1) if p == 1 else col.min(axis=-1)
+    row = ax.sum(axis=-1)
+    return row.max(axis=-1) if p == np.inf else row.min(axis=-1)
+
+
+def cond(a, p=None, backend=None):
+    """numpp::cond (src/tensor/tensor.cpp:359-393) for the inverse-based norms.
+
+    p in {1, -1, inf, -inf, "fro"}: norm(a, p) * norm(inv(a), p) in float64,
+    inf for a singular matrix (the reference catches linalg_error). A stack
+    (..., n, n) gives one number per matrix. p None / 2 / -2 rest on singular
+    values, outside this path: ``Declined``."""
+    if p is None or (not isinstance(p, str) and p in (2, -2)):
+        raise Declined("cond with the 2-norm needs singular values, which the B200 path does not compute")
+    if isinstance(p, str):
+        if p != "fro":
+            raise ValueError(f"cond: unsupported norm {p!r}")
+    elif p not in (1, -1, np.inf, -np.inf):
+        raise ValueError(f"cond: unsupported norm {p!r}")
+    be = backend or default_backend()
+    a = np.asarray(a)
+    _la_out(a.dtype)
+    if a.ndim < 2:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+    lead, cnt, n, A3 = _stack(a)
+    if n == 0:
+        raise LinAlgError("cond is not defined on empty arrays")
+    if cnt == 0:
+        return np.zeros(lead)
+    Ai, info = be.inv(A3)
+    c = _matrix_norm(A3, p) * _matrix_norm(Ai, p)
+    c = np.where(info != 0, np.inf, c)
+    return c.reshape(lead) if lead else np.float64(c[0])

@@ -106,6 +106,33 @@ class Oracle:
         self.L.oracle_matmul(m, n, k, _ptr(A), _ptr(B), _ptr(Cm))
         return Cm
 
+    def matrix_power(self, A, p):
+        """(count, n, n) stack to the integer power p, restating src/linalg/linalg.cpp:443-455
+        per matrix (batched.cpp:83-84): the identity for p = 0, the inverse first for p < 0,
+        then binary exponentiation with the p-order matmul. ok[i] = 0 when p < 0 and
+        matrix i is singular (the reference raises linalg_error there)."""
+        A = np.ascontiguousarray(A, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        R = np.zeros_like(A)
+        ok = np.ones(cnt, np.intc)
+        for i in range(cnt):
+            if p < 0:
+                base, o = self.inv(A[i:i + 1])
+                base = base[0]
+                ok[i] = o[0]
+            else:
+                base = A[i].copy()
+            e = -p if p < 0 else p
+            res = np.eye(n)
+            while e > 0:
+                if e & 1:
+                    res = self.matmul(res, base)
+                e >>= 1
+                if e:
+                    base = self.matmul(base, base)
+            R[i] = res
+        return R, ok
+
     def solve_grouped(self, sys, want_slogdet=True, want_inv=True):
         """sys: a packed uneven batch (numpp_b200 grouped layout as a dict of arrays)."""
         cnt = len(sys["n"])
@@ -142,6 +169,11 @@ class RefLib:
         L.ref_det.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_slogdet.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_matmul_cpu.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int, vp, vp, vp, cp, C.c_int]
+        L.ref_matrix_power.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int64, vp, _ip, _i64p, cp,
+                                       C.c_int]
+        L.ref_tensorsolve.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int, _i64p, C.c_int, vp, C.c_int,
+                                      _i64p, vp, _ip, _i64p, cp, C.c_int]
+        L.ref_tensorinv.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int64, vp, _ip, _i64p, cp, C.c_int]
         L.ref_solve_grouped.argtypes = [C.c_int64, _i32p, _i32p, _i64p, _i64p, _i64p, _dp, _dp,
                                         _dp, _dp, _dp, _dp, _i32p, C.c_int]
         L.ref_standard_normal2.argtypes = [C.c_uint64, C.c_int64, _dp, C.c_int64, _dp]
@@ -218,6 +250,42 @@ class RefLib:
         self._call(self.L.ref_matmul_cpu, A.shape[0], B.shape[1], A.shape[1], F64, A.ctypes.data,
                    B.ctypes.data, Cm.ctypes.data)
         return Cm
+
+    def matrix_power(self, A, p):
+        A = np.ascontiguousarray(A)
+        sa = np.array(A.shape, np.int64)
+        out = np.zeros(max(A.size, 1), np.float64)
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(self.L.ref_matrix_power, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data, p,
+                   out.ctypes.data, C.byref(dt), C.byref(sz))
+        return np.frombuffer(out.tobytes(), self._np(dt.value), sz.value).reshape(A.shape)
+
+    def tensorsolve(self, A, B, axes=()):
+        """out shape: the unknown's shape, a.shape[b.ndim:] after the axes move."""
+        A = np.ascontiguousarray(A)
+        B = np.ascontiguousarray(B)
+        sa = np.array(A.shape, np.int64)
+        sb = np.array(B.shape, np.int64)
+        ax = np.array(list(axes) or [0], np.int64)
+        out = np.zeros(max(A.size, 1), np.float64)
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(self.L.ref_tensorsolve, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data, B.ndim,
+                   _ptr(sb, _i64p), self._dt(B), B.ctypes.data, len(axes), _ptr(ax, _i64p),
+                   out.ctypes.data, C.byref(dt), C.byref(sz))
+        return np.frombuffer(out.tobytes(), self._np(dt.value), sz.value)
+
+    def tensorinv(self, A, ind=2):
+        """Flat result; its shape is a.shape[ind:] + a.shape[:ind]."""
+        A = np.ascontiguousarray(A)
+        sa = np.array(A.shape, np.int64)
+        out = np.zeros(max(A.size, 1), np.float64)
+        dt = C.c_int()
+        sz = C.c_int64()
+        self._call(self.L.ref_tensorinv, A.ndim, _ptr(sa, _i64p), self._dt(A), A.ctypes.data, ind,
+                   out.ctypes.data, C.byref(dt), C.byref(sz))
+        return np.frombuffer(out.tobytes(), self._np(dt.value), sz.value)
 
     def standard_normal2(self, seed, n1, n2):
         a = np.zeros(n1)

@@ -1,7 +1,8 @@
 // REFERENCE SHIM — TEST INFRASTRUCTURE ONLY.
 //
 // extern "C" wrappers around the reference library's own public API
-// (numpp::linalg::solve/inv/det/slogdet and numpp::matmul), compiled together
+// (numpp::linalg::solve/inv/det/slogdet/matrix_power/tensorsolve/tensorinv
+// and numpp::matmul), compiled together
 // with the reference's unmodified CPU sources into oracle/_ref/libnumpp_ref.so
 // by oracle/Makefile. Tests use it to pin the C oracle and to make golden
 // fixtures; bench.py's reference arm times it. The product never loads it.
@@ -84,6 +85,29 @@ int ref_slogdet(int nda, const int64_t* sa, int dta, const void* A, void* sign, 
     put(r.sign, sign, o_dt, o_size);
     put(r.logabsdet, logabs, nullptr, nullptr);
   });
+}
+
+// matrix_power (src/linalg/linalg.cpp:443-455; stacks batched.cpp:83-84).
+int ref_matrix_power(int nda, const int64_t* sa, int dta, const void* A, int64_t p, void* out,
+                     int* o_dt, int64_t* o_size, char* err, int errlen) {
+  return guard(err, errlen, [&] {
+    put(numpp::linalg::matrix_power(make(nda, sa, dta, A), p), out, o_dt, o_size);
+  });
+}
+
+// tensorsolve / tensorinv (src/linalg/tensor_solve.cpp:10-49). naxes = 0: no axes.
+int ref_tensorsolve(int nda, const int64_t* sa, int dta, const void* A, int ndb, const int64_t* sb,
+                    int dtb, const void* B, int naxes, const int64_t* axes, void* X, int* x_dt,
+                    int64_t* x_size, char* err, int errlen) {
+  return guard(err, errlen, [&] {
+    std::vector<int64_t> ax(axes, axes + naxes);
+    put(numpp::linalg::tensorsolve(make(nda, sa, dta, A), make(ndb, sb, dtb, B), ax), X, x_dt, x_size);
+  });
+}
+
+int ref_tensorinv(int nda, const int64_t* sa, int dta, const void* A, int64_t ind, void* out, int* o_dt,
+                  int64_t* o_size, char* err, int errlen) {
+  return guard(err, errlen, [&] { put(numpp::linalg::tensorinv(make(nda, sa, dta, A), ind), out, o_dt, o_size); });
 }
 
 int ref_matmul_cpu(int64_t m, int64_t n, int64_t k, int dt, const void* A, const void* B, void* C,

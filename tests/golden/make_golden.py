@@ -12,6 +12,9 @@ NumPP's tests and on small seeded workloads, and stores inputs + outputs:
 * tests/test_gpu.cpp:56-69                        the 40x50 @ 50x30 GEMM
 * seeded uniform batch (16 x 32x32 + 32 I) and a seeded uneven batch (n in 1..80)
 * numpp::random::default_rng draws (PCG64 + ziggurat) for seeds 12345 / 7
+* tests/test_linalg_mined3.cpp:29-40             matrix_power of [[1,2],[3,4]] for 0, 1, 2, 7, -1, -3
+* tests/test_tensor_solve.cpp:9-71                tensorsolve / tensorinv of the (2,2,2,2) tridiagonal
+* a seeded (6, 9, 9) stack to the powers 3, 8, -2, -4 (src/linalg/batched.cpp:83-84)
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref; run where it was built)
 """
@@ -102,6 +105,34 @@ def main():
         g["uneven_" + k] = sysu[k]
     g["uneven_inv_size"] = np.array(sysu["inv_size"])
     g["uneven_x"], g["uneven_sign"], g["uneven_logabs"], g["uneven_inv"], g["uneven_ok"] = X, s, la, inv, ok
+
+    P = np.array([[1.0, 2], [3, 4]])
+    g["mp2_A"] = P
+    for p in (0, 1, 2, 7, -1, -3):
+        g[f"mp2_p{p}"] = r.matrix_power(P, p)
+    g["mp2_f32_p0"] = r.matrix_power(P.astype(np.float32), 0)
+    g["mp_sing_err"] = np.array(err_of(r.matrix_power, Sg, -1))
+    rng = np.random.default_rng(2024)
+    Ms = rng.standard_normal((6, 9, 9)) / 3.0 + 0.5 * np.eye(9)
+    g["mp9_A"] = Ms
+    for p in (3, 8, -2, -4):
+        g[f"mp9_p{p}"] = r.matrix_power(Ms, p)
+
+    T = np.array([4.0, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4]).reshape(2, 2, 2, 2)
+    bt = np.array([1.0, 2, 3, 4]).reshape(2, 2)
+    g["tens_A"], g["tens_b"] = T, bt
+    g["tens_x"] = r.tensorsolve(T, bt).reshape(2, 2)
+    g["tens_x_ax0"] = r.tensorsolve(T, bt, (0,)).reshape(2, 2)
+    g["tens_inv"] = r.tensorinv(T, 2).reshape(2, 2, 2, 2)
+    T3 = rng.standard_normal((3, 4, 12))
+    b3r = rng.standard_normal((3, 4))
+    g["tens3_A"], g["tens3_b"] = T3, b3r
+    g["tens3_x"] = r.tensorsolve(T3, b3r).reshape(12)
+    T4 = rng.standard_normal((4, 6, 8, 3))
+    g["tens4_A"] = T4
+    g["tens4_inv"] = r.tensorinv(T4, 2).reshape(8, 3, 4, 6)
+    g["tensinv_ind0_err"] = np.array(err_of(r.tensorinv, T, 0))
+    g["tenssolve_shape_err"] = np.array(err_of(r.tensorsolve, rng.standard_normal((2, 3, 5)), b3r[:2, :3]))
 
     for seed in (12345, 7):
         a, b = r.standard_normal2(seed, 64, 16)

@@ -35,6 +35,15 @@ class OracleBackend:
         self.calls.append(("gemm", A.shape, B.shape))
         return self.o.matmul(A, B).astype(A.dtype)
 
+    def gemm_batched(self, A, B):
+        self.calls.append(("gemm_batched", A.shape, B.shape))
+        return np.stack([self.o.matmul(A[i], B[i]) for i in range(A.shape[0])])
+
+    def matrix_power(self, A, p):
+        self.calls.append(("matrix_power", A.shape, p))
+        R, ok = self.o.matrix_power(A, p)
+        return R, (ok == 0).astype(np.int32)
+
 
 @pytest.fixture()
 def be(oracle):
@@ -132,3 +141,77 @@ def test_stack_is_passed_as_one_batch(be):
     A = np.stack([np.eye(4) * (i + 1) for i in range(6)]).reshape(2, 3, 4, 4)
     la.det(A, backend=be)
     assert be.calls[-1] == ("det", (6, 4, 4))
+
+
+def test_matrix_power(golden, be):
+    """linalg.cpp:443-455 through the mirror: same values, dtype and errors as the reference."""
+    for p in (0, 1, 2, 7, -1, -3):
+        R = la.matrix_power(golden["mp2_A"], p, backend=be)
+        assert R.shape == (2, 2) and np.array_equal(R, golden[f"mp2_p{p}"]), p
+    R = la.matrix_power(golden["mp2_A"].astype(np.float32), 0, backend=be)
+    assert R.dtype == golden["mp2_f32_p0"].dtype and np.array_equal(R, golden["mp2_f32_p0"])
+    for p in (3, 8, -2, -4):
+        assert np.array_equal(la.matrix_power(golden["mp9_A"], p, backend=be), golden[f"mp9_p{p}"])
+    with pytest.raises(la.LinAlgError, match=str(golden["mp_sing_err"])):
+        la.matrix_power(golden["sing_A"], -1, backend=be)
+    with pytest.raises(la.LinAlgError, match="square"):
+        la.matrix_power(np.zeros((2, 3)), 2, backend=be)
+    assert la.matrix_power(np.zeros((0, 4, 4)), 3, backend=be).shape == (0, 4, 4)
+    # one batched call for the whole stack (batched.cpp:83-84 maps one matrix at a time)
+    be.calls.clear()
+    la.matrix_power(np.ones((2, 3, 5, 5)), 2, backend=be)
+    assert be.calls == [("matrix_power", (6, 5, 5), 2)]
+
+
+def test_tensorsolve_tensorinv(golden, be):
+    """tensor_solve.cpp:10-49 semantics against the reference's own outputs."""
+    T, b = golden["tens_A"], golden["tens_b"]
+    x = la.tensorsolve(T, b, backend=be)
+    assert x.shape == (2, 2) and np.array_equal(x, golden["tens_x"])
+    assert np.array_equal(la.tensorsolve(T, b, axes=(0,), backend=be), golden["tens_x_ax0"])
+    ti = la.tensorinv(T, 2, backend=be)
+    assert ti.shape == (2, 2, 2, 2) and np.array_equal(ti, golden["tens_inv"])
+    x3 = la.tensorsolve(golden["tens3_A"], golden["tens3_b"], backend=be)
+    assert x3.shape == (12,) and np.array_equal(x3, golden["tens3_x"])
+    t4 = la.tensorinv(golden["tens4_A"], 2, backend=be)
+    assert t4.shape == (8, 3, 4, 6) and np.array_equal(t4, golden["tens4_inv"])
+    np.testing.assert_allclose(x3, np.linalg.tensorsolve(golden["tens3_A"], golden["tens3_b"]), rtol=1e-10)
+    with pytest.raises(ValueError, match=str(golden["tensinv_ind0_err"])):
+        la.tensorinv(T, 0, backend=be)
+    with pytest.raises(ValueError, match="Invalid ind"):
+        la.tensorinv(T, 5, backend=be)
+    with pytest.raises(la.LinAlgError, match="must equal"):
+        la.tensorsolve(np.ones((2, 3, 5)), np.ones((2, 3)), backend=be)
+
+
+def test_matmul_batched(golden, be):
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((2, 3, 4, 5))
+    B = rng.standard_normal((3, 5, 6))          # broadcasts over the leading 2
+    Cm = la.matmul_batched(A, B, backend=be)
+    assert Cm.shape == (2, 3, 4, 6)
+    np.testing.assert_allclose(Cm, A @ B, rtol=1e-13, atol=1e-13)
+    assert be.calls[-1] == ("gemm_batched", (6, 4, 5), (6, 5, 6))
+    assert la.matmul_batched(A.astype(np.float32), B.astype(np.float32), backend=be).dtype == np.float32
+    assert la.matmul_batched(np.zeros((0, 2, 3)), np.zeros((0, 3, 4)), backend=be).shape == (0, 2, 4)
+    with pytest.raises(ValueError, match="shape mismatch"):
+        la.matmul_batched(A, A, backend=be)
+    with pytest.raises(la.Declined):
+        la.matmul_batched(A.astype(np.complex128), B, backend=be)
+
+
+def test_cond(be):
+    rng = np.random.default_rng(6)
+    A = rng.standard_normal((3, 7, 7)) + 3 * np.eye(7)
+    for p in (1, -1, np.inf, -np.inf, "fro"):
+        c = la.cond(A, p, backend=be)
+        np.testing.assert_allclose(c, np.linalg.cond(A, p), rtol=1e-12)
+        assert isinstance(la.cond(A[0], p, backend=be), np.floating)
+    S = np.stack([A[0], np.zeros((7, 7))])
+    c = la.cond(S, 1, backend=be)
+    assert np.isfinite(c[0]) and c[1] == np.inf   # singular -> inf (tensor.cpp:361-368)
+    for p in (None, 2, -2):
+        with pytest.raises(la.Declined):
+            la.cond(A, p, backend=be)
+    with pytest.raises(ValueError):
+        la.cond(A, "nuc", backend=be)

@@ -33,7 +33,9 @@ def check_vs_oracle(sys, X, Inv, Det, Sign, Logabs, info, oracle):
             o = sys["inv_off"][i]
             d = Inv[o:o + n * n] - invo[o:o + n * n]
             assert np.linalg.norm(d) <= 1e-12 * cond * max(np.linalg.norm(invo[o:o + n * n]), 1e-300)
-    np.testing.assert_allclose(Det, Sign * np.exp(Logabs), rtol=1e-9)
+    fin = Logabs < 700.0   # det overflows to +-inf past e^709; compare where it is finite
+    np.testing.assert_allclose(Det[fin], (Sign * np.exp(Logabs))[fin], rtol=1e-9)
+    assert np.all(np.isinf(Det[~fin]) | (np.abs(Det[~fin]) > 1e300))
 
 
 def test_one_shot_uneven(lib, oracle):

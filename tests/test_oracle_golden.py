@@ -117,3 +117,37 @@ def test_oracle_vs_numpy_tolerance(oracle):
     x, _ = oracle.solve(A, B)
     np.testing.assert_allclose(x, np.linalg.solve(A, B), rtol=1e-12, atol=1e-12)
     np.testing.assert_allclose(oracle.det(A), np.linalg.det(A), rtol=1e-12)
+
+
+def test_matrix_power_known_answers(golden, oracle):
+    """test_linalg_mined3.cpp:29-40 and a seeded stack: the restatement of
+    linalg.cpp:443-455 reproduces the reference bit for bit."""
+    P = golden["mp2_A"][None]
+    for p in (0, 1, 2, 7, -1, -3):
+        R, ok = oracle.matrix_power(P, p)
+        assert ok.all() and bits_equal(R[0], golden[f"mp2_p{p}"]), p
+    np.testing.assert_allclose(golden["mp2_p-3"], np.linalg.matrix_power(golden["mp2_A"], -3), rtol=1e-12)
+    for p in (3, 8, -2, -4):
+        R, ok = oracle.matrix_power(golden["mp9_A"], p)
+        assert ok.all() and bits_equal(R, golden[f"mp9_p{p}"]), p
+    _, ok = oracle.matrix_power(golden["sing_A"][None], -1)
+    assert ok[0] == 0 and str(golden["mp_sing_err"]) == "Singular matrix"
+    assert golden["mp2_f32_p0"].dtype == np.float32
+
+
+def test_tensor_solve_known_answers(golden, oracle):
+    """tensor_solve.cpp:10-49 is a reshape around solve / inv: the oracle's solve
+    and inv on the reshaped matrices give the reference's tensorsolve / tensorinv."""
+    T, b = golden["tens_A"], golden["tens_b"]
+    x, ok = oracle.solve(T.reshape(1, 4, 4), b.reshape(1, 4, 1))
+    assert ok.all() and bits_equal(x.reshape(2, 2), golden["tens_x"])
+    Tm = np.ascontiguousarray(np.transpose(T, (1, 2, 3, 0))).reshape(1, 4, 4)
+    x, _ = oracle.solve(Tm, b.reshape(1, 4, 1))
+    assert bits_equal(x.reshape(2, 2), golden["tens_x_ax0"])
+    inv, _ = oracle.inv(T.reshape(1, 4, 4))
+    assert bits_equal(inv.reshape(2, 2, 2, 2), golden["tens_inv"])
+    x, _ = oracle.solve(golden["tens3_A"].reshape(1, 12, 12), golden["tens3_b"].reshape(1, 12, 1))
+    assert bits_equal(x.reshape(12), golden["tens3_x"])
+    inv, _ = oracle.inv(golden["tens4_A"].reshape(1, 24, 24))
+    assert bits_equal(inv.reshape(8, 3, 4, 6), golden["tens4_inv"])
+    assert str(golden["tensinv_ind0_err"]) == "Invalid ind argument"
