@@ -85,7 +85,7 @@ int nppb_d_gemm_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const do
 int nppb_gemm_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const double* A, const double* B,
                       double* C);
 /* matrix_power over a (count, n, n) FP64 stack (src/linalg/batched.cpp:83-84
- * mapping src/linalg/linalg.cpp:443-455): binary exponentiation with the
+ * mapping src/linalg/linalg.cpp:440-454): binary exponentiation with the
  * batched GEMM, the batched inverse first when p < 0 (info[i] != 0: system i
  * is singular, its R is then undefined), the identity for p = 0. */
 int nppb_matrix_power_batched(int64_t count, int32_t n, int64_t p, const double* A, double* R, int32_t* info);

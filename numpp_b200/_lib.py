@@ -1,4 +1,5 @@
-"""ctypes binding of libnumpp_b200.so (the C ABI declared in include/numpp_b200.h).
+"""ctypes binding of libnumpp_b200.so (the C ABI declared in include/numpp_b200.h
+and include/numpp_b200_dlpack.h).
 
 Loading fails loudly: there is no CPU fallback anywhere in this package.
 """
@@ -22,7 +23,7 @@ _i32 = C.c_int32
 _i64 = C.c_int64
 _int = C.c_int
 
-# name -> (restype, argtypes); every symbol include/numpp_b200.h declares.
+# name -> (restype, argtypes); every symbol include/numpp_b200*.h declare.
 SIGNATURES = {
     "nppb_abi_version": (_int, []),
     "nppb_device_available": (_int, []),
@@ -64,6 +65,8 @@ SIGNATURES = {
     "nppb_d_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
     "nppb_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp]),
     "nppb_matrix_power_batched": (_int, [_i64, _i32, _i64, _vp, _vp, _vp]),
+    "nppb_dl_linalg": (_int, [_int] + [_vp] * 9),
+    "nppb_dl_matmul": (_int, [_vp] * 4),
     "nppb_server_create": (_int, [C.POINTER(_vp), _i64, C.c_double, _i32]),
     "nppb_server_submit": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, C.POINTER(_i64), C.POINTER(_i64)]),
     "nppb_server_wait": (_int, [_vp, _i64, C.c_double, C.POINTER(_i32), C.POINTER(C.c_double)]),

@@ -2,7 +2,7 @@
 //
 // The reference's matmul is 2-D only (src/backend/backend.cpp:121-177 rejects
 // ndim > 2) and its stacked matrix_power maps the 2-D routine over the stack
-// (src/linalg/batched.cpp:83-84 -> linalg.cpp:443-455: binary exponentiation
+// (src/linalg/batched.cpp:83-84 -> linalg.cpp:440-454: binary exponentiation
 // with matmul, inv first for negative powers). Here both run on the device
 // over a whole stack at once: the batched DMMA GEMM (one launch per product
 // for every matrix of the stack) and the batched inverse.

@@ -13,7 +13,7 @@ on numpy arrays:
   batched DMMA GEMM. The reference has no stacked matmul (backend.cpp:122
   rejects ndim != 2); this is the product its stacked ``matrix_power`` runs per
   matrix, offered as one call. Leading axes broadcast as in numpy.matmul.
-* ``matrix_power(a, n)`` -- linalg.cpp:443-455, stacks batched.cpp:83-84.
+* ``matrix_power(a, n)`` -- linalg.cpp:440-454, stacks batched.cpp:83-84.
 * ``tensorsolve(a, b, axes)``, ``tensorinv(a, ind)`` -- tensor_solve.cpp:10-49.
 * ``cond(a, p)`` -- tensor.cpp:359-393 for p in {1, -1, inf, -inf, "fro"}:
   norm(a, p) * norm(inv(a), p), inf when a is singular. The 2-norm forms
@@ -285,7 +285,7 @@ def matmul_batched(a, b, backend=None):
 
 
 def matrix_power(a, n, backend=None):
-    """numpp::linalg::matrix_power (linalg.cpp:443-455; stacks batched.cpp:83-84).
+    """numpp::linalg::matrix_power (linalg.cpp:440-454; stacks batched.cpp:83-84).
 
     n = 0 gives the identity, n < 0 inverts first (``LinAlgError("Singular
     matrix")`` when a matrix of the stack is singular), then binary

@@ -107,7 +107,7 @@ class Oracle:
         return Cm
 
     def matrix_power(self, A, p):
-        """(count, n, n) stack to the integer power p, restating src/linalg/linalg.cpp:443-455
+        """(count, n, n) stack to the integer power p, restating src/linalg/linalg.cpp:440-454
         per matrix (batched.cpp:83-84): the identity for p = 0, the inverse first for p < 0,
         then binary exponentiation with the p-order matmul. ok[i] = 0 when p < 0 and
         matrix i is singular (the reference raises linalg_error there)."""

@@ -87,7 +87,7 @@ int ref_slogdet(int nda, const int64_t* sa, int dta, const void* A, void* sign, 
   });
 }
 
-// matrix_power (src/linalg/linalg.cpp:443-455; stacks batched.cpp:83-84).
+// matrix_power (src/linalg/linalg.cpp:440-454; stacks batched.cpp:83-84).
 int ref_matrix_power(int nda, const int64_t* sa, int dta, const void* A, int64_t p, void* out,
                      int* o_dt, int64_t* o_size, char* err, int errlen) {
   return guard(err, errlen, [&] {

@@ -1,4 +1,4 @@
-"""The C-ABI library loads, exports every symbol include/numpp_b200.h declares,
+"""The C-ABI library loads, exports every symbol include/numpp_b200*.h declare,
 and fails loudly (an error status, no fallback) where no sm_100 device is visible.
 No compute call is made here."""
 import ctypes as C
@@ -12,11 +12,11 @@ import pytest
 from numpp_b200 import _lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "numpp_b200.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in ("numpp_b200.h", "numpp_b200_dlpack.h")]
 
 
 def declared():
-    text = open(HEADER).read()
+    text = "".join(open(h).read() for h in HEADERS)
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(nppb_\w+)\s*\(", text)))
 
@@ -25,7 +25,7 @@ def test_header_declares_the_path():
     names = declared()
     for must in ("nppb_gemm", "nppb_solve_batched", "nppb_inv_batched", "nppb_det_batched",
                  "nppb_slogdet_batched", "nppb_getrf_batched", "nppb_getrs_batched",
-                 "nppb_plan_create", "nppb_plan_execute"):
+                 "nppb_plan_create", "nppb_plan_execute", "nppb_dl_linalg", "nppb_dl_matmul"):
         assert must in names
 
 

@@ -144,7 +144,7 @@ def test_stack_is_passed_as_one_batch(be):
 
 
 def test_matrix_power(golden, be):
-    """linalg.cpp:443-455 through the mirror: same values, dtype and errors as the reference."""
+    """linalg.cpp:440-454 through the mirror: same values, dtype and errors as the reference."""
     for p in (0, 1, 2, 7, -1, -3):
         R = la.matrix_power(golden["mp2_A"], p, backend=be)
         assert R.shape == (2, 2) and np.array_equal(R, golden[f"mp2_p{p}"]), p
@@ -215,3 +215,17 @@ def test_cond(be):
             la.cond(A, p, backend=be)
     with pytest.raises(ValueError):
         la.cond(A, "nuc", backend=be)
+
+
+def test_device_mirror_declines_host_tensors():
+    """numpp_b200.device serves CUDA tensors only; host tensors go to the host mirror."""
+    torch = pytest.importorskip("torch")
+    from numpp_b200 import device as dev
+    with pytest.raises(la.Declined):
+        dev.det(torch.eye(3, dtype=torch.float64))
+    with pytest.raises(la.Declined):
+        dev.solve(torch.eye(3, dtype=torch.float64), torch.ones(3, dtype=torch.float64))
+    with pytest.raises(la.Declined):       # numpy speaks DLPack too, from the host
+        dev.inv(np.eye(3))
+    with pytest.raises(TypeError):
+        dev.inv([[1.0, 0.0], [0.0, 1.0]])

@@ -34,7 +34,7 @@ def check_vs_oracle(sys, X, Inv, Det, Sign, Logabs, info, oracle):
             d = Inv[o:o + n * n] - invo[o:o + n * n]
             assert np.linalg.norm(d) <= 1e-12 * cond * max(np.linalg.norm(invo[o:o + n * n]), 1e-300)
     fin = Logabs < 700.0   # det overflows to +-inf past e^709; compare where it is finite
-    np.testing.assert_allclose(Det[fin], (Sign * np.exp(Logabs))[fin], rtol=1e-9)
+    np.testing.assert_allclose(Det[fin], Sign[fin] * np.exp(Logabs[fin]), rtol=1e-9)
     assert np.all(np.isinf(Det[~fin]) | (np.abs(Det[~fin]) > 1e300))
 
 

@@ -121,7 +121,7 @@ def test_oracle_vs_numpy_tolerance(oracle):
 
 def test_matrix_power_known_answers(golden, oracle):
     """test_linalg_mined3.cpp:29-40 and a seeded stack: the restatement of
-    linalg.cpp:443-455 reproduces the reference bit for bit."""
+    linalg.cpp:440-454 reproduces the reference bit for bit."""
     P = golden["mp2_A"][None]
     for p in (0, 1, 2, 7, -1, -3):
         R, ok = oracle.matrix_power(P, p)
