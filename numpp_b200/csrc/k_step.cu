@@ -123,25 +123,73 @@ __device__ __forceinline__ typename Pair<T>::type make_pair2(T x, T y) {
 }
 
 // ---------------------------------------------------------------------------
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool pred) {
+  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(BYTES),
+               "r"(pred ? BYTES : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Pivot candidate of one column among this warp's rows: the first largest
+// |a| in position order over rows at or below position j (the reference's
+// rule, linalg.cpp:55-57), reduced over the warp. The thread holding it also
+// returns 1 / value in rp (the multiplier scale if it wins).
+template <class T, int RPT>
+__device__ __forceinline__ void column_candidate(const T (&v)[RPT], const int (&pos)[RPT], const bool (&valid)[RPT],
+                                                 int j, T& best, int& key, T& rp) {
+  best = T(-1);
+  key = INT_MAX;
+#pragma unroll
+  for (int q = 0; q < RPT; ++q) {
+    if (valid[q] && pos[q] >= j) {
+      const T x = fabs(v[q]);
+      if (x > best || (x == best && pos[q] < key)) { best = x; key = pos[q]; }
+    }
+  }
+  warp_argmax_abs(best, key);
+  rp = T(0);
+#pragma unroll
+  for (int q = 0; q < RPT; ++q)
+    if (valid[q] && pos[q] == key) rp = T(1) / v[q];
+}
+
 // k_panel
 // CS CTAs per system (a cluster when CS > 1); CTA `rank` holds panel rows
 // [rank*NT*RPT, (rank+1)*NT*RPT). Rank 0 holds the top rows and does the
 // per-panel bookkeeping (pivots, L11^-1, det, row moves of the top rows).
+// The panel moves between global memory and registers through a shared
+// staging tile (whole rows per warp: coalesced); the column loop is fully
+// unrolled, so every register index and every column range is static.
+template <class T, int NT, int RPT>
+constexpr size_t panel_smem() {
+  return sizeof(T) * (size_t)NT * RPT * (NB + 1) + sizeof(int) * (size_t)NT * RPT;
+}
+
 template <class T, int NT, int RPT, int CS>
 __global__ void __launch_bounds__(NT, (RPT == 1 ? 65536 / (NT * 128) : 1))
 k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
   using P2 = typename Pair<T>::type;
   constexpr int NW = NT / 32;
+  constexpr int ROWS = NT * RPT;  // panel rows held by this CTA
+  constexpr int PS = NB + 1;      // staging row stride: conflict-free row-per-thread access
   __shared__ __align__(16) T cand_row[2][NW][NB];
   __shared__ T cand_v[2][NW];
   __shared__ int cand_k[2][NW];
+  __shared__ T cand_rp[2][NW];
   __shared__ __align__(16) T xc_row[2][CS][NB];  // each CTA's candidate, pushed by every CTA of the cluster
   __shared__ T xc_v[2][CS];
   __shared__ int xc_k[2][CS];
+  __shared__ T xc_rp[2][CS];
   __shared__ T L11[NB][LS];
   __shared__ T Xinv[NB][LS];
   __shared__ T pvals[NB];
   __shared__ int s_ndisp;
+  extern __shared__ __align__(16) unsigned char panel_dyn[];
+  T* stage = reinterpret_cast<T*>(panel_dyn);                // ROWS x PS
+  int* spos = reinterpret_cast<int*>(stage + (size_t)ROWS * PS);  // ROWS
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int rank = CS > 1 ? (int)blockIdx.x % CS : 0;
@@ -165,146 +213,149 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
     }
   }
 
+  // rows in: warp w copies rows w, w + NW, ... (lane = column; past kb and m zero)
+  const int r0 = rank * ROWS;
+#pragma unroll 4
+  for (int rr = warp; rr < ROWS; rr += NW) {
+    const int r = r0 + rr;
+    const bool ok = r < m && lane < kb;
+    cp_async<sizeof(T)>(&stage[rr * PS + lane], ok ? src + (int64_t)(k0 + r) * n + k0 + lane : src, ok);
+  }
+  cp_async_commit();
+  if (tid == 0) s_ndisp = 0;
+  cp_async_wait<0>();
+  __syncthreads();
   T a[RPT][NB];
   int pos[RPT];
   bool valid[RPT];
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
-    const int r = rank * NT * RPT + tid + q * NT;
+    const int r = r0 + tid + q * NT;
     valid[q] = r < m;
     pos[q] = r;
-    const T* row = src + (int64_t)(k0 + r) * n + k0;
 #pragma unroll
-    for (int c = 0; c < NB; ++c) a[q][c] = (valid[q] && c < kb) ? row[c] : T(0);
+    for (int c = 0; c < NB; ++c) a[q][c] = stage[(tid + q * NT) * PS + c];
   }
-  if (tid == 0) s_ndisp = 0;
 
-  // Column loop. Each row is kept rotated so that the current block of 8
-  // columns always sits in a[q][0..7]: the body below is written once for 8
-  // columns (compile-time register indices) and run 4 times, with an 8-place
-  // circular rotation in between; after the 4th rotation the row is back in
-  // column order. The multiplier L (rows below the pivot) overwrites the
-  // column entry it came from. Small code, few moves per column.
+  // Column loop, software-pipelined: iteration j publishes the candidates of
+  // column j (found at the end of iteration j-1), takes the winner after the
+  // barrier, updates column j+1 first and searches it (the warp reductions and
+  // the candidate owner's reciprocal overlap the rank-1 update of the columns
+  // after it). The multiplier L (rows below the pivot) overwrites the column
+  // entry it came from. Every element sees the same operations in the same
+  // order as in a plain right-looking column loop.
   int info = 0;
   int nswap = 0;
+  T nbest;
+  int nkey;
+  T nrp;  // 1 / (this thread's candidate value), valid in the owner of nkey
+  {
+    T v[RPT];
+#pragma unroll
+    for (int q = 0; q < RPT; ++q) v[q] = a[q][0];
+    column_candidate<T, RPT>(v, pos, valid, 0, nbest, nkey, nrp);
+  }
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    if (j < kb && !info) {  // uniform across the CTA
+      const int par = j & 1;
+      if (lane == 0) { cand_v[par][warp] = nbest; cand_k[par][warp] = nkey; }
+      // the candidate row from column j on (earlier columns are never read)
+#pragma unroll
+      for (int q = 0; q < RPT; ++q) {
+        if (valid[q] && pos[q] == nkey) {
+          P2* cr = reinterpret_cast<P2*>(cand_row[par][warp]);
+#pragma unroll
+          for (int c2 = j / 2; c2 < NB / 2; ++c2) cr[c2] = make_pair2<T>(a[q][2 * c2], a[q][2 * c2 + 1]);
+          cand_rp[par][warp] = nrp;
+        }
+      }
+      __syncthreads();
+      T gb = T(-1);
+      int gk = INT_MAX, gw = 0;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) {
+        const T v = cand_v[par][w];
+        const int k = cand_k[par][w];
+        if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
+      }
+      const T* prow = cand_row[par][gw];
+      T rp = cand_rp[par][gw];
+      if constexpr (CS > 1) {
+        // every CTA pushes its candidate into slot `rank` of every CTA, then
+        // one cluster barrier; the slots alternate with the column parity, so
+        // a slot is rewritten only after every CTA has passed the next barrier
+        cg::cluster_group cl = cg::this_cluster();
+        if (warp == 0) {
+          const T rv = lane >= (j & ~1) ? prow[lane] : T(0);
 #pragma unroll 1
-  for (int jb = 0; jb < NB; jb += 8) {
-#pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int j = jb + u;
-      if (j < kb && !info) {  // uniform across the CTA
-        T best = T(-1);
-        int key = INT_MAX;
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          if (valid[q] && pos[q] >= j) {
-            const T v = fabs(a[q][u]);
-            if (v > best || (v == best && pos[q] < key)) { best = v; key = pos[q]; }
-          }
-        }
-        warp_argmax_abs(best, key);
-        const int par = j & 1;
-        if (lane == 0) { cand_v[par][warp] = best; cand_k[par][warp] = key; }
-        // the candidate row is published with its finished columns (rotated
-        // slots past lim) zeroed, so the update below needs no predicates
-        const int lim = NB - 1 - jb;
-#pragma unroll
-        for (int q = 0; q < RPT; ++q) {
-          if (valid[q] && pos[q] == key) {
-            P2* cr = reinterpret_cast<P2*>(cand_row[par][warp]);
-#pragma unroll
-            for (int c = 0; c < NB / 2; ++c)
-              cr[c] = make_pair2<T>(2 * c <= lim ? a[q][2 * c] : T(0), 2 * c + 1 <= lim ? a[q][2 * c + 1] : T(0));
-          }
-        }
-        __syncthreads();
-        T gb = T(-1);
-        int gk = INT_MAX, gw = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-          const T v = cand_v[par][w];
-          const int k = cand_k[par][w];
-          if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
-        }
-        const T* prow = cand_row[par][gw];
-        if constexpr (CS > 1) {
-          // every CTA pushes its candidate into slot `rank` of every CTA, then
-          // one cluster barrier; the slots alternate with the column parity, so
-          // a slot is rewritten only after every CTA has passed the next barrier
-          cg::cluster_group cl = cg::this_cluster();
-          if (warp == 0) {
-            const T rv = prow[lane];
-#pragma unroll 1
-            for (int to = 0; to < CS; ++to) {
-              cl.map_shared_rank(&xc_row[par][rank][0], to)[lane] = rv;
-              if (lane == 0) {
-                *cl.map_shared_rank(&xc_v[par][rank], to) = gb;
-                *cl.map_shared_rank(&xc_k[par][rank], to) = gk;
-              }
+          for (int to = 0; to < CS; ++to) {
+            cl.map_shared_rank(&xc_row[par][rank][0], to)[lane] = rv;
+            if (lane == 0) {
+              *cl.map_shared_rank(&xc_v[par][rank], to) = gb;
+              *cl.map_shared_rank(&xc_k[par][rank], to) = gk;
+              *cl.map_shared_rank(&xc_rp[par][rank], to) = rp;
             }
           }
-          cl.sync();
-          gb = T(-1);
-          gk = INT_MAX;
-          int gr = 0;
-#pragma unroll
-          for (int r = 0; r < CS; ++r) {
-            const T v = xc_v[par][r];
-            const int k = xc_k[par][r];
-            if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gr = r; }
-          }
-          prow = xc_row[par][gr];
         }
-        if (gb == T(0)) {
-          info = k0 + j + 1;
-        } else {
-          const P2* pr2 = reinterpret_cast<const P2*>(prow);
-          const T pj = prow[u];
+        cl.sync();
+        gb = T(-1);
+        gk = INT_MAX;
+        int gr = 0;
+#pragma unroll
+        for (int r = 0; r < CS; ++r) {
+          const T v = xc_v[par][r];
+          const int k = xc_k[par][r];
+          if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gr = r; }
+        }
+        prow = xc_row[par][gr];
+        rp = xc_rp[par][gr];
+      }
+      if (gb == T(0)) {
+        info = k0 + j + 1;
+      } else {
+        const P2* pr2 = reinterpret_cast<const P2*>(prow);
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          if (valid[q]) {
+            if (pos[q] == j) pos[q] = gk;
+            else if (pos[q] == gk) pos[q] = j;
+          }
+        }
+        if (tid == 0 && rank == 0) {
+          pvals[j] = prow[j];
+          if (sa.ipiv) sa.ipiv[d.piv_off + k0 + j] = k0 + gk;
+        }
+        nswap += (gk != j);
+        T f[RPT];
+#pragma unroll
+        for (int q = 0; q < RPT; ++q) {
+          const bool below = valid[q] && pos[q] > j;
+          f[q] = below ? a[q][j] * rp : T(0);
+          if (below) a[q][j] = f[q];
+        }
+        if (j + 1 < NB) {
+          // column j+1 first, then its candidates
+          const T t = prow[j + 1];
+          T v[RPT];
 #pragma unroll
           for (int q = 0; q < RPT; ++q) {
-            if (valid[q]) {
-              if (pos[q] == j) pos[q] = gk;
-              else if (pos[q] == gk) pos[q] = j;
-            }
+            a[q][j + 1] = fma(-f[q], t, a[q][j + 1]);
+            v[q] = a[q][j + 1];
           }
-          if (tid == 0 && rank == 0) {
-            pvals[j] = pj;
-            if (sa.ipiv) sa.ipiv[d.piv_off + k0 + j] = k0 + gk;
-          }
-          nswap += (gk != j);
-          // rotated columns u+1 .. lim hold the trailing columns j+1 .. 31; the
-          // published pivot row is zero beyond lim, so those slots stay as they are
-          const T rp = T(1) / pj;
-          T f[RPT];
+          if (j + 1 < kb) column_candidate<T, RPT>(v, pos, valid, j + 1, nbest, nkey, nrp);
 #pragma unroll
-          for (int q = 0; q < RPT; ++q) {
-            const bool below = valid[q] && pos[q] > j;
-            f[q] = below ? a[q][u] * rp : T(0);
-            if (below) a[q][u] = f[q];
-          }
-#pragma unroll
-          for (int c2 = (u + 1) / 2; c2 < NB / 2; ++c2) {
-            const P2 t = pr2[c2];
+          for (int c2 = (j + 2) / 2; c2 < NB / 2; ++c2) {
+            const P2 t2 = pr2[c2];
             const int c = 2 * c2;
 #pragma unroll
             for (int q = 0; q < RPT; ++q) {
-              if (c > u) a[q][c] = fma(-f[q], t.x, a[q][c]);
-              a[q][c + 1] = fma(-f[q], t.y, a[q][c + 1]);
+              if (c > j + 1) a[q][c] = fma(-f[q], t2.x, a[q][c]);
+              a[q][c + 1] = fma(-f[q], t2.y, a[q][c + 1]);
             }
           }
         }
       }
-    }
-    // circular rotation by 8
-#pragma unroll
-    for (int q = 0; q < RPT; ++q) {
-      T t[8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) t[c] = a[q][c];
-#pragma unroll
-      for (int c = 0; c < NB - 8; ++c) a[q][c] = a[q][c + 8];
-#pragma unroll
-      for (int c = 0; c < 8; ++c) a[q][NB - 8 + c] = t[c];
     }
   }
 
@@ -319,24 +370,25 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
     return;
   }
 
-  // panel back at the pivoted positions; the strictly lower part of L11 into
-  // rank 0's shared memory (identity-initialised before the column loop)
+  // panel back at the pivoted positions: each thread stages its rows with
+  // their positions, then warps write whole rows; the strictly lower part of
+  // L11 into rank 0's shared memory (identity-initialised before the loop)
   T(*L11r)[LS] = L11;
   if constexpr (CS > 1) L11r = reinterpret_cast<T(*)[LS]>(cg::this_cluster().map_shared_rank(&L11[0][0], 0));
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
+    const int sl = tid + q * NT;
+    spos[sl] = valid[q] ? pos[q] : -1;
     if (valid[q]) {
-      T* row = dst + (int64_t)(k0 + pos[q]) * n + k0;
-#pragma unroll 32
-      for (int c = 0; c < NB; ++c)
-        if (c < kb) row[c] = a[q][c];
+#pragma unroll
+      for (int c = 0; c < NB; ++c) stage[sl * PS + c] = a[q][c];
       if (pos[q] < kb) {
-#pragma unroll 32
+#pragma unroll
         for (int c = 0; c < NB; ++c)
           if (c < pos[q]) L11r[pos[q]][c] = a[q][c];
       }
       // row moves for the other columns (rows r < kb all live in rank 0)
-      const int r = rank * NT * RPT + tid + q * NT;
+      const int r = r0 + sl;
       if (pos[q] < kb) {
         sc->top_src[pos[q]] = r;
       } else if (r < kb) {
@@ -345,6 +397,12 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
         sc->disp_src[k] = r;
       }
     }
+  }
+  __syncthreads();
+#pragma unroll 4
+  for (int sl = warp; sl < ROWS; sl += NW) {
+    const int p = spos[sl];
+    if (p >= 0 && lane < kb) dst[(int64_t)(k0 + p) * n + k0 + lane] = stage[sl * PS + lane];
   }
   if constexpr (CS > 1) {
     cg::this_cluster().sync();  // no shared memory of another CTA is touched after this
@@ -404,15 +462,6 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
 
 // ---------------------------------------------------------------------------
 // Shared helpers for the 64-column strip kernels.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, bool pred) {
-  const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(sa), "l"(gmem), "n"(BYTES),
-               "r"(pred ? BYTES : 0));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 template <class T>
 struct Seg {
@@ -1781,8 +1830,28 @@ cudaError_t prepare_narrow() {
                               (int)narrow_smem<T>());
 }
 
+template <class T, int NT, int RPT, int CS>
+cudaError_t prepare_panel1() {
+  return cudaFuncSetAttribute(k_panel<T, NT, RPT, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)panel_smem<T, NT, RPT>());
+}
+
+template <class T>
+cudaError_t prepare_panel() {
+  cudaError_t e = prepare_panel1<T, 64, 1, 1>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 128, 1, 1>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 256, 1, 1>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 1>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 2>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 4>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 8>();
+  return e;
+}
+
 cudaError_t step_prepare() {
   cudaError_t e = prepare_narrow<double>();
+  if (e == cudaSuccess) e = prepare_panel<double>();
+  if (e == cudaSuccess) e = prepare_panel<float>();
   if (e == cudaSuccess) e = prepare_narrow<float>();
   if (e == cudaSuccess) e = prepare_update<double, kUpdFp32>();
   if (e == cudaSuccess) e = prepare_update<float, kUpdFp32>();
@@ -1803,7 +1872,7 @@ cudaError_t launch_cluster_panel(const StepArgsT<T>& sa, const int32_t* list, in
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)nsys * CS);
   cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = panel_smem<T, 256, 2>();
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1819,10 +1888,10 @@ template <class T>
 cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int mmax, int k0,
                          cudaStream_t st) {
   if (nsys <= 0) return cudaSuccess;
-  if (mmax <= 64) k_panel<T, 64, 1, 1><<<nsys, 64, 0, st>>>(sa, list, k0);
-  else if (mmax <= 128) k_panel<T, 128, 1, 1><<<nsys, 128, 0, st>>>(sa, list, k0);
-  else if (mmax <= 256) k_panel<T, 256, 1, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
-  else if (mmax <= 512) k_panel<T, 256, 2, 1><<<nsys, 256, 0, st>>>(sa, list, k0);
+  if (mmax <= 64) k_panel<T, 64, 1, 1><<<nsys, 64, panel_smem<T, 64, 1>(), st>>>(sa, list, k0);
+  else if (mmax <= 128) k_panel<T, 128, 1, 1><<<nsys, 128, panel_smem<T, 128, 1>(), st>>>(sa, list, k0);
+  else if (mmax <= 256) k_panel<T, 256, 1, 1><<<nsys, 256, panel_smem<T, 256, 1>(), st>>>(sa, list, k0);
+  else if (mmax <= 512) k_panel<T, 256, 2, 1><<<nsys, 256, panel_smem<T, 256, 2>(), st>>>(sa, list, k0);
   else if (mmax <= 1024) return launch_cluster_panel<T, 2>(sa, list, nsys, k0, st);
   else if (mmax <= 2048) return launch_cluster_panel<T, 4>(sa, list, nsys, k0, st);
   else if (mmax <= 4096) return launch_cluster_panel<T, 8>(sa, list, nsys, k0, st);
