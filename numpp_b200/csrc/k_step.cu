@@ -273,11 +273,21 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
       __syncthreads();
       T gb = T(-1);
       int gk = INT_MAX, gw = 0;
+      if constexpr (NW > 4) {
+        // lane w < NW holds warp w's candidate; the same rule by warp reductions
+        const int ck = lane < NW ? cand_k[par][lane] : INT_MAX;
+        gb = lane < NW ? cand_v[par][lane] : T(-1);
+        gk = ck;
+        warp_argmax_abs(gb, gk);
+        gw = __ffs(__ballot_sync(0xffffffffu, lane < NW && ck == gk)) - 1;
+        if (gw < 0) gw = 0;  // no candidate anywhere: gb is 0 and the column is singular
+      } else {
 #pragma unroll
-      for (int w = 0; w < NW; ++w) {
-        const T v = cand_v[par][w];
-        const int k = cand_k[par][w];
-        if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
+        for (int w = 0; w < NW; ++w) {
+          const T v = cand_v[par][w];
+          const int k = cand_k[par][w];
+          if (v > gb || (v == gb && k < gk)) { gb = v; gk = k; gw = w; }
+        }
       }
       const T* prow = cand_row[par][gw];
       T rp = cand_rp[par][gw];
@@ -1841,10 +1851,10 @@ cudaError_t prepare_panel() {
   cudaError_t e = prepare_panel1<T, 64, 1, 1>();
   if (e == cudaSuccess) e = prepare_panel1<T, 128, 1, 1>();
   if (e == cudaSuccess) e = prepare_panel1<T, 256, 1, 1>();
-  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 1>();
-  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 2>();
-  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 4>();
-  if (e == cudaSuccess) e = prepare_panel1<T, 256, 2, 8>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 512, 1, 1>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 512, 1, 2>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 512, 1, 4>();
+  if (e == cudaSuccess) e = prepare_panel1<T, 512, 1, 8>();
   return e;
 }
 
@@ -1871,8 +1881,8 @@ template <class T, int CS>
 cudaError_t launch_cluster_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, int k0, cudaStream_t st) {
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)nsys * CS);
-  cfg.blockDim = dim3(256);
-  cfg.dynamicSmemBytes = panel_smem<T, 256, 2>();
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = panel_smem<T, 512, 1>();
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -1881,7 +1891,7 @@ cudaError_t launch_cluster_panel(const StepArgsT<T>& sa, const int32_t* list, in
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_panel<T, 256, 2, CS>, sa, list, k0);
+  return cudaLaunchKernelEx(&cfg, k_panel<T, 512, 1, CS>, sa, list, k0);
 }
 
 template <class T>
@@ -1891,7 +1901,7 @@ cudaError_t launch_panel(const StepArgsT<T>& sa, const int32_t* list, int nsys, 
   if (mmax <= 64) k_panel<T, 64, 1, 1><<<nsys, 64, panel_smem<T, 64, 1>(), st>>>(sa, list, k0);
   else if (mmax <= 128) k_panel<T, 128, 1, 1><<<nsys, 128, panel_smem<T, 128, 1>(), st>>>(sa, list, k0);
   else if (mmax <= 256) k_panel<T, 256, 1, 1><<<nsys, 256, panel_smem<T, 256, 1>(), st>>>(sa, list, k0);
-  else if (mmax <= 512) k_panel<T, 256, 2, 1><<<nsys, 256, panel_smem<T, 256, 2>(), st>>>(sa, list, k0);
+  else if (mmax <= 512) k_panel<T, 512, 1, 1><<<nsys, 512, panel_smem<T, 512, 1>(), st>>>(sa, list, k0);
   else if (mmax <= 1024) return launch_cluster_panel<T, 2>(sa, list, nsys, k0, st);
   else if (mmax <= 2048) return launch_cluster_panel<T, 4>(sa, list, nsys, k0, st);
   else if (mmax <= 4096) return launch_cluster_panel<T, 8>(sa, list, nsys, k0, st);
