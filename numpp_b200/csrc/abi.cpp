@@ -109,6 +109,12 @@ int d_linalg(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA
     NPPB_RC(scratch<StepScratch>(sc_m, (size_t)count, st));
     StepArgs sa{};
     sa.scratch = sc_m.as<StepScratch>();
+    DevMem hist_m;
+    const int bmin = blocked_min_n();
+    if (bmin > 0 && n >= bmin) {  // two-level factorisation: per-system record of a block's panels
+      NPPB_RC(scratch<StepHist>(hist_m, (size_t)count, st));
+      sa.hist = hist_m.as<StepHist>();
+    }
     sa.A = (dA == LU) ? nullptr : dA;
     sa.LU = LU;
     sa.ipiv = dipiv;

@@ -80,20 +80,31 @@ __device__ __forceinline__ SysDesc step_desc(const StepArgsT<T>& sa, int s) {
 template <class T>
 __device__ __forceinline__ StepItem uniform_item(const StepArgsT<T>& sa, int b, int k0, bool back) {
   const int n = sa.un;
-  const int trail = n - k0 - NB;
+  StepItem it;
+  it.pad_ = 0;
+  if (sa.utrail) {  // trailing pass of a two-level factorisation: matrix strips right of the block
+    const int per = trailing_strips(n, sa.ubend);
+    it.sys = b / per;
+    it.kind = kSegMatrix;
+    it.c0 = sa.ubend + 64 * (b % per);
+    it.width = (int16_t)min(64, n - it.c0);
+    return it;
+  }
+  const bool blk = sa.ubend > 0 && !back;
+  const int mend = blk ? sa.ubend : n;  // matrix strips end here
+  const int trail = mend - k0 - NB;
   const int nm = back ? 0 : (trail > 0 ? (trail + 63) / 64 : 0);
   const int nr = (sa.unrhs + 63) / 64;
   const int ni = sa.uinv ? (n + 63) / 64 : 0;
-  const int nl = (!back && sa.uleft) ? (k0 + 63) / 64 : 0;
+  const int lo = (blk && !sa.uleft) ? sa.ubbeg : 0;  // moves-only strips from here to the panel
+  const int nl = (!back && (sa.uleft || blk) && k0 > lo) ? (k0 - lo + 63) / 64 : 0;
   const int per = nm + nr + ni + nl;
-  StepItem it;
   it.sys = b / per;
   int r = b % per;
-  it.pad_ = 0;
   if (r < nm) {
     it.kind = kSegMatrix;
     it.c0 = k0 + NB + 64 * r;
-    it.width = (int16_t)min(64, n - it.c0);
+    it.width = (int16_t)min(64, mend - it.c0);
   } else if ((r -= nm) < nr) {
     it.kind = kSegRhs;
     it.c0 = 64 * r;
@@ -105,7 +116,7 @@ __device__ __forceinline__ StepItem uniform_item(const StepArgsT<T>& sa, int b, 
   } else {
     r -= ni;
     it.kind = kSegLeft;
-    it.c0 = 64 * r;
+    it.c0 = lo + 64 * r;
     it.width = (int16_t)min(64, k0 - it.c0);
   }
   return it;
@@ -421,6 +432,14 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
     __syncthreads();
   }
   if (tid == 0) sc->ndisp = s_ndisp;
+  StepHistT<T>* hs = sa.hist ? sa.hist + d.pad_ : nullptr;
+  if (hs && tid < NB) {
+    // every CTA's writes of the row moves are visible after the barrier above
+    hs->top_src[sa.hslot][tid] = sc->top_src[tid];
+    hs->disp_dst[sa.hslot][tid] = sc->disp_dst[tid];
+    hs->disp_src[sa.hslot][tid] = sc->disp_src[tid];
+    if (tid == 0) hs->ndisp[sa.hslot] = s_ndisp;
+  }
 
   // L11^-1 (unit lower, identity-padded past kb): lane c builds column c in
   // shared memory; four partial sums per entry shorten the dependent chain
@@ -441,6 +460,7 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
       const T x = (p0 + p1) + (p2 + p3);
       Xinv[i][lane] = x;
       sc->linv[i * NB + lane] = x;
+      if (hs) hs->linv[sa.hslot][i * NB + lane] = x;
     }
   }
 
@@ -840,7 +860,8 @@ __device__ __forceinline__ bool update_item(const StepArgsT<T>& sa, const StepIt
     it = uniform_item(sa, blockIdx.x, k0, false);
     return true;
   }
-  const int per = uniform_update_strips(sa.un, sa.unrhs, sa.uinv, k0, sa.uleft);
+  const int per = sa.ubend > 0 ? blocked_update_strips(sa.un, sa.unrhs, sa.uinv, k0, sa.uleft, sa.ubbeg, sa.ubend)
+                               : uniform_update_strips(sa.un, sa.unrhs, sa.uinv, k0, sa.uleft);
   if (part == 1) {
     it = uniform_item(sa, (int)blockIdx.x * per, k0, false);
     return it.kind == kSegMatrix;
@@ -870,11 +891,15 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
   if (sc->info) return;
   const int n = d.n, m = n - k0, kb = min(NB, m), w = it.width, c0 = it.c0;
   const Seg<T> s = segment(sa, d, it.kind, k0);
-  const int nd = sc->ndisp;
+  // the trailing pass of a two-level factorisation replays a recorded panel
+  const StepHistT<T>* hs = sa.utrail ? sa.hist + d.pad_ : nullptr;
+  const int hsl = sa.hslot;
+  const int mv = hs ? sa.umoves : 0;  // 1: row moves only, 2: U12 of rows already in place
+  const int nd = mv == 2 ? 0 : hs ? hs->ndisp[hsl] : sc->ndisp;
   if (tid < NB) {
-    tsrc[tid] = tid < kb ? sc->top_src[tid] : 0;
-    ddst[tid] = tid < nd ? sc->disp_dst[tid] : 0;
-    dsrc[tid] = tid < nd ? sc->disp_src[tid] : 0;
+    tsrc[tid] = tid < kb ? (mv == 2 ? tid : hs ? hs->top_src[hsl][tid] : sc->top_src[tid]) : 0;
+    ddst[tid] = tid < nd ? (hs ? hs->disp_dst[hsl][tid] : sc->disp_dst[tid]) : 0;
+    dsrc[tid] = tid < nd ? (hs ? hs->disp_src[hsl][tid] : sc->disp_src[tid]) : 0;
   }
   __syncthreads();
   for (int idx = tid; idx < NB * 64; idx += UT) {
@@ -888,14 +913,15 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     const int i = idx >> 6, c = idx & 63;
     if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
   }
-  if (it.kind == kSegLeft) {
+  if (it.kind == kSegLeft || mv == 1) {
     for (int idx = tid; idx < NB * 64; idx += UT) {
       const int i = idx >> 6, c = idx & 63;
       if (c < w && i < kb) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = Tm[i * WS + c];
     }
     return;
   }
-  for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = sc->linv[idx];
+  const T* linv = hs ? hs->linv[hsl] : sc->linv;
+  for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
   __syncthreads();
   Acc32<T> u;
   u.mma(Li, Tm);
@@ -1000,8 +1026,9 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) 
   const int n = d.n;
   const int rg = part == 1 ? RG1 : RG;  // rows per CTA
   const int rb = k0 + NB + (int)blockIdx.y * rg;
-  if (rb >= n) return;  // includes the last panel (nothing below it)
-  const int re = min(n, rb + rg), w = it.width, c0 = it.c0;
+  const int rlim = sa.urow_end > 0 ? min(n, sa.urow_end) : n;
+  if (rb >= rlim) return;  // includes the last panel (nothing below it)
+  const int re = min(rlim, rb + rg), w = it.width, c0 = it.c0;
   const Seg<T> s = segment(sa, d, it.kind, k0);
   const int64_t ld = s.ld;
   // step 0 out of place: rows holding a displaced row are already in dst
@@ -1182,8 +1209,9 @@ k_update_tc(StepArgsT<float> sa, const StepItem* __restrict__ items, int k0, int
   const int n = d.n;
   const int rg = part == 1 ? RG1 : RG;  // rows per CTA
   const int rb = k0 + NB + (int)blockIdx.y * rg;
-  if (rb >= n) return;  // includes the last panel (nothing below it)
-  const int re = min(n, rb + rg), w = it.width, c0 = it.c0;
+  const int rlim = sa.urow_end > 0 ? min(n, sa.urow_end) : n;
+  if (rb >= rlim) return;  // includes the last panel (nothing below it)
+  const int re = min(rlim, rb + rg), w = it.width, c0 = it.c0;
   const Seg<float> s = segment(sa, d, it.kind, k0);
   const int64_t ld = s.ld;
   // step 0 out of place: rows holding a displaced row are already in dst
@@ -1819,6 +1847,201 @@ cudaError_t windowed(const StepArgsT<T>& sa, const StepItem* items, int nitems, 
   return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// k_block_rows: the trailing pass after an outer block of the two-level
+// factorisation, one CTA per (system, 64-column strip right of the block).
+// First the block's recorded row moves, panel by panel, on the strip in
+// global memory (rows no update has touched yet, as LAPACK's laswp); then the
+// block's rows of the strip in shared memory: per panel, U12 = L11^-1 A12
+// (DMMA) and the update of the block rows below that panel; then the rows go
+// back. What is left below the block is one GEMM (k_block_gemm).
+template <class T>
+constexpr size_t block_rows_smem() {
+  return sizeof(T) * ((size_t)kStepNBO * WS + 64 * LS + NB * LS);
+}
+
+template <class T>
+__global__ void __launch_bounds__(UT)
+k_block_rows(StepArgsT<T> sa, int bbeg, int bend) {
+  extern __shared__ __align__(16) unsigned char br_raw[];
+  T* X = reinterpret_cast<T*>(br_raw);  // the block's rows of the strip, kStepNBO x WS
+  T* Lt = X + kStepNBO * WS;            // L rows below a panel inside the block, 64 x LS
+  T* Li = Lt + 64 * LS;                 // L11^-1 of a panel, NB x LS
+  __shared__ int tsrc[NB], ddst[NB], dsrc[NB];
+  const int tid = threadIdx.x;
+  const StepItem it = uniform_item(sa, blockIdx.x, bbeg, false);
+  const SysDesc d = step_desc(sa, it.sys);
+  if (sa.scratch[d.pad_].info) return;
+  const StepHistT<T>* hs = sa.hist + d.pad_;
+  const int n = d.n, w = it.width, c0 = it.c0, bw = bend - bbeg;
+  const int64_t ld = n;
+  T* const F = sa.LU + d.lu_off + c0;  // column c0 of row 0
+  // 1. row moves, in panel order (all reads of a panel before its writes)
+  for (int s = 0; s * NB < bw; ++s) {
+    const int k0 = bbeg + s * NB, kb = min(NB, n - k0), nd = hs->ndisp[s];
+    if (tid < NB) {
+      tsrc[tid] = tid < kb ? hs->top_src[s][tid] : 0;
+      ddst[tid] = tid < nd ? hs->disp_dst[s][tid] : 0;
+      dsrc[tid] = tid < nd ? hs->disp_src[s][tid] : 0;
+    }
+    __syncthreads();
+    T* Tm = X;
+    T* D = X + NB * WS;
+    for (int idx = tid; idx < NB * 64; idx += UT) {
+      const int i = idx >> 6, c = idx & 63;
+      const bool in = c < w;
+      Tm[i * WS + c] = (in && i < kb) ? F[(int64_t)(k0 + tsrc[i]) * ld + c] : T(0);
+      D[i * WS + c] = (in && i < nd) ? F[(int64_t)(k0 + dsrc[i]) * ld + c] : T(0);
+    }
+    __syncthreads();
+    for (int idx = tid; idx < NB * 64; idx += UT) {
+      const int i = idx >> 6, c = idx & 63;
+      if (c < w && i < nd) F[(int64_t)(k0 + ddst[i]) * ld + c] = D[i * WS + c];
+      if (c < w && i < kb) F[(int64_t)(k0 + i) * ld + c] = Tm[i * WS + c];
+    }
+    __syncthreads();
+  }
+  // 2. the block's rows into shared memory
+  for (int idx = tid; idx < kStepNBO * 64; idx += UT) {
+    const int i = idx >> 6, c = idx & 63;
+    X[i * WS + c] = (i < bw && c < w) ? F[(int64_t)(bbeg + i) * ld + c] : T(0);
+  }
+  // 3. per panel: U12, then the block rows below it
+  for (int s = 0; s * NB < bw; ++s) {
+    const int k0 = bbeg + s * NB;
+    const T* linv = hs->linv[s];
+    for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+    __syncthreads();
+    T* Xs = X + s * NB * WS;
+    {
+      Acc32<T> u;
+      u.mma(Li, Xs);
+      __syncthreads();
+      u.each([&](int i, int c, T& x) { Xs[i * WS + c] = x; });
+    }
+    for (int r0 = (s + 1) * NB; r0 < bw; r0 += 64) {
+      const int rows = min(64, bw - r0);
+      __syncthreads();
+      for (int idx = tid; idx < 64 * NB; idx += UT) {
+        const int i = idx >> 5, c = idx & 31;
+        Lt[i * LS + c] = i < rows ? sa.LU[d.lu_off + (int64_t)(bbeg + r0 + i) * ld + k0 + c] : T(0);
+      }
+      __syncthreads();
+      Acc64<T> acc;
+      acc.each([&](int r, int c, T& v) { v = r < rows ? X[(r0 + r) * WS + c] : T(0); });
+      acc.sub_mma(Lt, Xs);
+      acc.each([&](int r, int c, T& v) {
+        if (r < rows) X[(r0 + r) * WS + c] = v;
+      });
+    }
+    __syncthreads();
+  }
+  // 4. back
+  for (int idx = tid; idx < kStepNBO * 64; idx += UT) {
+    const int i = idx >> 6, c = idx & 63;
+    if (i < bw && c < w) F[(int64_t)(bbeg + i) * ld + c] = X[i * WS + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_block_gemm: the trailing update after an outer block of the two-level
+// factorisation, C -= L U with C = rows [bend, n) x columns [cbeg, cend), L =
+// rows [bend, n) x columns [bbeg, bend), U = rows [bbeg, bend) x [cbeg, cend),
+// all in place in the system's factor matrix (row-major, leading dimension n).
+// One CTA per 128 x 64 tile of C (grid.z = system); K = bend - bbeg <= 128 in
+// 8-deep slabs double-buffered through shared memory (cp.async), C read once
+// into the DMMA accumulators and written once.
+constexpr int GBM = 128, GBN = 64, GBK = 8, GNT = 256;
+constexpr int GAS = GBK + 1, GBS = GBN + 1;
+
+__global__ void __launch_bounds__(GNT, 2)
+k_block_gemm(StepArgsT<double> sa, int bbeg, int bend, int cbeg, int cend) {
+  __shared__ double As[2][GBM * GAS];
+  __shared__ double Bs[2][GBK * GBS];
+  const SysDesc d = step_desc(sa, (int)blockIdx.z);
+  if (sa.scratch[d.pad_].info) return;
+  const int n = d.n;
+  const int M = n - bend, N = cend - cbeg, K = bend - bbeg;
+  double* const F = sa.LU + d.lu_off;
+  const double* const Lp = F + (int64_t)bend * n + bbeg;  // M x K
+  const double* const Up = F + (int64_t)bbeg * n + cbeg;  // K x N
+  double* const Cp = F + (int64_t)bend * n + cbeg;        // M x N
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  const int bm = (int)blockIdx.y * GBM, bn = (int)blockIdx.x * GBN;
+  if (bm >= M || bn >= N) return;
+  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+
+  auto load = [&](int stage, int k0) {
+#pragma unroll
+    for (int i = 0; i < (GBM * GBK) / GNT; ++i) {
+      const int idx = tid + i * GNT;
+      const int r = idx / GBK, c = idx % GBK;
+      const bool ok = bm + r < M && k0 + c < K;
+      cp_async<8>(&As[stage][r * GAS + c], ok ? Lp + (int64_t)(bm + r) * n + k0 + c : Lp, ok);
+    }
+#pragma unroll
+    for (int i = 0; i < (GBK * GBN) / GNT; ++i) {
+      const int idx = tid + i * GNT;
+      const int r = idx / GBN, c = idx % GBN;
+      const bool ok = k0 + r < K && bn + c < N;
+      cp_async<8>(&Bs[stage][r * GBS + c], ok ? Up + (int64_t)(k0 + r) * n + bn + c : Up, ok);
+    }
+    cp_async_commit();
+  };
+
+  const int nk = (K + GBK - 1) / GBK;
+  load(0, 0);
+  double acc[4][4][2];
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi) {
+    const int row = bm + wm + mi * 8 + g;
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = bn + wn + ni * 8 + 2 * tq + e;
+        acc[mi][ni][e] = (row < M && col < N) ? Cp[(int64_t)row * n + col] : 0.0;
+      }
+    }
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    const int st = kt & 1;
+    if (kt + 1 < nk) {
+      load(st ^ 1, (kt + 1) * GBK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GBK; kk += 4) {
+      double af[4], bf[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi) af[mi] = -As[st][(wm + mi * 8 + g) * GAS + kk + tq];
+#pragma unroll
+      for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[st][(kk + tq) * GBS + wn + ni * 8 + g];
+#pragma unroll
+      for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) dmma884(acc[mi][ni], af[mi], bf[ni]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int mi = 0; mi < 4; ++mi) {
+    const int row = bm + wm + mi * 8 + g;
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int col = bn + wn + ni * 8 + 2 * tq + e;
+        if (row < M && col < N) Cp[(int64_t)row * n + col] = acc[mi][ni][e];
+      }
+    }
+  }
+}
+
 }  // namespace
 
 int tc_timeouts_take() {
@@ -1860,6 +2083,12 @@ cudaError_t prepare_panel() {
 
 cudaError_t step_prepare() {
   cudaError_t e = prepare_narrow<double>();
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_block_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_rows_smem<double>());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_block_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)block_rows_smem<float>());
   if (e == cudaSuccess) e = prepare_panel<double>();
   if (e == cudaSuccess) e = prepare_panel<float>();
   if (e == cudaSuccess) e = prepare_narrow<float>();
@@ -1957,6 +2186,32 @@ cudaError_t launch_update(const StepArgsT<T>& sa, const StepItem* items, int nit
 }
 
 template <class T>
+cudaError_t launch_block_gemm(const StepArgsT<T>& sa, int count, int bbeg, int bend, int cbeg, int cend,
+                              cudaStream_t st) {
+  const int M = sa.un - bend, N = cend - cbeg;
+  if (M <= 0 || N <= 0 || count <= 0) return cudaSuccess;
+  if constexpr (!std::is_same_v<T, double>) {
+    return cudaErrorInvalidValue;  // FP32 factors keep the one-level schedule
+  } else {
+    const dim3 grid((unsigned)((N + GBN - 1) / GBN), (unsigned)((M + GBM - 1) / GBM), (unsigned)count);
+    k_block_gemm<<<grid, GNT, 0, st>>>(sa, bbeg, bend, cbeg, cend);
+    return cudaGetLastError();
+  }
+}
+
+template <class T>
+cudaError_t launch_block_rows(const StepArgsT<T>& sa, int count, int bbeg, int bend, cudaStream_t st) {
+  const int64_t items = (int64_t)count * trailing_strips(sa.un, bend);
+  if (items <= 0) return cudaSuccess;
+  if (items > INT32_MAX) return cudaErrorInvalidValue;
+  StepArgsT<T> tr = sa;
+  tr.utrail = 1;
+  tr.ubend = bend;
+  k_block_rows<T><<<(unsigned)items, UT, block_rows_smem<T>(), st>>>(tr, bbeg, bend);
+  return cudaGetLastError();
+}
+
+template <class T>
 cudaError_t launch_back(const StepArgsT<T>& sa, const StepItem* items, int nitems, int nmax, int wmax,
                         cudaStream_t st) {
   if (nitems <= 0) return cudaSuccess;
@@ -1978,6 +2233,8 @@ cudaError_t launch_forward(const StepArgsT<T>& sa, const StepItem* items, int ni
 #define NPPB_STEP_INSTANTIATE(T)                                                                          \
   template cudaError_t launch_panel<T>(const StepArgsT<T>&, const int32_t*, int, int, int, cudaStream_t);     \
   template cudaError_t launch_update<T>(const StepArgsT<T>&, const StepItem*, int, int, int, cudaStream_t);   \
+  template cudaError_t launch_block_gemm<T>(const StepArgsT<T>&, int, int, int, int, int, cudaStream_t);    \
+  template cudaError_t launch_block_rows<T>(const StepArgsT<T>&, int, int, int, cudaStream_t);              \
   template cudaError_t launch_rows<T>(const StepArgsT<T>&, const StepItem*, int, int, cudaStream_t);          \
   template cudaError_t launch_trailing<T>(const StepArgsT<T>&, const StepItem*, int, int, int, int,          \
                                           cudaStream_t);                                                     \

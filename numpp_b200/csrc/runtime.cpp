@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -167,9 +168,21 @@ Lookahead* lookahead_for_device() {
 // order: its out-of-place update reads the panel's row-move lists, which the
 // next panel overwrites.
 template <class T>
+cudaError_t run_step_blocked(const StepArgsT<T>& sa0, int count, cudaStream_t st);
+
+int blocked_min_n() {
+  static const int v = [] {
+    const char* s = std::getenv("NPPB_BLOCKED_MIN_N");
+    return s ? std::atoi(s) : 0;  // off unless asked for: not yet faster than look-ahead at 1024..4096
+  }();
+  return v;
+}
+
+template <class T>
 cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st) {
   const int n = sa.un;
   if (n <= 32 || n > kStepMaxN || count <= 0) return cudaErrorInvalidValue;
+  if (sa.hist) return run_step_blocked(sa, count, st);
   Lookahead* la = lookahead_for_device();
   cudaError_t e = launch_panel(sa, nullptr, count, n, 0, st);
   for (int k0 = 0; k0 < n && e == cudaSuccess; k0 += kStepNB) {
@@ -200,6 +213,91 @@ cudaError_t run_step_uniform(const StepArgsT<T>& sa, int count, cudaStream_t st)
   if (back > INT32_MAX) return cudaErrorInvalidValue;
   return launch_back(sa, nullptr, (int)back, sa.un, sa.uinv ? 64 : std::min(64, sa.unrhs), st);
 }
+// Two-level factorisation (sa.hist set): outer blocks of kStepNBO columns.
+// The panels of a block update only the block's columns (all rows below),
+// the right-hand sides and the inverse, and carry their row moves left of the
+// panel inside the block; each records its row moves and L11^-1. Then every
+// strip right of the block gets the recorded row moves, U12 and the block
+// rows' updates (k_block_rows), and one DMMA GEMM with K = kStepNBO updates
+// everything below and right of the block: the trailing matrix is read and
+// written once per block instead of once per panel.
+//
+// Look-ahead across blocks: the GEMM's first kStepNBO columns (the next
+// block) run first; the next block's panels then go on a high-priority
+// stream while the rest of the GEMM runs on a side stream, and the next
+// trailing pass waits for it. Every element sees the same operations in the
+// same order either way.
+template <class T>
+cudaError_t run_step_blocked(const StepArgsT<T>& sa0, int count, cudaStream_t st) {
+  StepArgsT<T> sa = sa0;
+  const int n = sa.un;
+  cudaError_t e = cudaSuccess;
+  if (sa.A && sa.A != sa.LU) {  // in place from the start: the trailing pass reads the factor matrix
+    e = cudaMemcpyAsync(sa.LU, sa.A, sizeof(T) * (size_t)count * n * n, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+  }
+  sa.A = nullptr;
+  sa.utrail = 0;
+  sa.urow_end = 0;
+  // (not when factors are kept: their row moves reach the L columns the GEMM remainder reads)
+  Lookahead* la = sa.uleft ? nullptr : lookahead_for_device();
+  cudaStream_t cs = st;  // the chain of panels and block updates
+  if (la) {
+    e = cudaEventRecord(la->first, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(la->panel, la->first, 0);
+    if (e != cudaSuccess) return e;
+    cs = la->panel;
+  }
+  bool rest_pending = false;  // a GEMM remainder on the side stream
+  for (int K0 = 0; K0 < n && e == cudaSuccess; K0 += kStepNBO) {
+    const int bend = std::min(n, K0 + kStepNBO);
+    sa.ubbeg = K0;
+    sa.ubend = bend;
+    for (int k0 = K0; k0 < bend && e == cudaSuccess; k0 += kStepNB) {
+      sa.hslot = (k0 - K0) / kStepNB;
+      e = launch_panel(sa, nullptr, count, n - k0, k0, cs);
+      if (e != cudaSuccess) break;
+      const int64_t items =
+          (int64_t)count * blocked_update_strips(n, sa.unrhs, sa.uinv, k0, sa.uleft, K0, bend);
+      if (items > INT32_MAX) return cudaErrorInvalidValue;
+      if (items > 0) {
+        e = launch_rows(sa, nullptr, (int)items, k0, cs);
+        if (e == cudaSuccess && k0 + kStepNB < n) e = launch_trailing(sa, nullptr, (int)items, n, k0, 0, cs);
+      }
+    }
+    if (e != cudaSuccess || bend >= n) break;
+    if (rest_pending) {  // the previous block's GEMM remainder covers these columns
+      e = cudaStreamWaitEvent(cs, la->rest, 0);
+      rest_pending = false;
+      if (e != cudaSuccess) break;
+    }
+    e = launch_block_rows(sa, count, K0, bend, cs);
+    if (e != cudaSuccess) break;
+    const int split = std::min(n, bend + kStepNBO);
+    if (la && split < n) {
+      e = cudaEventRecord(la->next, cs);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(la->side, la->next, 0);
+      if (e == cudaSuccess) e = launch_block_gemm(sa, count, K0, bend, split, n, la->side);
+      if (e == cudaSuccess) e = cudaEventRecord(la->rest, la->side);
+      rest_pending = true;
+      if (e == cudaSuccess) e = launch_block_gemm(sa, count, K0, bend, bend, split, cs);
+    } else {
+      e = launch_block_gemm(sa, count, K0, bend, bend, n, cs);
+    }
+  }
+  if (rest_pending && e == cudaSuccess) e = cudaStreamWaitEvent(cs, la->rest, 0);
+  if (e != cudaSuccess) return e;
+  sa.ubbeg = sa.ubend = 0;
+  const int64_t back = (int64_t)count * uniform_back_strips(n, sa.unrhs, sa.uinv);
+  if (back > INT32_MAX) return cudaErrorInvalidValue;
+  e = launch_back(sa, nullptr, (int)back, sa.un, sa.uinv ? 64 : std::min(64, sa.unrhs), cs);
+  if (e == cudaSuccess && cs != st) {
+    e = cudaEventRecord(la->first, cs);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, la->first, 0);
+  }
+  return e;
+}
+
 template cudaError_t run_step_uniform<double>(const StepArgsT<double>&, int, cudaStream_t);
 template cudaError_t run_step_uniform<float>(const StepArgsT<float>&, int, cudaStream_t);
 
