@@ -55,6 +55,10 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the side measurements (mixed vs FP64, small batch, serving)")
     p.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per serving rate")
+    p.add_argument("--orders", type=int, nargs=2, metavar=("LO", "HI"), default=None,
+                   help="profiling aid: only the systems of the batch with LO <= n <= HI")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="profiling aid: keep the plan's chain count (NPPB_CHAINS) instead of tuning it")
     return p.parse_args()
 
 
@@ -436,6 +440,10 @@ def run_b200(args):
     assert L.nppb_device_available() == 1, _lib.last_error()
 
     sys_ = workloads.uneven_batch(seed=SEED + rank, count=args.count)
+    if args.orders:
+        keep = (sys_["n"] >= args.orders[0]) & (sys_["n"] <= args.orders[1])
+        sys_ = workloads.packed_batch(SEED + rank, sys_["n"][keep], sys_["nrhs"][keep],
+                                      (sys_["inv_off"] >= 0)[keep], shift=True)
     flags = _lib.WANT_SOLVE | _lib.WANT_SLOGDET | _lib.WANT_INV
     plan = Plan(sys_, flags)
     cnt = len(sys_["n"])
@@ -450,7 +458,10 @@ def run_b200(args):
     bufs = (dA, dB, dX, dInv, dDet, dSign, dLog, dInfo)
     stream = torch.cuda.Stream()
     # the plan's chain count, tuned on these buffers before anything is timed
-    chains, lookahead, _ = plan.autotune(*bufs, stream=stream)
+    if args.no_autotune:
+        chains, lookahead = None, None
+    else:
+        chains, lookahead, _ = plan.autotune(*bufs, stream=stream)
     nlaunch = plan.launches()
 
     def step():
@@ -560,7 +571,8 @@ def run_b200(args):
             "config": {"workload": WORKLOAD, "count": cnt, "parallelism": f"replicas{world}",
                        "l2": "inputs (%.2f GB of A) larger than L2; no flush" % (8 * plan.a_elems / 1e9),
                        "graph": True, "autotuned_chains": chains, "autotuned_lookahead": lookahead,
-                       "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls]},
+                       "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls],
+                       **({"orders_only": list(args.orders)} if args.orders else {})},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "gflops": flops_step * world / (ms_step * 1e-3) / 1e9,
             "max_backward_error_sample": worst,
