@@ -89,6 +89,16 @@ int nppb_gemm_batched(int64_t batch, int64_t m, int64_t n, int64_t k, const doub
  * batched GEMM, the batched inverse first when p < 0 (info[i] != 0: system i
  * is singular, its R is then undefined), the identity for p = 0. */
 int nppb_matrix_power_batched(int64_t count, int32_t n, int64_t p, const double* A, double* R, int32_t* info);
+/* cholesky over a (count, n, n) FP64 stack (src/linalg/linalg.cpp:117-136;
+ * stacks src/linalg/batched.cpp:77): lower-triangular L with A = L L^T, read
+ * from A's lower triangle only. info[i] = k > 0: system i is not positive
+ * definite (its k-th pivot is <= 0; the reference raises "Matrix is not
+ * positive definite"); L of that system is then undefined. Orders <= 4096. */
+int nppb_cholesky_batched(int64_t count, int32_t n, const double* A, double* L, int32_t* info);
+/* The same on device buffers, enqueued on `stream` (workspace allocated
+ * stream-ordered for the call). */
+int nppb_d_cholesky_batched(int64_t count, int32_t n, const double* dA, double* dL, int32_t* dinfo,
+                            void* stream);
 
 /* ---- uniform batches: count systems of order n (host buffers) ----------- */
 /* getrf: LU with partial pivoting in place (src/linalg/linalg.cpp:48-71),

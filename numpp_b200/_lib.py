@@ -65,6 +65,8 @@ SIGNATURES = {
     "nppb_d_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),
     "nppb_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp]),
     "nppb_matrix_power_batched": (_int, [_i64, _i32, _i64, _vp, _vp, _vp]),
+    "nppb_cholesky_batched": (_int, [_i64, _i32, _vp, _vp, _vp]),
+    "nppb_d_cholesky_batched": (_int, [_i64, _i32, _vp, _vp, _vp, _vp]),
     "nppb_dl_linalg": (_int, [_int] + [_vp] * 9),
     "nppb_dl_matmul": (_int, [_vp] * 4),
     "nppb_server_create": (_int, [C.POINTER(_vp), _i64, C.c_double, _i32]),

@@ -64,8 +64,10 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
 #pragma unroll 64
     for (int k = 0; k < NP; ++k) {
       if (k >= n || info) continue;
-      const bool cand = live && pos >= k;
-      double best = cand ? fabs(a[k]) : -1.0;
+      const bool nopiv = flags & kNoPivot;
+      const bool cand = live && (nopiv ? pos == k : pos >= k);
+      // without pivoting the diagonal is the only candidate; <= 0 counts as a zero pivot
+      double best = cand ? (nopiv ? (a[k] > 0.0 ? a[k] : 0.0) : fabs(a[k])) : -1.0;
       int key = cand ? pos : INT_MAX;
 #pragma unroll 64
       for (int off = 16; off; off >>= 1) {

@@ -146,16 +146,21 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // Pivot candidate of one column among this warp's rows: the first largest
 // |a| in position order over rows at or below position j (the reference's
-// rule, linalg.cpp:55-57), reduced over the warp. The thread holding it also
-// returns 1 / value in rp (the multiplier scale if it wins).
+// rule, linalg.cpp:55-57), reduced over the warp; without pivoting, the row at
+// position j. The thread holding it also returns 1 / value in rp (the
+// multiplier scale if it wins).
 template <class T, int RPT>
 __device__ __forceinline__ void column_candidate(const T (&v)[RPT], const int (&pos)[RPT], const bool (&valid)[RPT],
-                                                 int j, T& best, int& key, T& rp) {
+                                                 int j, T& best, int& key, T& rp, bool nopiv) {
   best = T(-1);
   key = INT_MAX;
 #pragma unroll
   for (int q = 0; q < RPT; ++q) {
-    if (valid[q] && pos[q] >= j) {
+    if (nopiv) {
+      // no row exchanges (the LU behind cholesky): the diagonal is the only
+      // candidate, and a value <= 0 counts as a zero pivot
+      if (valid[q] && pos[q] == j) { best = v[q] > T(0) ? v[q] : T(0); key = j; }
+    } else if (valid[q] && pos[q] >= j) {
       const T x = fabs(v[q]);
       if (x > best || (x == best && pos[q] < key)) { best = x; key = pos[q]; }
     }
@@ -264,7 +269,7 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
     T v[RPT];
 #pragma unroll
     for (int q = 0; q < RPT; ++q) v[q] = a[q][0];
-    column_candidate<T, RPT>(v, pos, valid, 0, nbest, nkey, nrp);
+    column_candidate<T, RPT>(v, pos, valid, 0, nbest, nkey, nrp, sa.unopiv != 0);
   }
 #pragma unroll
   for (int j = 0; j < NB; ++j) {
@@ -364,7 +369,7 @@ k_panel(StepArgsT<T> sa, const int32_t* __restrict__ list, int k0) {
             a[q][j + 1] = fma(-f[q], t, a[q][j + 1]);
             v[q] = a[q][j + 1];
           }
-          if (j + 1 < kb) column_candidate<T, RPT>(v, pos, valid, j + 1, nbest, nkey, nrp);
+          if (j + 1 < kb) column_candidate<T, RPT>(v, pos, valid, j + 1, nbest, nkey, nrp, sa.unopiv != 0);
 #pragma unroll
           for (int c2 = (j + 2) / 2; c2 < NB / 2; ++c2) {
             const P2 t2 = pr2[c2];

@@ -31,6 +31,8 @@ enum : int {
   kWantInv = 16,      // inverse (only systems with inv_off >= 0 in grouped mode)
   kInPlace = 32,      // A == LU: factor in place, skip the copy
   kSolveOnly = 64,    // getrs from existing LU + ipiv (no factorisation)
+  kNoPivot = 128,     // no row exchanges: the pivot is the diagonal, and a pivot <= 0
+                      // stops the system (the LU behind the Cholesky factor)
 };
 
 // A batch of systems. With desc == nullptr the batch is uniform: system s has

@@ -79,6 +79,7 @@ struct StepArgsT {
   // scratch slot s; an inverse for every system when uinv != 0.
   int un, unrhs, uinv;
   int uleft;         // uniform batch keeps its factors: carry row moves left of each panel
+  int unopiv;        // no row exchanges: pivot on the diagonal, a pivot <= 0 stops the system
   int umode;         // FP32 factors: trailing product in FP32 FMA (0), TF32 (1), BF16 (2), 3xTF32 (3) on mma.sync,
                      // or TF32 (4) / 3xTF32 (5) on tcgen05 with TMEM accumulators
   // Two-level factorisation of a uniform batch (ubend > 0): the panels of the

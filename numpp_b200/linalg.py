@@ -13,6 +13,8 @@ on numpy arrays:
   batched DMMA GEMM. The reference has no stacked matmul (backend.cpp:122
   rejects ndim != 2); this is the product its stacked ``matrix_power`` runs per
   matrix, offered as one call. Leading axes broadcast as in numpy.matmul.
+* ``cholesky(a)`` -- linalg.cpp:117-136, stacks batched.cpp:77: the lower
+  triangle of a is read, ``LinAlgError("Matrix is not positive definite")``.
 * ``matrix_power(a, n)`` -- linalg.cpp:440-454, stacks batched.cpp:83-84.
 * ``tensorsolve(a, b, axes)``, ``tensorinv(a, ind)`` -- tensor_solve.cpp:10-49.
 * ``cond(a, p)`` -- tensor.cpp:359-393 for p in {1, -1, inf, -inf, "fro"}:
@@ -109,6 +111,13 @@ class NativeBackend:
         _check(self.L.nppb_gemm(dt, m, n, k, _lib.ptr(A), _lib.ptr(B), _lib.ptr(Cm)))
         return Cm
 
+
+    def cholesky(self, A):
+        cnt, n = A.shape[0], A.shape[-1]
+        Lm = np.empty_like(A)
+        info = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_cholesky_batched(cnt, n, _lib.ptr(A), _lib.ptr(Lm), _lib.ptr(info)))
+        return Lm, info
 
     def gemm_batched(self, A, B):
         cnt, m, k = A.shape
@@ -388,3 +397,23 @@ def cond(a, p=None, backend=None):
     c = _matrix_norm(A3, p) * _matrix_norm(Ai, p)
     c = np.where(info != 0, np.inf, c)
     return c.reshape(lead) if lead else np.float64(c[0])
+
+
+def cholesky(a, backend=None):
+    """numpp::linalg::cholesky (linalg.cpp:117-136; stacks batched.cpp:77).
+
+    Lower-triangular L with a = L L^T, computed from a's lower triangle (the
+    upper one is never read). One matrix of a stack that is not positive
+    definite fails the whole call, as the reference loop does."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    out = _la_out(a.dtype)
+    if a.ndim < 2:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+    lead, cnt, n, A3 = _stack(a)
+    if cnt == 0 or n == 0:
+        return np.zeros(a.shape, out)
+    Lm, info = be.cholesky(A3)
+    if info.any():
+        raise LinAlgError("Matrix is not positive definite")
+    return Lm.reshape(a.shape).astype(out, copy=False)

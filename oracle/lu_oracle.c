@@ -226,3 +226,31 @@ void oracle_solve_grouped(int64_t count, const int* n, const int* nrhs, const in
     if (inv && inv_off[i] >= 0) oracle_inv(Ai, inv + inv_off[i], n[i]);
   }
 }
+
+/* src/linalg/linalg.cpp:117-136 (cholesky_impl<T>, real case): column by
+ * column, diag = A[j,j] - sum_p L[j,p]^2 (subtracting in p order), stop when
+ * diag <= 0 ("Matrix is not positive definite"); L[j,j] = sqrt(diag); below
+ * it L[i,j] = (A[i,j] - sum_p L[i,p] L[j,p]) / L[j,j]. Only the lower triangle
+ * of A is read. Returns 1, or 0 when A is not positive definite (L is then
+ * partly filled, as far as the reference got). */
+int oracle_cholesky(const double* A, double* L, int n) {
+  memset(L, 0, sizeof(double) * (size_t)n * n);
+  for (int j = 0; j < n; ++j) {
+    double sum = A[(int64_t)j * n + j];
+    for (int p = 0; p < j; ++p) sum -= L[(int64_t)j * n + p] * L[(int64_t)j * n + p];
+    if (sum <= 0.0) return 0;
+    const double ljj = sqrt(sum);
+    L[(int64_t)j * n + j] = ljj;
+    for (int i = j + 1; i < n; ++i) {
+      double s = A[(int64_t)i * n + j];
+      for (int p = 0; p < j; ++p) s -= L[(int64_t)i * n + p] * L[(int64_t)j * n + p];
+      L[(int64_t)i * n + j] = s / ljj;
+    }
+  }
+  return 1;
+}
+
+void oracle_cholesky_batched(int64_t count, int n, const double* A, double* L, int* ok) {
+  for (int64_t b = 0; b < count; ++b)
+    ok[b] = oracle_cholesky(A + b * (int64_t)n * n, L + b * (int64_t)n * n, n);
+}

@@ -50,6 +50,7 @@ class Oracle:
         L.oracle_inv_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _ip]
         L.oracle_det_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp]
         L.oracle_slogdet_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _dp]
+        L.oracle_cholesky_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _ip]
         L.oracle_solve_grouped.argtypes = [C.c_int64, _ip, _ip, _i64p, _i64p, _i64p,
                                            _dp, _dp, _dp, _dp, _dp, _dp, _ip]
         self.L = L
@@ -96,6 +97,15 @@ class Oracle:
         la = np.zeros(cnt)
         self.L.oracle_slogdet_batched(cnt, n, _ptr(A), _ptr(s), _ptr(la))
         return s, la
+
+    def cholesky(self, A):
+        """(count, n, n) stack -> (L, ok); ok[i] = 0 where matrix i is not positive definite."""
+        A = np.ascontiguousarray(A, np.float64)
+        cnt, n = A.shape[0], A.shape[-1]
+        Lm = np.zeros_like(A)
+        ok = np.zeros(cnt, np.intc)
+        self.L.oracle_cholesky_batched(cnt, n, _ptr(A), _ptr(Lm), _ptr(ok, _ip))
+        return Lm, ok
 
     def matmul(self, A, B):
         A = np.ascontiguousarray(A, np.float64)
@@ -169,6 +179,7 @@ class RefLib:
         L.ref_det.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_slogdet.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_matmul_cpu.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int, vp, vp, vp, cp, C.c_int]
+        L.ref_cholesky.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_matrix_power.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int64, vp, _ip, _i64p, cp,
                                        C.c_int]
         L.ref_tensorsolve.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int, _i64p, C.c_int, vp, C.c_int,
@@ -250,6 +261,9 @@ class RefLib:
         self._call(self.L.ref_matmul_cpu, A.shape[0], B.shape[1], A.shape[1], F64, A.ctypes.data,
                    B.ctypes.data, Cm.ctypes.data)
         return Cm
+
+    def cholesky(self, A):
+        return self._unary(self.L.ref_cholesky, A, A.shape)
 
     def matrix_power(self, A, p):
         A = np.ascontiguousarray(A)

@@ -1,7 +1,7 @@
 // REFERENCE SHIM — TEST INFRASTRUCTURE ONLY.
 //
 // extern "C" wrappers around the reference library's own public API
-// (numpp::linalg::solve/inv/det/slogdet/matrix_power/tensorsolve/tensorinv
+// (numpp::linalg::solve/inv/det/slogdet/cholesky/matrix_power/tensorsolve/tensorinv
 // and numpp::matmul), compiled together
 // with the reference's unmodified CPU sources into oracle/_ref/libnumpp_ref.so
 // by oracle/Makefile. Tests use it to pin the C oracle and to make golden
@@ -85,6 +85,12 @@ int ref_slogdet(int nda, const int64_t* sa, int dta, const void* A, void* sign, 
     put(r.sign, sign, o_dt, o_size);
     put(r.logabsdet, logabs, nullptr, nullptr);
   });
+}
+
+// cholesky (src/linalg/linalg.cpp:117-136; stacks batched.cpp:77).
+int ref_cholesky(int nda, const int64_t* sa, int dta, const void* A, void* out, int* o_dt, int64_t* o_size,
+                 char* err, int errlen) {
+  return guard(err, errlen, [&] { put(numpp::linalg::cholesky(make(nda, sa, dta, A)), out, o_dt, o_size); });
 }
 
 // matrix_power (src/linalg/linalg.cpp:440-454; stacks batched.cpp:83-84).

@@ -15,6 +15,8 @@ NumPP's tests and on small seeded workloads, and stores inputs + outputs:
 * tests/test_linalg_mined3.cpp:29-40             matrix_power of [[1,2],[3,4]] for 0, 1, 2, 7, -1, -3
 * tests/test_tensor_solve.cpp:9-71                tensorsolve / tensorinv of the (2,2,2,2) tridiagonal
 * a seeded (6, 9, 9) stack to the powers 3, 8, -2, -4 (src/linalg/batched.cpp:83-84)
+* tests/test_linalg.cpp:61-69, tests/test_batched_linalg.cpp:53-58   cholesky of the 3x3 SPD
+  matrix, of the (2,2,2) stack, the not-positive-definite error, and a seeded (5, 40, 40) stack
 
 Usage: python tests/golden/make_golden.py   (needs oracle/_ref; run where it was built)
 """
@@ -117,6 +119,15 @@ def main():
     g["mp9_A"] = Ms
     for p in (3, 8, -2, -4):
         g[f"mp9_p{p}"] = r.matrix_power(Ms, p)
+
+    g["chol_spd3"] = r.cholesky(M)
+    S2 = np.array([[[2.0, 0], [0, 3]], [[4, 1], [1, 3]]])
+    g["chol_stack_A"], g["chol_stack_L"] = S2, r.cholesky(S2)
+    g["chol_notpd_err"] = np.array(err_of(r.cholesky, np.array([[-1.0, 0], [0, -1]])))
+    Xc = np.random.default_rng(77).standard_normal((5, 40, 40))
+    Ac = Xc @ Xc.transpose(0, 2, 1) + 40 * np.eye(40)
+    Ac[:, 0, 39] = 7.0  # the upper triangle is never read
+    g["chol40_A"], g["chol40_L"] = Ac, r.cholesky(Ac)
 
     T = np.array([4.0, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4]).reshape(2, 2, 2, 2)
     bt = np.array([1.0, 2, 3, 4]).reshape(2, 2)

@@ -39,6 +39,11 @@ class OracleBackend:
         self.calls.append(("gemm_batched", A.shape, B.shape))
         return np.stack([self.o.matmul(A[i], B[i]) for i in range(A.shape[0])])
 
+    def cholesky(self, A):
+        self.calls.append(("cholesky", A.shape))
+        Lm, ok = self.o.cholesky(A)
+        return Lm, (ok == 0).astype(np.int32)
+
     def matrix_power(self, A, p):
         self.calls.append(("matrix_power", A.shape, p))
         R, ok = self.o.matrix_power(A, p)
@@ -229,3 +234,19 @@ def test_device_mirror_declines_host_tensors():
         dev.inv(np.eye(3))
     with pytest.raises(TypeError):
         dev.inv([[1.0, 0.0], [0.0, 1.0]])
+
+
+def test_cholesky(golden, be):
+    """linalg.cpp:117-136 through the mirror, against the reference's outputs."""
+    assert np.array_equal(la.cholesky(golden["spd3_A"], backend=be), golden["chol_spd3"])
+    assert np.array_equal(la.cholesky(golden["chol_stack_A"], backend=be), golden["chol_stack_L"])
+    assert np.array_equal(la.cholesky(golden["chol40_A"], backend=be), golden["chol40_L"])
+    with pytest.raises(la.LinAlgError, match=str(golden["chol_notpd_err"])):
+        la.cholesky(np.array([[-1.0, 0], [0, -1]]), backend=be)
+    with pytest.raises(la.LinAlgError, match="square"):
+        la.cholesky(np.ones((2, 3)), backend=be)
+    assert la.cholesky(np.eye(3, dtype=np.float32), backend=be).dtype == np.float32
+    assert la.cholesky(np.zeros((0, 5, 5)), backend=be).shape == (0, 5, 5)
+    be.calls.clear()
+    la.cholesky(np.stack([np.eye(4)] * 6).reshape(2, 3, 4, 4), backend=be)
+    assert be.calls == [("cholesky", (6, 4, 4))]

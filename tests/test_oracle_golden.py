@@ -151,3 +151,16 @@ def test_tensor_solve_known_answers(golden, oracle):
     inv, _ = oracle.inv(golden["tens4_A"].reshape(1, 24, 24))
     assert bits_equal(inv.reshape(8, 3, 4, 6), golden["tens4_inv"])
     assert str(golden["tensinv_ind0_err"]) == "Invalid ind argument"
+
+
+def test_cholesky_known_answers(golden, oracle):
+    """test_linalg.cpp:61-69 and test_batched_linalg.cpp:53-58 plus a seeded
+    stack: the restatement of linalg.cpp:117-136 is bit-exact with the reference."""
+    L, ok = oracle.cholesky(golden["spd3_A"][None])
+    assert ok.all() and bits_equal(L[0], golden["chol_spd3"])
+    L, ok = oracle.cholesky(golden["chol_stack_A"])
+    assert ok.all() and bits_equal(L, golden["chol_stack_L"])
+    L, ok = oracle.cholesky(golden["chol40_A"])
+    assert ok.all() and bits_equal(L, golden["chol40_L"])
+    _, ok = oracle.cholesky(np.array([[[-1.0, 0], [0, -1]]]))
+    assert ok[0] == 0 and str(golden["chol_notpd_err"]) == "Matrix is not positive definite"
