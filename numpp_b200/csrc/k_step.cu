@@ -937,9 +937,12 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
 
 // ---------------------------------------------------------------------------
 // k_update: A22 -= L21 U12 on one strip, rows [k0+32 + RG*blockIdx.y, +RG), in
-// 64-row tiles, software-pipelined: while tile t is multiplied, tile t+1's L21
-// rows stream into shared memory (cp.async, 16-byte pieces when aligned) and
-// its accumulator inputs into registers (paired loads when aligned).
+// 64-row tiles: while tile t is multiplied, tile t+1's L21 rows stream into
+// shared memory (cp.async, 16-byte pieces when aligned); each tile's
+// accumulator inputs are read when the tile starts (paired loads when
+// aligned). At 128 registers four CTAs fit on an SM and hide those reads from
+// one another (measured faster than prefetching them into a second register
+// tile at three CTAs per SM).
 constexpr int RG = 512;
 constexpr int RG1 = 128;  // rows per CTA of the look-ahead strip (part 1): short critical path
 
@@ -1010,7 +1013,7 @@ __device__ __forceinline__ bool pair_aligned(const T* p, int64_t ld) {
 }
 
 template <class T, int MODE>
-__global__ void __launch_bounds__(UT, 3)
+__global__ void __launch_bounds__(UT, 4)
 k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) {
   using P2 = typename Pair<T>::type;
   using Acc = typename AccSel<T, MODE>::type;
@@ -1080,15 +1083,14 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) 
       }
     });
   };
-  Acc cur, nxt;
+  Acc cur;
   prefetch_a(As0, rb);
-  load_c(cur, rb);
   bool b1 = false;
   for (int r0 = rb; r0 < re; r0 += 64) {
     const bool more = r0 + 64 < re;
+    load_c(cur, r0);
     if (more) {
       prefetch_a(b1 ? As0 : As1, r0 + 64);
-      load_c(nxt, r0 + 64);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -1107,7 +1109,6 @@ k_update(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0, int part) 
         }
       }
     });
-    if (more) cur = nxt;
     b1 = !b1;
     __syncthreads();  // the buffer just read is refilled by the next iteration's prefetch
   }
