@@ -907,26 +907,35 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     dsrc[tid] = tid < nd ? (hs ? hs->disp_src[hsl][tid] : sc->disp_src[tid]) : 0;
   }
   __syncthreads();
-  for (int idx = tid; idx < NB * 64; idx += UT) {
-    const int i = idx >> 6, c = idx & 63;
+  // fixed trip counts, fully unrolled: every load of the gather is in flight at once
+#pragma unroll
+  for (int it = 0; it < NB * 64 / UT; ++it) {
+    const int idx = tid + it * UT, i = idx >> 6, c = idx & 63;
     const bool in = c < w;
     Tm[i * WS + c] = (in && i < kb) ? seg_load(s, k0 + tsrc[i], c0 + c) : T(0);
     D[i * WS + c] = (in && i < nd) ? seg_load(s, k0 + dsrc[i], c0 + c) : T(0);
   }
   __syncthreads();
-  for (int idx = tid; idx < NB * 64; idx += UT) {
-    const int i = idx >> 6, c = idx & 63;
+#pragma unroll
+  for (int it = 0; it < NB * 64 / UT; ++it) {
+    const int idx = tid + it * UT, i = idx >> 6, c = idx & 63;
     if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
   }
   if (it.kind == kSegLeft || mv == 1) {
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       if (c < w && i < kb) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = Tm[i * WS + c];
     }
     return;
   }
   const T* linv = hs ? hs->linv[hsl] : sc->linv;
-  for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+#pragma unroll
+  for (int it_ = 0; it_ < NB * NB / UT; ++it_) {
+    const int idx = tid + it_ * UT;
+    Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+  }
   __syncthreads();
   Acc32<T> u;
   u.mma(Li, Tm);
@@ -1269,7 +1278,9 @@ k_update_tc(StepArgsT<float> sa, const StepItem* __restrict__ items, int k0, int
     cp_async_commit();
   };
   // U12^T (64 x 32, K-major) from the strip's top rows, split for 3xTF32
-  for (int idx = tid; idx < 64 * NB; idx += UT) {
+#pragma unroll
+  for (int it_ = 0; it_ < 64 * NB / UT; ++it_) {
+    const int idx = tid + it_ * UT;
     const int c = idx >> 5, q = idx & 31;  // column of the strip, row of U12
     const float u = c < w ? dst[(int64_t)(k0 + q) * ld + c] : 0.f;
     if constexpr (SPLIT) {
@@ -1457,11 +1468,15 @@ __device__ __forceinline__ void window_solve(const T* __restrict__ M, int n, T* 
   for (int bi = 0; bi < nblk; ++bi) {
     const int kb0 = UPPER ? lo + (nblk - 1 - bi) * NB : lo + bi * NB;
     const int bw = min(NB, hi - kb0);
-    for (int idx = tid; idx < NB * NB; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * NB / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 5, q = idx & 31;
       Db[i * LS + q] = (i < bw && q < bw) ? M[(int64_t)(kb0 + i) * n + kb0 + q] : (i == q ? T(1) : T(0));
     }
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       Xb[i * WS + c] = (i < bw && c < w) ? X[(int64_t)(kb0 + i) * ld + c0 + c] : T(0);
     }
@@ -1515,14 +1530,18 @@ __device__ __forceinline__ void window_solve(const T* __restrict__ M, int n, T* 
       }
     }
     __syncthreads();
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       if (i < bw && c < w) X[(int64_t)(kb0 + i) * ld + c0 + c] = Xb[i * WS + c];
     }
     // the rest of the window: above the block (UPPER) or below it
     const int r_lo = UPPER ? lo : kb0 + bw, r_hi = UPPER ? kb0 : hi;
     for (int r0 = r_lo; r0 < r_hi; r0 += 64) {
-      for (int idx = tid; idx < 64 * NB; idx += UT) {
+#pragma unroll
+      for (int it_ = 0; it_ < 64 * NB / UT; ++it_) {
+        const int idx = tid + it_ * UT;
         const int i = idx >> 5, q = idx & 31;
         As[i * LS + q] = (r0 + i < r_hi && q < bw) ? M[(int64_t)(r0 + i) * n + kb0 + q] : T(0);
       }
@@ -1619,11 +1638,15 @@ __device__ __forceinline__ void window_apply(const T* __restrict__ M, int n, T* 
   acc.each([&](int r, int cc, T& x) { x = (r0 + r < rend && cc < w) ? X[(int64_t)(r0 + r) * ld + c0 + cc] : T(0); });
   for (int kc = lo; kc < hi; kc += NB) {
     const int kw = min(NB, hi - kc);
-    for (int idx = tid; idx < 64 * NB; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < 64 * NB / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 5, q = idx & 31;
       As[i * LS + q] = (r0 + i < rend && q < kw) ? M[(int64_t)(r0 + i) * n + kc + q] : T(0);
     }
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       Bs[i * WS + c] = (i < kw && c < w) ? X[(int64_t)(kc + i) * ld + c0 + c] : T(0);
     }
@@ -1893,14 +1916,18 @@ k_block_rows(StepArgsT<T> sa, int bbeg, int bend) {
     __syncthreads();
     T* Tm = X;
     T* D = X + NB * WS;
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       const bool in = c < w;
       Tm[i * WS + c] = (in && i < kb) ? F[(int64_t)(k0 + tsrc[i]) * ld + c] : T(0);
       D[i * WS + c] = (in && i < nd) ? F[(int64_t)(k0 + dsrc[i]) * ld + c] : T(0);
     }
     __syncthreads();
-    for (int idx = tid; idx < NB * 64; idx += UT) {
+#pragma unroll
+    for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
+      const int idx = tid + it_ * UT;
       const int i = idx >> 6, c = idx & 63;
       if (c < w && i < nd) F[(int64_t)(k0 + ddst[i]) * ld + c] = D[i * WS + c];
       if (c < w && i < kb) F[(int64_t)(k0 + i) * ld + c] = Tm[i * WS + c];
@@ -1916,7 +1943,11 @@ k_block_rows(StepArgsT<T> sa, int bbeg, int bend) {
   for (int s = 0; s * NB < bw; ++s) {
     const int k0 = bbeg + s * NB;
     const T* linv = hs->linv[s];
-    for (int idx = tid; idx < NB * NB; idx += UT) Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+#pragma unroll
+    for (int it_ = 0; it_ < NB * NB / UT; ++it_) {
+      const int idx = tid + it_ * UT;
+      Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+    }
     __syncthreads();
     T* Xs = X + s * NB * WS;
     {
@@ -1928,7 +1959,9 @@ k_block_rows(StepArgsT<T> sa, int bbeg, int bend) {
     for (int r0 = (s + 1) * NB; r0 < bw; r0 += 64) {
       const int rows = min(64, bw - r0);
       __syncthreads();
-      for (int idx = tid; idx < 64 * NB; idx += UT) {
+#pragma unroll
+      for (int it_ = 0; it_ < 64 * NB / UT; ++it_) {
+        const int idx = tid + it_ * UT;
         const int i = idx >> 5, c = idx & 31;
         Lt[i * LS + c] = i < rows ? sa.LU[d.lu_off + (int64_t)(bbeg + r0 + i) * ld + k0 + c] : T(0);
       }
