@@ -125,6 +125,27 @@ def uneven_bytes(sys: dict) -> float:
     return float(8 * nn.sum() + 16 * nb.sum() + 8 * nn[inv].sum() + 20 * len(nn))
 
 
+def step_update_bytes(sys: dict, nb: int = 32) -> float:
+    """Algorithmic DRAM bytes of the step-wise trailing updates (row moves + U12
+    and A22 -= L21 U12) of one uneven batch, FP64: at each 32-column step of a
+    system of order n > 32, every trailing element (matrix columns right of the
+    panel, right-hand sides, inverse columns) below the panel is read and
+    written once (16 B), L21 is read once per 64-column strip (8 B x 32 per
+    row), and the 32 panel rows of those columns are read and written by the
+    row-move / U12 pass (16 B each). Orders <= 32 take the warp kernel."""
+    total = 0.0
+    for n, k, inv in zip(sys["n"].astype(np.int64), sys["nrhs"].astype(np.int64), sys["inv_off"] >= 0):
+        if n <= nb:
+            continue
+        for k0 in range(0, n, nb):
+            below = n - k0 - nb
+            width = max(below, 0) + k + (n if inv else 0)
+            if below > 0:
+                total += 16.0 * below * width + 8.0 * below * nb * ((width + 63) // 64)
+            total += 16.0 * min(nb, n - k0) * width
+    return total
+
+
 def conditioned_batch(seed: int, count: int, n: int, kappa: float, nrhs: int = 1,
                       row_scale_decades: float = 0.0):
     """A = Q1 diag(sigma) Q2^T with Q from the QR of N(0,1) matrices and sigma
