@@ -906,6 +906,15 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     ddst[tid] = tid < nd ? (hs ? hs->disp_dst[hsl][tid] : sc->disp_dst[tid]) : 0;
     dsrc[tid] = tid < nd ? (hs ? hs->disp_src[hsl][tid] : sc->disp_src[tid]) : 0;
   }
+  const bool u12 = !(it.kind == kSegLeft || mv == 1);  // else row moves only
+  if (u12) {  // L11^-1 comes in together with the move lists (one round trip fewer)
+    const T* linv = hs ? hs->linv[hsl] : sc->linv;
+#pragma unroll
+    for (int it_ = 0; it_ < NB * NB / UT; ++it_) {
+      const int idx = tid + it_ * UT;
+      Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
+    }
+  }
   __syncthreads();
   // fixed trip counts, fully unrolled: every load of the gather is in flight at once
 #pragma unroll
@@ -921,7 +930,7 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     const int idx = tid + it * UT, i = idx >> 6, c = idx & 63;
     if (c < w && i < nd) s.dst[(int64_t)(k0 + ddst[i]) * s.ld + c0 + c] = D[i * WS + c];
   }
-  if (it.kind == kSegLeft || mv == 1) {
+  if (!u12) {
 #pragma unroll
     for (int it_ = 0; it_ < NB * 64 / UT; ++it_) {
       const int idx = tid + it_ * UT;
@@ -930,14 +939,7 @@ k_rows(StepArgsT<T> sa, const StepItem* __restrict__ items, int k0) {
     }
     return;
   }
-  const T* linv = hs ? hs->linv[hsl] : sc->linv;
-#pragma unroll
-  for (int it_ = 0; it_ < NB * NB / UT; ++it_) {
-    const int idx = tid + it_ * UT;
-    Li[(idx >> 5) * LS + (idx & 31)] = linv[idx];
-  }
-  __syncthreads();
-  Acc32<T> u;
+  Acc32<T> u;  // Tm and Li are complete since the barrier after the gather
   u.mma(Li, Tm);
   u.each([&](int i, int c, T& x) {
     if (i < kb && c < w) s.dst[(int64_t)(k0 + i) * s.ld + c0 + c] = x;
