@@ -65,6 +65,11 @@ typedef struct {
 int nppb_dl_linalg(int flags, const DLTensor* a, const DLTensor* b, DLTensor* x, DLTensor* inv, DLTensor* det,
                    DLTensor* sign, DLTensor* logabs, DLTensor* info, void* stream);
 
+/* cholesky of a (..., n, n) stack (src/linalg/linalg.cpp:117-136): l gets
+ * a's shape, info the lead shape (int32; > 0: not positive definite). Only
+ * the lower triangle of a is read. info is required. */
+int nppb_dl_cholesky(const DLTensor* a, DLTensor* l, DLTensor* info, void* stream);
+
 /* c = a @ b over a stack: a lead + (m, k), b lead + (k, n), c lead + (m, n),
  * the same lead on all three (src/backend/backend.cpp:121-177 for one matrix). */
 int nppb_dl_matmul(const DLTensor* a, const DLTensor* b, DLTensor* c, void* stream);

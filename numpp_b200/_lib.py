@@ -69,6 +69,7 @@ SIGNATURES = {
     "nppb_d_cholesky_batched": (_int, [_i64, _i32, _vp, _vp, _vp, _vp]),
     "nppb_dl_linalg": (_int, [_int] + [_vp] * 9),
     "nppb_dl_matmul": (_int, [_vp] * 4),
+    "nppb_dl_cholesky": (_int, [_vp] * 4),
     "nppb_server_create": (_int, [C.POINTER(_vp), _i64, C.c_double, _i32]),
     "nppb_server_submit": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _i64, _i32, C.POINTER(_i64), C.POINTER(_i64)]),
     "nppb_server_wait": (_int, [_vp, _i64, C.c_double, C.POINTER(_i32), C.POINTER(C.c_double)]),

@@ -192,9 +192,39 @@ int dl_matmul(const DLTensor* a, const DLTensor* b, DLTensor* c, cudaStream_t st
                              reinterpret_cast<const double*>(B.ptr), reinterpret_cast<double*>(Cv.ptr), st);
 }
 
+int dl_cholesky(const DLTensor* a, DLTensor* l, DLTensor* info, cudaStream_t st) {
+  View A, Lv, I;
+  NPPB_RC(view_of(a, Kind::F64, "a", A));
+  const int nd = static_cast<int>(A.shape.size());
+  if (nd < 2 || A.shape[nd - 1] != A.shape[nd - 2])
+    return fail(NPPB_E_ARG, "a: last 2 dimensions of the array must be square, got " + shape_str(A.shape));
+  NPPB_RC(view_of(l, Kind::F64, "l", Lv));
+  if (!same(Lv.shape, A.shape)) return fail(NPPB_E_ARG, "l: must have a's shape " + shape_str(A.shape));
+  NPPB_RC(view_of(info, Kind::I32, "info", I));
+  const std::vector<int64_t> lead(A.shape.begin(), A.shape.end() - 2);
+  if (!same(I.shape, lead)) return fail(NPPB_E_ARG, "info: must have shape " + shape_str(lead));
+  const int64_t n = A.shape[nd - 1];
+  int64_t count = 1;
+  for (int64_t s : lead) count *= s;
+  if (n > INT32_MAX) return fail(NPPB_E_RANGE, "order above 2^31-1");
+  return nppb_d_cholesky_batched(count, static_cast<int32_t>(n), reinterpret_cast<const double*>(A.ptr),
+                                 reinterpret_cast<double*>(Lv.ptr), reinterpret_cast<int32_t*>(I.ptr), st);
+}
+
 }  // namespace
 
 extern "C" {
+
+int nppb_dl_cholesky(const DLTensor* a, DLTensor* l, DLTensor* info, void* stream) {
+  try {
+    clear_error();
+    return dl_cholesky(a, l, info, static_cast<cudaStream_t>(stream));
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return NPPB_E_NOMEM;
+  }
+}
+
 
 int nppb_dl_linalg(int flags, const DLTensor* a, const DLTensor* b, DLTensor* x, DLTensor* inv, DLTensor* det,
                    DLTensor* sign, DLTensor* logabs, DLTensor* info, void* stream) {

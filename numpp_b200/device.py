@@ -1,10 +1,11 @@
 """The linalg mirror on device-resident stacks, handed over through DLPack.
 
-``solve``, ``inv``, ``det``, ``slogdet`` and ``matmul_batched`` take any tensor
+``solve``, ``inv``, ``det``, ``slogdet``, ``cholesky`` and ``matmul_batched`` take any tensor
 that speaks the DLPack protocol (``__dlpack__`` / ``__dlpack_device__``) and
 lives on the current CUDA device -- a torch tensor, a CuPy array, ... -- and
 return torch tensors on the same device. The stacks never visit the host: the
-DLTensor descriptors go straight to ``nppb_dl_linalg`` / ``nppb_dl_matmul``
+DLTensor descriptors go straight to ``nppb_dl_linalg`` / ``nppb_dl_cholesky`` /
+``nppb_dl_matmul``
 (include/numpp_b200_dlpack.h), which enqueue on torch's current stream.
 
 Semantics follow numpp_b200.linalg (NumPP's front-end, linalg.cpp:366-439 and
@@ -183,3 +184,27 @@ def matmul_batched(a, b):
     with torch.cuda.device(A.device):
         _check(_lib.load().nppb_dl_matmul(h.ptr(A), h.ptr(B), h.ptr(Cm), stream))
     return Cm.to(_out_dtype(a, b))
+
+
+def cholesky(a, check=True):
+    """Lower-triangular L with a = L L^T on the device (linalg.cpp:117-136; stacks
+    batched.cpp:77), from a's lower triangle. ``LinAlgError("Matrix is not
+    positive definite")`` if any matrix of the stack is not; ``check=False``
+    returns ``(L, info)`` with nothing synchronised."""
+    torch = _torch()
+    a = _as_torch(a)
+    if a.dim() < 2 or a.shape[-1] != a.shape[-2]:
+        raise LinAlgError("Last 2 dimensions of the array must be square")
+    stream = torch.cuda.current_stream(a.device).cuda_stream
+    A = _f64(a)
+    Lm = torch.empty_like(A)
+    info = torch.zeros(tuple(A.shape[:-2]), dtype=torch.int32, device=A.device)
+    h = _Handoff(stream)
+    with torch.cuda.device(A.device):
+        _check(_lib.load().nppb_dl_cholesky(h.ptr(A), h.ptr(Lm), h.ptr(info), stream))
+    Lm = Lm.to(_out_dtype(a))
+    if not check:
+        return Lm, info
+    if bool(info.any()):
+        raise LinAlgError("Matrix is not positive definite")
+    return Lm

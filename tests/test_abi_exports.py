@@ -25,7 +25,8 @@ def test_header_declares_the_path():
     names = declared()
     for must in ("nppb_gemm", "nppb_solve_batched", "nppb_inv_batched", "nppb_det_batched",
                  "nppb_slogdet_batched", "nppb_getrf_batched", "nppb_getrs_batched",
-                 "nppb_plan_create", "nppb_plan_execute", "nppb_dl_linalg", "nppb_dl_matmul"):
+                 "nppb_plan_create", "nppb_plan_execute", "nppb_dl_linalg", "nppb_dl_matmul",
+                 "nppb_dl_cholesky", "nppb_cholesky_batched"):
         assert must in names
 
 

@@ -123,3 +123,19 @@ def test_abi_checks_each_tensor(lib):
     torch.cuda.synchronize()
     np.testing.assert_allclose(x.cpu().numpy(), A.cpu().numpy() @ b.cpu().numpy(), rtol=1e-13)
     assert lib.nppb_dl_matmul(h.ptr(A), h.ptr(A), h.ptr(x), st) == _lib.E_ARG
+
+
+def test_cholesky_on_device(lib, oracle):
+    rng = np.random.default_rng(9)
+    X = rng.standard_normal((2, 3, 70, 70))
+    A = X @ X.transpose(0, 1, 3, 2) / 70 + np.eye(70)
+    Lt = dev.cholesky(Foreign(torch.from_numpy(A).cuda()))
+    assert Lt.is_cuda and tuple(Lt.shape) == (2, 3, 70, 70)
+    Lo, ok = oracle.cholesky(A.reshape(6, 70, 70))
+    assert ok.all()
+    np.testing.assert_allclose(Lt.cpu().numpy().reshape(6, 70, 70), Lo, rtol=1e-11, atol=1e-13)
+    bad = torch.from_numpy(-np.eye(5)[None].repeat(2, 0)).cuda()
+    with pytest.raises(la.LinAlgError, match="positive definite"):
+        dev.cholesky(bad)
+    _, info = dev.cholesky(bad, check=False)
+    assert bool((info > 0).all())
