@@ -250,3 +250,15 @@ def test_cholesky(golden, be):
     be.calls.clear()
     la.cholesky(np.stack([np.eye(4)] * 6).reshape(2, 3, 4, 4), backend=be)
     assert be.calls == [("cholesky", (6, 4, 4))]
+
+
+def test_step_update_bytes_counts():
+    """The algorithmic-bytes model behind the bench's HBM roofline of the
+    trailing update, on one system counted by hand."""
+    from numpp_b200 import workloads
+    sys_ = {"n": np.array([64, 20]), "nrhs": np.array([1, 3]), "inv_off": np.array([-1, 0])}
+    # n = 64, one right-hand side, no inverse: step 0 has 32 rows below and
+    # 32 + 1 trailing columns (one strip), step 32 only the row-move pass on 1 column;
+    # the order-20 system takes the warp kernel and adds nothing
+    want = (16 * 32 * 33 + 8 * 32 * 32 * 1 + 16 * 32 * 33) + (16 * 32 * 1)
+    assert workloads.step_update_bytes(sys_) == want
