@@ -69,3 +69,25 @@ def test_argument_errors_before_device_work():
     assert L.nppb_gemm(5, 2, 2, 2, None, None, None) == _lib.DECLINED  # int64 gemm: CPU path
     h = C.c_void_p()
     assert L.nppb_plan_create(C.byref(h), -3, None, None, None, None, None, 2) == _lib.E_ARG
+
+
+def test_argument_errors_before_any_device_work():
+    """Bad sizes are refused with an error status and a message, whether or
+    not a device is present (the checks come before the device probe)."""
+    L = _lib.load()
+    z = np.zeros(4)
+    cases = [
+        (L.nppb_gemm_batched, (-1, 2, 2, 2, z.ctypes.data, z.ctypes.data, z.ctypes.data), _lib.E_ARG),
+        (L.nppb_d_gemm_batched, (1, -2, 2, 2, None, None, None, None), _lib.E_ARG),
+        (L.nppb_matrix_power_batched, (-1, 2, 3, z.ctypes.data, z.ctypes.data, None), _lib.E_ARG),
+        (L.nppb_cholesky_batched, (1, 5000, z.ctypes.data, z.ctypes.data, z.ctypes.data), _lib.E_RANGE),
+        (L.nppb_d_cholesky_batched, (-3, 4, None, None, None, None), _lib.E_ARG),
+        (L.nppb_solve_batched, (1, 5000, 1, z.ctypes.data, z.ctypes.data, z.ctypes.data, z.ctypes.data),
+         _lib.E_RANGE),
+    ]
+    for fn, args, want in cases:
+        assert fn(*args) == want, fn.__name__
+        assert _lib.last_error()
+    # nothing to do is not an error
+    assert L.nppb_cholesky_batched(0, 4, None, None, None) == _lib.OK
+    assert L.nppb_gemm_batched(0, 2, 2, 2, None, None, None) == _lib.OK
