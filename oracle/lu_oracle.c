@@ -254,3 +254,136 @@ void oracle_cholesky_batched(int64_t count, int n, const double* A, double* L, i
   for (int64_t b = 0; b < count; ++b)
     ok[b] = oracle_cholesky(A + b * (int64_t)n * n, L + b * (int64_t)n * n, n);
 }
+
+/* src/linalg/linalg.cpp:620-712 (svd_jacobi<T>, real case, economy size) and
+ * :755-784 (lstsq). Cyclic one-sided Jacobi on the tall orientation (A, or
+ * A^T when m < n): for every column pair in order, the squared norms and the
+ * dot product (sums in row order), a sign flip of column j making the dot
+ * product positive, then the rotation with zeta = (bb - aa) / (2|c|); at most
+ * 60 sweeps, stopping once the largest |c| / sqrt(aa bb) is below 1e-15.
+ * Singular values are the column norms, sorted descending (stable here; the
+ * reference's std::sort orders equal values arbitrarily). lstsq: tol = (rcond
+ * < 0 ? eps * max(m, n) : rcond) * s_max, rank = #{s > tol}, x = V diag(1/s or
+ * 0) U^T b with both products accumulated in p order (cpu_matmul). The
+ * residuals (m > n and full rank) are sum_i (b - A x)_ij^2 per column j.
+ * B is m x k row-major, X n x k. Returns 1 when residuals were formed. */
+static void matmul_p(const double* A, const double* B, double* C, int m, int kdim, int n) {
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < n; ++j) C[(int64_t)i * n + j] = 0.0;
+  for (int i = 0; i < m; ++i)
+    for (int p = 0; p < kdim; ++p) {
+      const double a = A[(int64_t)i * kdim + p];
+      for (int j = 0; j < n; ++j) C[(int64_t)i * n + j] += a * B[(int64_t)p * n + j];
+    }
+}
+
+int oracle_lstsq(const double* A, int m, int n, const double* B, int k, double rcond, double* X, double* s,
+                 int* rank, double* resid) {
+  const int kk = m < n ? m : n, wide = m < n, M = wide ? n : m, N = wide ? m : n;
+  double* W = (double*)malloc(sizeof(double) * (size_t)M * N);
+  double* V = (double*)calloc((size_t)N * N, sizeof(double));
+  for (int i = 0; i < M; ++i)
+    for (int j = 0; j < N; ++j) W[(int64_t)i * N + j] = wide ? A[(int64_t)j * n + i] : A[(int64_t)i * n + j];
+  for (int i = 0; i < N; ++i) V[(int64_t)i * N + i] = 1.0;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double maxoff = 0.0;
+    for (int i = 0; i < N; ++i)
+      for (int j = i + 1; j < N; ++j) {
+        double aa = 0, bb = 0, cc = 0;
+        for (int r = 0; r < M; ++r) {
+          const double xi = W[(int64_t)r * N + i], xj = W[(int64_t)r * N + j];
+          aa += fabs(xi) * fabs(xi);
+          bb += fabs(xj) * fabs(xj);
+          cc += xi * xj;
+        }
+        if (aa == 0.0 || bb == 0.0) continue;
+        const double magc = fabs(cc), off = magc / sqrt(aa * bb);
+        if (off > maxoff) maxoff = off;
+        if (off < 1e-300) continue;
+        const double w = cc / magc;
+        for (int r = 0; r < M; ++r) W[(int64_t)r * N + j] = W[(int64_t)r * N + j] * w;
+        for (int r = 0; r < N; ++r) V[(int64_t)r * N + j] = V[(int64_t)r * N + j] * w;
+        const double zeta = (bb - aa) / (2.0 * magc);
+        const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        const double cs = 1.0 / sqrt(1.0 + t * t), sn = cs * t;
+        for (int r = 0; r < M; ++r) {
+          const double xi = W[(int64_t)r * N + i], xj = W[(int64_t)r * N + j];
+          W[(int64_t)r * N + i] = cs * xi - sn * xj;
+          W[(int64_t)r * N + j] = sn * xi + cs * xj;
+        }
+        for (int r = 0; r < N; ++r) {
+          const double vi = V[(int64_t)r * N + i], vj = V[(int64_t)r * N + j];
+          V[(int64_t)r * N + i] = cs * vi - sn * vj;
+          V[(int64_t)r * N + j] = sn * vi + cs * vj;
+        }
+      }
+    if (maxoff < 1e-15) break;
+  }
+  double* sig = (double*)malloc(sizeof(double) * (size_t)N);
+  int* ord = (int*)malloc(sizeof(int) * (size_t)N);
+  for (int j = 0; j < N; ++j) {
+    double s2 = 0;
+    for (int r = 0; r < M; ++r) {
+      const double aj = fabs(W[(int64_t)r * N + j]);
+      s2 += aj * aj;
+    }
+    sig[j] = sqrt(s2);
+    if (sig[j] > 0)
+      for (int r = 0; r < M; ++r) W[(int64_t)r * N + j] = W[(int64_t)r * N + j] / sig[j];
+    else
+      for (int r = 0; r < M; ++r) W[(int64_t)r * N + j] = 0.0;
+    ord[j] = j;
+  }
+  for (int a = 1; a < N; ++a) { /* stable insertion sort, descending */
+    const int o = ord[a];
+    int b = a - 1;
+    while (b >= 0 && sig[ord[b]] < sig[o]) { ord[b + 1] = ord[b]; --b; }
+    ord[b + 1] = o;
+  }
+  double* Us = (double*)malloc(sizeof(double) * (size_t)M * N); /* sorted tall U, M x N */
+  double* Vs = (double*)malloc(sizeof(double) * (size_t)N * N); /* sorted V, N x N */
+  for (int c = 0; c < N; ++c) {
+    s[c] = sig[ord[c]];
+    for (int r = 0; r < M; ++r) Us[(int64_t)r * N + c] = W[(int64_t)r * N + ord[c]];
+    for (int r = 0; r < N; ++r) Vs[(int64_t)r * N + c] = V[(int64_t)r * N + ord[c]];
+  }
+  const double smax = kk ? s[0] : 0.0;
+  const double eps = 2.220446049250313e-16;
+  const double tol = (rcond < 0 ? eps * (m > n ? m : n) : rcond) * smax;
+  int rk = 0;
+  double* sinv = (double*)malloc(sizeof(double) * (size_t)(kk ? kk : 1));
+  for (int i = 0; i < kk; ++i) {
+    const int ok = s[i] > tol;
+    sinv[i] = ok ? 1.0 / s[i] : 0.0;
+    rk += ok;
+  }
+  *rank = rk;
+  /* u (m x kk) and V = conj(vh)^T (n x kk) of the reference's economy svd */
+  const double* Um = wide ? Vs : Us;
+  const double* Vm = wide ? Us : Vs;
+  double* Uh = (double*)malloc(sizeof(double) * (size_t)kk * m);
+  for (int c = 0; c < kk; ++c)
+    for (int p = 0; p < m; ++p) Uh[(int64_t)c * m + p] = Um[(int64_t)p * kk + c];
+  double* T1 = (double*)malloc(sizeof(double) * (size_t)kk * k);
+  matmul_p(Uh, B, T1, kk, m, k);
+  for (int c = 0; c < kk; ++c)
+    for (int j = 0; j < k; ++j) T1[(int64_t)c * k + j] = sinv[c] * T1[(int64_t)c * k + j];
+  matmul_p(Vm, T1, X, n, kk, k);
+  int has = 0;
+  if (m > n && rk == n) {
+    double* AX = (double*)malloc(sizeof(double) * (size_t)m * k);
+    matmul_p(A, X, AX, m, n, k);
+    for (int j = 0; j < k; ++j) {
+      double acc = 0.0;
+      for (int i = 0; i < m; ++i) {
+        const double d = B[(int64_t)i * k + j] - AX[(int64_t)i * k + j];
+        acc += fabs(d) * fabs(d);
+      }
+      resid[j] = acc;
+    }
+    free(AX);
+    has = 1;
+  }
+  free(W); free(V); free(sig); free(ord); free(Us); free(Vs); free(sinv); free(Uh); free(T1);
+  return has;
+}

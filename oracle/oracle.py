@@ -51,6 +51,8 @@ class Oracle:
         L.oracle_det_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp]
         L.oracle_slogdet_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _dp]
         L.oracle_cholesky_batched.argtypes = [C.c_int64, C.c_int, _dp, _dp, _ip]
+        L.oracle_lstsq.argtypes = [_dp, C.c_int, C.c_int, _dp, C.c_int, C.c_double, _dp, _dp, _ip, _dp]
+        L.oracle_lstsq.restype = C.c_int
         L.oracle_solve_grouped.argtypes = [C.c_int64, _ip, _ip, _i64p, _i64p, _i64p,
                                            _dp, _dp, _dp, _dp, _dp, _dp, _ip]
         self.L = L
@@ -97,6 +99,21 @@ class Oracle:
         la = np.zeros(cnt)
         self.L.oracle_slogdet_batched(cnt, n, _ptr(A), _ptr(s), _ptr(la))
         return s, la
+
+    def lstsq(self, A, B, rcond=-1.0):
+        """One 2-D problem: (x, residuals (size 0 or k), rank, singular values); B (m,) or (m, k)."""
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.asarray(B, np.float64)
+        bvec = B.ndim == 1
+        Bm = np.ascontiguousarray(B.reshape(len(B), -1))
+        m, n = A.shape
+        k = Bm.shape[1]
+        X = np.zeros((n, k))
+        sv = np.zeros(min(m, n))
+        rk = C.c_int()
+        res = np.zeros(max(k, 1))
+        has = self.L.oracle_lstsq(_ptr(A), m, n, _ptr(Bm), k, rcond, _ptr(X), _ptr(sv), C.byref(rk), _ptr(res))
+        return (X[:, 0] if bvec else X), (res[:k] if has else np.zeros(0)), rk.value, sv
 
     def cholesky(self, A):
         """(count, n, n) stack -> (L, ok); ok[i] = 0 where matrix i is not positive definite."""
@@ -180,6 +197,8 @@ class RefLib:
         L.ref_slogdet.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, vp, _ip, _i64p, cp, C.c_int]
         L.ref_matmul_cpu.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int, vp, vp, vp, cp, C.c_int]
         L.ref_cholesky.argtypes = [C.c_int, _i64p, C.c_int, vp, vp, _ip, _i64p, cp, C.c_int]
+        L.ref_lstsq.argtypes = [C.c_int, _i64p, vp, C.c_int, _i64p, vp, C.c_double, vp, _i64p, vp, _i64p, _i64p,
+                                vp, _i64p, cp, C.c_int]
         L.ref_matrix_power.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int64, vp, _ip, _i64p, cp,
                                        C.c_int]
         L.ref_tensorsolve.argtypes = [C.c_int, _i64p, C.c_int, vp, C.c_int, _i64p, C.c_int, vp, C.c_int,
@@ -264,6 +283,20 @@ class RefLib:
 
     def cholesky(self, A):
         return self._unary(self.L.ref_cholesky, A, A.shape)
+
+    def lstsq(self, A, B, rcond=-1.0):
+        A = np.ascontiguousarray(A, np.float64)
+        B = np.ascontiguousarray(B, np.float64)
+        sa = np.array(A.shape, np.int64)
+        sb = np.array(B.shape, np.int64)
+        X = np.zeros(max(A.shape[1] * (B.shape[1] if B.ndim == 2 else 1), 1))
+        R = np.zeros(max(B.shape[1] if B.ndim == 2 else 1, 1))
+        S = np.zeros(max(min(A.shape), 1))
+        xs, rs, ss, rk = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        self._call(self.L.ref_lstsq, 2, _ptr(sa, _i64p), A.ctypes.data, B.ndim, _ptr(sb, _i64p), B.ctypes.data, rcond,
+                   X.ctypes.data, C.byref(xs), R.ctypes.data, C.byref(rs), C.byref(rk), S.ctypes.data, C.byref(ss))
+        xshape = (A.shape[1],) if B.ndim == 1 else (A.shape[1], B.shape[1])
+        return X[:xs.value].reshape(xshape), R[:rs.value], rk.value, S[:ss.value]
 
     def matrix_power(self, A, p):
         A = np.ascontiguousarray(A)

@@ -87,6 +87,20 @@ int ref_slogdet(int nda, const int64_t* sa, int dta, const void* A, void* sign, 
   });
 }
 
+// lstsq (src/linalg/linalg.cpp:755-784): solution, residuals (size 0 or k),
+// rank and singular values, each copied out with its element count.
+int ref_lstsq(int nda, const int64_t* sa, const void* A, int ndb, const int64_t* sb, const void* B,
+              double rcond, void* X, int64_t* x_size, void* R, int64_t* r_size, int64_t* rank, void* S,
+              int64_t* s_size, char* err, int errlen) {
+  return guard(err, errlen, [&] {
+    numpp::linalg::LstsqResult r = numpp::linalg::lstsq(make(nda, sa, 11, A), make(ndb, sb, 11, B), rcond);
+    put(r.solution, X, nullptr, x_size);
+    put(r.residuals, R, nullptr, r_size);
+    put(r.singular_values, S, nullptr, s_size);
+    *rank = r.rank.astype(numpp::kInt64).item<int64_t>({});
+  });
+}
+
 // cholesky (src/linalg/linalg.cpp:117-136; stacks batched.cpp:77).
 int ref_cholesky(int nda, const int64_t* sa, int dta, const void* A, void* out, int* o_dt, int64_t* o_size,
                  char* err, int errlen) {

@@ -15,6 +15,8 @@ NumPP's tests and on small seeded workloads, and stores inputs + outputs:
 * tests/test_linalg_mined3.cpp:29-40             matrix_power of [[1,2],[3,4]] for 0, 1, 2, 7, -1, -3
 * tests/test_tensor_solve.cpp:9-71                tensorsolve / tensorinv of the (2,2,2,2) tridiagonal
 * a seeded (6, 9, 9) stack to the powers 3, 8, -2, -4 (src/linalg/batched.cpp:83-84)
+* tests/test_linalg3.cpp:12-25,70-77        lstsq of the 4x3 and 3x4 matrices, plus seeded tall,
+  wide, square and rank-deficient problems (solution, residuals, rank, singular values)
 * tests/test_linalg.cpp:61-69, tests/test_batched_linalg.cpp:53-58   cholesky of the 3x3 SPD
   matrix, of the (2,2,2) stack, the not-positive-definite error, and a seeded (5, 40, 40) stack
 
@@ -128,6 +130,20 @@ def main():
     Ac = Xc @ Xc.transpose(0, 2, 1) + 40 * np.eye(40)
     Ac[:, 0, 39] = 7.0  # the upper triangle is never read
     g["chol40_A"], g["chol40_L"] = Ac, r.cholesky(Ac)
+
+    rl = np.random.default_rng(99)
+    Rm = np.array([[1.0, 2, 3], [4, 5, 6], [7, 8, 10], [1, 0, 2]])
+    lcases = {"R": (Rm, np.array([1.0, 2, 3, 4])),
+              "W": (np.array([[1.0, 4, 7, 1], [2, 5, 8, 0], [3, 6, 10, 2]]), np.array([1.0, 2, 3])),
+              "tall": (rl.standard_normal((30, 8)), rl.standard_normal((30, 3))),
+              "wide": (rl.standard_normal((7, 19)), rl.standard_normal((7, 2))),
+              "sq": (rl.standard_normal((24, 24)), rl.standard_normal(24)),
+              "def": (np.hstack([rl.standard_normal((16, 4))] * 2), rl.standard_normal((16, 2)))}
+    for key, (Al, Bl) in lcases.items():
+        x, res, rk, sv = r.lstsq(Al, Bl)
+        g[f"lsq_{key}_A"], g[f"lsq_{key}_b"] = Al, Bl
+        g[f"lsq_{key}_x"], g[f"lsq_{key}_res"] = x, res
+        g[f"lsq_{key}_rank"], g[f"lsq_{key}_s"] = np.array(rk), sv
 
     T = np.array([4.0, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4, 1, 0, 0, 1, 4]).reshape(2, 2, 2, 2)
     bt = np.array([1.0, 2, 3, 4]).reshape(2, 2)

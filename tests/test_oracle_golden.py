@@ -164,3 +164,22 @@ def test_cholesky_known_answers(golden, oracle):
     assert ok.all() and bits_equal(L, golden["chol40_L"])
     _, ok = oracle.cholesky(np.array([[[-1.0, 0], [0, -1]]]))
     assert ok[0] == 0 and str(golden["chol_notpd_err"]) == "Matrix is not positive definite"
+
+
+LSQ_CASES = ("R", "W", "tall", "wide", "sq", "def")
+
+
+def test_lstsq_known_answers(golden, oracle):
+    """test_linalg3.cpp:70-77 and seeded tall / wide / square / rank-deficient
+    problems: the restatement of the reference's Jacobi SVD and lstsq
+    (linalg.cpp:620-712, 755-784) reproduces its solution, residuals, rank and
+    singular values bit for bit."""
+    for key in LSQ_CASES:
+        x, res, rk, sv = oracle.lstsq(golden[f"lsq_{key}_A"], golden[f"lsq_{key}_b"])
+        assert bits_equal(x, golden[f"lsq_{key}_x"]), key
+        assert bits_equal(sv, golden[f"lsq_{key}_s"]), key
+        assert rk == int(golden[f"lsq_{key}_rank"]), key
+        assert bits_equal(res, golden[f"lsq_{key}_res"]), key
+    assert int(golden["lsq_def_rank"]) == 4 and golden["lsq_def_res"].size == 0
+    np.testing.assert_allclose(golden["lsq_R_x"], np.linalg.lstsq(golden["lsq_R_A"], golden["lsq_R_b"], rcond=None)[0],
+                               rtol=1e-12)
