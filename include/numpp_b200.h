@@ -95,6 +95,21 @@ int nppb_matrix_power_batched(int64_t count, int32_t n, int64_t p, const double*
  * definite (its k-th pivot is <= 0; the reference raises "Matrix is not
  * positive definite"); L of that system is then undefined. Orders <= 4096. */
 int nppb_cholesky_batched(int64_t count, int32_t n, const double* A, double* L, int32_t* info);
+/* lstsq over `count` problems of one shape (src/linalg/linalg.cpp:755-784;
+ * its SVD :620-712): A (count, m, n), B (count, m, k) row-major; per problem
+ * X (n, k) = pinv(A) B with singular values below
+ * tol = (rcond < 0 ? eps * max(m, n) : rcond) * s_max dropped, S
+ * (min(m, n), descending), rank, and resid (k) with has_resid = 1 when
+ * m > n and rank == n (else resid is not written, as the reference returns
+ * no residuals). k = 0: singular values and rank only (B, X, resid, has_resid
+ * may be NULL). NPPB_DECLINED past min(m, n) = 64, k = 64 or about
+ * m * n + min(m, n)^2 = 26000 (one problem's matrices must fit in shared
+ * memory): the CPU path keeps those. */
+int nppb_lstsq_batched(int64_t count, int32_t m, int32_t n, int32_t k, const double* A, const double* B,
+                       double rcond, double* X, double* S, int32_t* rank, double* resid, int32_t* has_resid);
+int nppb_d_lstsq_batched(int64_t count, int32_t m, int32_t n, int32_t k, const double* dA, const double* dB,
+                         double rcond, double* dX, double* dS, int32_t* drank, double* dres, int32_t* dhas,
+                         void* stream);
 /* The same on device buffers, enqueued on `stream` (workspace allocated
  * stream-ordered for the call). */
 int nppb_d_cholesky_batched(int64_t count, int32_t n, const double* dA, double* dL, int32_t* dinfo,

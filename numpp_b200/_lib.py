@@ -67,6 +67,8 @@ SIGNATURES = {
     "nppb_matrix_power_batched": (_int, [_i64, _i32, _i64, _vp, _vp, _vp]),
     "nppb_cholesky_batched": (_int, [_i64, _i32, _vp, _vp, _vp]),
     "nppb_d_cholesky_batched": (_int, [_i64, _i32, _vp, _vp, _vp, _vp]),
+    "nppb_lstsq_batched": (_int, [_i64, _i32, _i32, _i32, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp]),
+    "nppb_d_lstsq_batched": (_int, [_i64, _i32, _i32, _i32, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp]),
     "nppb_dl_linalg": (_int, [_int] + [_vp] * 9),
     "nppb_dl_matmul": (_int, [_vp] * 4),
     "nppb_dl_cholesky": (_int, [_vp] * 4),

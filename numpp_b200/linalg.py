@@ -17,10 +17,11 @@ on numpy arrays:
   triangle of a is read, ``LinAlgError("Matrix is not positive definite")``.
 * ``matrix_power(a, n)`` -- linalg.cpp:440-454, stacks batched.cpp:83-84.
 * ``tensorsolve(a, b, axes)``, ``tensorinv(a, ind)`` -- tensor_solve.cpp:10-49.
-* ``cond(a, p)`` -- tensor.cpp:359-393 for p in {1, -1, inf, -inf, "fro"}:
-  norm(a, p) * norm(inv(a), p), inf when a is singular. The 2-norm forms
-  (p None, 2, -2) need singular values, which this path does not compute:
-  they raise ``Declined``.
+* ``cond(a, p)`` -- tensor.cpp:359-393: p in {1, -1, inf, -inf, "fro"} as
+  norm(a, p) * norm(inv(a), p), inf when a is singular; p None / 2 / -2 from
+  the singular values.
+* ``lstsq(a, b, rcond)`` -- linalg.cpp:755-784 (its Jacobi SVD :620-712):
+  solution, residuals, rank, singular values; ``svdvals(a)`` -- :725.
 
 dtype policy (``la_kind``, linalg.cpp:20-26): the computation is float64;
 float32 results come back as float32, every other real dtype as float64.
@@ -118,6 +119,27 @@ class NativeBackend:
         info = np.zeros(cnt, np.int32)
         _check(self.L.nppb_cholesky_batched(cnt, n, _lib.ptr(A), _lib.ptr(Lm), _lib.ptr(info)))
         return Lm, info
+
+    def lstsq(self, A, B, rcond):
+        """A (count, m, n), B (count, m, k) -> X, S, rank, resid, has_resid."""
+        cnt, m, n = A.shape
+        k = B.shape[-1]
+        X = np.empty((cnt, n, k))
+        S = np.empty((cnt, min(m, n)))
+        rank = np.zeros(cnt, np.int32)
+        res = np.zeros((cnt, max(k, 1)))
+        has = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_lstsq_batched(cnt, m, n, k, _lib.ptr(A), _lib.ptr(B), float(rcond), _lib.ptr(X),
+                                         _lib.ptr(S), _lib.ptr(rank), _lib.ptr(res), _lib.ptr(has)))
+        return X, S, rank, res[:, :k], has
+
+    def svdvals(self, A):
+        cnt, m, n = A.shape
+        S = np.empty((cnt, min(m, n)))
+        rank = np.zeros(cnt, np.int32)
+        _check(self.L.nppb_lstsq_batched(cnt, m, n, 0, _lib.ptr(A), None, -1.0, None, _lib.ptr(S), _lib.ptr(rank),
+                                         None, None))
+        return S
 
     def gemm_batched(self, A, B):
         cnt, m, k = A.shape
@@ -373,11 +395,21 @@ def cond(a, p=None, backend=None):
     """numpp::cond (src/tensor/tensor.cpp:359-393) for the inverse-based norms.
 
     p in {1, -1, inf, -inf, "fro"}: norm(a, p) * norm(inv(a), p) in float64,
-    inf for a singular matrix (the reference catches linalg_error). A stack
-    (..., n, n) gives one number per matrix. p None / 2 / -2 rest on singular
-    values, outside this path: ``Declined``."""
+    inf for a singular matrix (the reference catches linalg_error). p None /
+    2: s_max / s_min (inf when s_min is 0), p -2: s_min / s_max (0 when s_max
+    is 0), from the singular values of ``svdvals`` (tensor.cpp:372-390). A
+    stack (..., n, n) gives one number per matrix."""
     if p is None or (not isinstance(p, str) and p in (2, -2)):
-        raise Declined("cond with the 2-norm needs singular values, which the B200 path does not compute")
+        s = svdvals(a, backend=backend)
+        if s.shape[-1] == 0:
+            return np.zeros(s.shape[:-1]) if s.ndim > 1 else np.float64(0.0)
+        hi, lo = s[..., 0], s[..., -1]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            if p == -2:
+                c = np.where(hi > 0, lo / np.where(hi > 0, hi, 1.0), 0.0)
+            else:
+                c = np.where(lo > 0, hi / np.where(lo > 0, lo, 1.0), np.inf)
+        return c if c.ndim else np.float64(c)
     if isinstance(p, str):
         if p != "fro":
             raise ValueError(f"cond: unsupported norm {p!r}")
@@ -417,3 +449,50 @@ def cholesky(a, backend=None):
     if info.any():
         raise LinAlgError("Matrix is not positive definite")
     return Lm.reshape(a.shape).astype(out, copy=False)
+
+
+def svdvals(a, backend=None):
+    """Singular values, descending, of a (..., m, n) stack (linalg.cpp:725;
+    the reference's one-sided Jacobi SVD, :620-712)."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    _la_out(a.dtype)
+    if a.ndim < 2:
+        raise ValueError("svdvals requires at least a 2-D array")
+    lead, (m, n) = a.shape[:-2], a.shape[-2:]
+    cnt = int(np.prod(lead)) if lead else 1
+    if cnt == 0 or m == 0 or n == 0:
+        return np.zeros(lead + (min(m, n),))
+    A3 = np.ascontiguousarray(a, np.float64).reshape(cnt, m, n)
+    return be.svdvals(A3).reshape(lead + (min(m, n),))
+
+
+def lstsq(a, b, rcond=-1.0, backend=None):
+    """numpp::linalg::lstsq (linalg.cpp:755-784): (solution, residuals, rank,
+    singular values) of a 2-D a (m, n) and b (m,) or (m, k). Singular values
+    at or below tol = (rcond < 0 ? eps * max(m, n) : rcond) * s_max are
+    dropped; residuals (sum of squares per column) only when m > n and the
+    rank is n, else an empty array. Shapes past the device limits (min(m, n)
+    or k above 64, or a problem too large for one SM's shared memory) are
+    ``Declined``."""
+    be = backend or default_backend()
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.ndim != 2:
+        raise LinAlgError("lstsq: a must be 2-D")
+    m, n = a.shape
+    bvec = b.ndim == 1
+    if b.ndim not in (1, 2) or b.shape[0] != m:
+        raise LinAlgError("lstsq: b must have a.shape[0] rows")
+    out = _la_out(np.result_type(a.dtype, b.dtype))
+    Bm = b.reshape(m, 1) if bvec else b
+    k = Bm.shape[1]
+    if m == 0 or n == 0 or k == 0:
+        x = np.zeros((n,) if bvec else (n, k), out)
+        return x, np.zeros(0), 0, np.zeros(min(m, n))
+    A3 = np.ascontiguousarray(a, np.float64).reshape(1, m, n)
+    B3 = np.ascontiguousarray(Bm, np.float64).reshape(1, m, k)
+    X, S, rank, res, has = be.lstsq(A3, B3, rcond)
+    x = X[0, :, 0] if bvec else X[0]
+    resid = res[0] if has[0] else np.zeros(0)
+    return x.astype(out, copy=False), resid, int(rank[0]), S[0]

@@ -44,6 +44,19 @@ class OracleBackend:
         Lm, ok = self.o.cholesky(A)
         return Lm, (ok == 0).astype(np.int32)
 
+    def lstsq(self, A, B, rcond):
+        self.calls.append(("lstsq", A.shape, B.shape))
+        x, res, rk, sv = self.o.lstsq(A[0], B[0], rcond)
+        has = np.array([1 if res.size else 0], np.int32)
+        r = np.zeros((1, B.shape[-1]))
+        if res.size:
+            r[0] = res
+        return x[None], sv[None], np.array([rk], np.int32), r, has
+
+    def svdvals(self, A):
+        self.calls.append(("svdvals", A.shape))
+        return np.stack([self.o.lstsq(A[i], np.zeros((A.shape[1], 1)))[3] for i in range(A.shape[0])])
+
     def matrix_power(self, A, p):
         self.calls.append(("matrix_power", A.shape, p))
         R, ok = self.o.matrix_power(A, p)
@@ -215,9 +228,8 @@ def test_cond(be):
     S = np.stack([A[0], np.zeros((7, 7))])
     c = la.cond(S, 1, backend=be)
     assert np.isfinite(c[0]) and c[1] == np.inf   # singular -> inf (tensor.cpp:361-368)
-    for p in (None, 2, -2):
-        with pytest.raises(la.Declined):
-            la.cond(A, p, backend=be)
+    for p in (None, 2, -2):  # from the singular values
+        np.testing.assert_allclose(la.cond(A, p, backend=be), np.linalg.cond(A, p), rtol=1e-11)
     with pytest.raises(ValueError):
         la.cond(A, "nuc", backend=be)
 
@@ -262,3 +274,18 @@ def test_step_update_bytes_counts():
     # the order-20 system takes the warp kernel and adds nothing
     want = (16 * 32 * 33 + 8 * 32 * 32 * 1 + 16 * 32 * 33) + (16 * 32 * 1)
     assert workloads.step_update_bytes(sys_) == want
+
+
+def test_lstsq_mirror(golden, be):
+    """linalg.cpp:755-784 semantics through the mirror, against the reference's outputs."""
+    for key in ("R", "W", "tall", "wide", "sq", "def"):
+        x, res, rk, sv = la.lstsq(golden[f"lsq_{key}_A"], golden[f"lsq_{key}_b"], backend=be)
+        assert np.array_equal(x, golden[f"lsq_{key}_x"]), key
+        assert np.array_equal(res, golden[f"lsq_{key}_res"]), key
+        assert rk == int(golden[f"lsq_{key}_rank"]) and np.array_equal(sv, golden[f"lsq_{key}_s"]), key
+    assert la.lstsq(golden["lsq_R_A"], golden["lsq_R_b"], backend=be)[0].shape == (3,)
+    with pytest.raises(la.LinAlgError):
+        la.lstsq(np.ones((2, 3, 4)), np.ones((2, 3)), backend=be)
+    x, res, rk, sv = la.lstsq(np.zeros((0, 3)), np.zeros(0), backend=be)
+    assert x.shape == (3,) and rk == 0
+    np.testing.assert_allclose(la.svdvals(golden["lsq_tall_A"], backend=be), golden["lsq_tall_s"], rtol=1e-14)
