@@ -95,3 +95,23 @@ def test_declined_and_device_entry(lib):
         xn, rn = np.linalg.lstsq(A[i], B[i], rcond=None)[:2]
         np.testing.assert_allclose(dX[i].cpu().numpy(), xn, rtol=1e-10, atol=1e-12)
         np.testing.assert_allclose(dres[i].cpu().numpy(), rn, rtol=1e-10)
+
+
+def test_rcond_and_wide_rank_deficient(lib, oracle):
+    """An explicit rcond drops the same singular values as the reference; a
+    wide rank-deficient problem gives the minimum-norm solution."""
+    rng = np.random.default_rng(8)
+    A = rng.standard_normal((25, 12)) @ np.diag(np.logspace(0, -9, 12)) @ rng.standard_normal((12, 12))
+    b = rng.standard_normal((25, 2))
+    for rcond in (1e-4, 1e-7, 0.0):
+        x, res, rk, sv = la.lstsq(A, b, rcond=rcond)
+        xo, reso, rko, svo = oracle.lstsq(A, b, rcond)
+        assert rk == rko, rcond
+        np.testing.assert_allclose(sv, svo, rtol=0, atol=1e-13 * svo[0])
+        if rk < 12:
+            np.testing.assert_allclose(x, xo, rtol=1e-8, atol=1e-9 * np.abs(xo).max())
+    W = rng.standard_normal((6, 3)) @ rng.standard_normal((3, 20))  # 6 x 20, rank 3
+    bw = rng.standard_normal(6)
+    x, res, rk, sv = la.lstsq(W, bw)
+    assert rk == 3 and res.size == 0
+    np.testing.assert_allclose(x, np.linalg.pinv(W) @ bw, rtol=1e-8, atol=1e-10)
