@@ -4,9 +4,10 @@ Workload (default, one step): the uneven FP64 batch — 8192 systems, order n
 log-uniform in [4, 512], nrhs uniform from {1, 8, 32}, A = N(0,1) + n I, b =
 N(0,1) from default_rng (PCG64, the reference's generator); solve and slogdet
 for every system, inverse for a seeded 10%. One step = one replay of the plan
-(one persistent launch per size class, one CUDA graph) over the whole batch
-with inputs already resident in HBM (1.8 GB of matrices: larger than L2, so
-no flush is needed between steps).
+(one CUDA graph: a warp-kernel launch per class of orders <= 32, a chain of
+step launches per class above, on parallel graph branches) over the whole
+batch with inputs already resident in HBM (1.8 GB of matrices: larger than
+L2, so no flush is needed between steps).
 
 Arms:
   python bench.py [--gpus N --steps K --warmup W]      this path (one rank per GPU)
@@ -50,11 +51,15 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--count", type=int, default=8192)
-    p.add_argument("--cpu-sample", type=int, default=512, help="systems in the bounded CPU sample")
+    p.add_argument("--cpu-sample", type=int, default=0,
+                   help="systems in the CPU baseline's sample (0: the whole batch)")
+    p.add_argument("--cpu-sample-1t", type=int, default=256,
+                   help="systems in the single-threaded CPU baseline's sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-extras", action="store_true",
                    help="skip the side measurements (mixed vs FP64, small batch, serving)")
-    p.add_argument("--serve-seconds", type=float, default=3.0, help="arrival window per serving rate")
+    p.add_argument("--serve-seconds", type=float, default=60.0,
+                   help="arrival window of the sustained serving rate (the other rates get 5 s)")
     p.add_argument("--orders", type=int, nargs=2, metavar=("LO", "HI"), default=None,
                    help="profiling aid: only the systems of the batch with LO <= n <= HI")
     p.add_argument("--no-autotune", action="store_true",
@@ -250,6 +255,20 @@ def mixed_vs_fp64(torch, dev, L, _lib):
     return out
 
 
+def mixed_summary(rows):
+    """One short entry per (workload, kappa, factor): solves/s ratio over the
+    FP64 LU, FP64 fallbacks, worst backward error."""
+    if not isinstance(rows, list):
+        return rows
+    out = []
+    for r in rows:
+        out.append([f"{r['count']}x{r['n']}" + ("rs" if r.get("row_scale_decades") else ""), r["kappa"],
+                    r["mixed_factor"], round(r["mixed_over_fp64"], 3), r["mixed_fp64_fallbacks"],
+                    float("%.2g" % r["mixed_max_berr"])])
+    return {"columns": ["batch", "kappa", "factor", "mixed_over_fp64", "fp64_fallbacks", "max_berr"],
+            "rows": out}
+
+
 def small_uniform(torch, dev, L, _lib, workloads):
     """C1: (256, 32, 32) + 32 I, solve + det, one launch of the warp kernel."""
     P = _lib.ptr
@@ -278,8 +297,10 @@ def small_uniform(torch, dev, L, _lib, workloads):
             "e2e_path": "nppb_solve_det_batched (host buffers, pageable)"}
 
 
-def serving_run(torch, dev, seconds, rates):
-    """C5: Poisson arrivals at each rate against the serving loop; n log-uniform
+def serving_run(torch, dev, sustained_seconds, rates=((500, 5.0), (2000, None), (5000, 5.0))):
+    """C5: Poisson arrivals at each rate against the serving loop (the rate
+    with window None runs for `sustained_seconds`, the others for their
+    window); n log-uniform
     [16, 2048] from a seeded pool of 48 matrices (kappa log-uniform [1e1, 1e10]),
     nrhs U[1, 64], 30% of requests new right-hand sides on a resident factor.
     A waiter thread collects completions so the arrival clock never blocks;
@@ -304,7 +325,8 @@ def serving_run(torch, dev, seconds, rates):
     slots = 384
     xring = torch.zeros(slots, 2048 * 64, dtype=torch.float64).pin_memory().numpy()
     results = []
-    for rate in rates:
+    for rate, window in rates:
+        seconds = sustained_seconds if window is None else window
         lat, statuses = [], []
         q = queue.Queue()
         free = threading.Semaphore(slots)
@@ -364,23 +386,33 @@ def serving_run(torch, dev, seconds, rates):
             st = srv.stats()
         lat_ms = np.asarray(lat) * 1e3
         ok = int(sum(1 for r in statuses if r == 0))
-        results.append({"rate_per_s": rate, "requests": n_req, "completed_ok": ok,
+        results.append({"rate_per_s": rate, "seconds": seconds, "requests": n_req, "completed_ok": ok,
                         "evicted_or_failed": n_req - ok, "solves_s": ok / seconds,
                         "p50_ms": float(np.percentile(lat_ms, 50)), "p99_ms": float(np.percentile(lat_ms, 99)),
                         "batches": st["batches"]})
     return {"workload": "Poisson arrivals, n log-uniform [16,2048] pool of 48, kappa log-uniform [1e1,1e10], "
                         "nrhs U[1,64], 30% re-solves on resident factors, 64 GB budget, FP64 LU",
-            "seconds_per_rate": seconds, "rates": results}
+            "rates": results}
 
-def cpu_reference_sample(sys, sample: int, threads: int, seed: int = 1):
-    """Time the reference's CPU path (oracle/_ref) on a bounded random sample of the
-    same workload; returns (solves/s, kind, cores, description)."""
+def bench_config(count: int, world: int) -> dict:
+    """The workload description both arms print (same dict, same keys)."""
+    return {"workload": WORKLOAD, "count": count, "parallelism": f"replicas{world}",
+            "l2": "inputs (1.76 GB of A at 8192 systems) larger than L2; no flush"}
+
+
+def cpu_reference_sample(sys, sample, threads: int, seed: int = 1):
+    """Time the reference's CPU path (oracle/_ref) on the workload, or on a
+    random sample of `sample` systems of it; returns (solves/s, kind, cores,
+    description, seconds)."""
     from numpp_b200 import workloads
     from oracle import load_oracle, load_ref, ref_available
 
-    rng = np.random.default_rng(seed)
-    idx = np.sort(rng.choice(len(sys["n"]), min(sample, len(sys["n"])), replace=False))
-    sub = workloads.take(sys, idx)
+    if sample is None or sample >= len(sys["n"]):
+        sub, what = sys, f"all {len(sys['n'])} systems"
+    else:
+        rng = np.random.default_rng(seed)
+        idx = np.sort(rng.choice(len(sys["n"]), sample, replace=False))
+        sub, what = workloads.take(sys, idx), f"{sample} of {len(sys['n'])} systems drawn uniformly (seed {seed})"
     if ref_available():
         r = load_ref()
         t0 = time.perf_counter()
@@ -393,30 +425,36 @@ def cpu_reference_sample(sys, sample: int, threads: int, seed: int = 1):
         o.solve_grouped(sub)
         dt = time.perf_counter() - t0
         kind, cores = "port", 1
-    desc = (f"{len(idx)} of {len(sys['n'])} systems drawn uniformly (seed {seed}), "
-            f"numpp::linalg::solve + slogdet + inv per system, {cores} thread(s)")
-    return len(idx) / dt, kind, cores, desc, dt
+    desc = f"{what}, numpp::linalg::solve + slogdet + inv per system, {cores} thread(s)"
+    return len(sub["n"]) / dt, kind, cores, desc, dt
 
 
 def run_reference(args):
+    """The reference's own CPU implementation (oracle/_ref, NumPP's portable LU
+    built from its sources) on every system of the same batch each step, the
+    systems fanned out over all host threads (NumPP itself is single-threaded).
+    ms_per_step is the measured wall time of a step."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     from numpp_b200 import workloads
     sys_ = workloads.uneven_batch(seed=SEED, count=args.count)
     threads = os.cpu_count() or 1
-    rates = []
+    secs = []
+    kind, cores, desc = "port", 1, ""
     for i in range(args.warmup + args.steps):
-        rate, kind, cores, desc, dt = cpu_reference_sample(sys_, args.cpu_sample, threads, seed=100 + i)
+        _, kind, cores, desc, dt = cpu_reference_sample(sys_, None, threads)
         if i >= args.warmup:
-            rates.append(rate)
-    value = float(np.mean(rates))
+            secs.append(dt)
+    step_s = float(np.mean(secs))
+    value = args.count / step_s
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * args.count / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * step_s,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (PCG64 default_rng, seed %d)" % SEED,
-        "config": {"workload": WORKLOAD, "count": args.count, "sample_per_step": args.cpu_sample},
+        "data": "synthetic (PCG64 default_rng, seed %d + rank)" % SEED,
+        "config": bench_config(args.count, world),
+        "p50_ms": 1e3 * float(np.percentile(secs, 50)), "p99_ms": 1e3 * float(np.percentile(secs, 99)),
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": kind, "sample": desc},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -553,30 +591,42 @@ def run_b200(args):
     d2h = 8 * (plan.b_elems + plan.inv_elems + 3 * cnt) + 4 * cnt
 
     cpu = None
+    cpu_1t = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, kind, cores, desc, _ = cpu_reference_sample(sys_, args.cpu_sample, os.cpu_count() or 1)
+        rate, kind, cores, desc, _ = cpu_reference_sample(sys_, args.cpu_sample or None, os.cpu_count() or 1)
         cpu = {"value": rate, "unit": "solves/s", "cores": cores, "kind": kind, "sample": desc}
+        # NumPP as a user calls it: one thread, one system after another
+        rate1, kind1, _, desc1, _ = cpu_reference_sample(sys_, args.cpu_sample_1t, 1)
+        cpu_1t = {"value": rate1, "unit": "solves/s", "cores": 1, "kind": kind1, "sample": desc1}
 
     flops_step = workloads.uneven_flops(sys_)
+    # The workload's bound is the FP64 tensor pipe (17 flop/B of algorithmic
+    # traffic, above the FP64 ridge): achieved = the dominant kind's algorithmic
+    # flops over its launch time, against cuBLAS DGEMM measured in this run.
+    # The HBM view beside it: the same kind's bytes (each trailing element read
+    # and written once per 32-column step) over the same time.
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    hbm_view = None
     if top == "update":
-        # HBM-bound (NB = 32: 4 flop/B): algorithmic bytes over the kind's launch time
-        peaks = measured_peaks()
-        hbm = peaks.get("hbm_gbs")
         bytes_top = workloads.step_update_bytes(sys_)
         ach_gbs = bytes_top / (top_ms * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "kernel": "k_update", "limiter": LIMITER[top], "achieved": ach_gbs,
-                    "peak": hbm or 6650.0, "unit": "GB/s", "frac": ach_gbs / (hbm or 6650.0),
+        hbm_view = {"achieved": ach_gbs, "peak": hbm or 6650.0, "unit": "GB/s", "frac": ach_gbs / (hbm or 6650.0),
                     "peak_source": ("measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs), of measured" if hbm
                                     else "6.65 TB/s, of fallback (no MEASURED_PEAKS.json)"),
-                    "traffic": traffic, "ms_per_step": top_ms, "bytes_per_step": bytes_top,
-                    "tflops": achieved, "tflops_frac_of_fp64": achieved / peak64,
-                    "note": "k_rows + k_update summed over one step's launches, each timed alone"}
-    else:
-        roofline = {"bound": "tensor", "kernel": KERNEL_NAMES[top], "limiter": LIMITER[top],
-                    "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
-                    "peak_source": "measured cuBLAS FP64 GEMM 8192^3 on this GPU (burst), of measured",
-                    "traffic": traffic, "ms_per_step": top_ms, "flops_per_step": flops_top,
-                    "note": "summed over the kernel's launches in one step, each timed alone"}
+                    "bytes_per_step": bytes_top,
+                    "algorithmic_min_bytes_whole_step": workloads.uneven_bytes(sys_),
+                    "traffic_per_step": traffic,
+                    "traffic_source": "ncu one-pass DRAM capture of one plan execution "
+                                      "(profiles/uneven8192_step_traffic.json)"}
+    roofline = {"bound": "tensor", "kernel": KERNEL_NAMES[top], "limiter": LIMITER[top],
+                "achieved": achieved, "peak": peak64, "unit": "TFLOP/s", "frac": achieved / peak64,
+                "peak_source": "measured cuBLAS FP64 GEMM 8192^3 on this GPU (burst), of measured",
+                "traffic": traffic, "ms_per_step": top_ms, "flops_per_step": flops_top,
+                "whole_step_tflops": flops_step / (ms_step * 1e-3) / 1e12,
+                "note": ("k_rows + k_update" if top == "update" else KERNEL_NAMES[top])
+                        + " summed over one step's launches on a one-chain copy of the plan, each timed alone",
+                **({"hbm_view": hbm_view} if hbm_view else {})}
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
         plan.close()
@@ -585,23 +635,22 @@ def run_b200(args):
         # a side measurement that fails is reported, not fatal to the headline line
         for key, fn in (("small_batch", lambda: small_uniform(torch, dev, L, _lib, workloads)),
                         ("mixed_vs_fp64", lambda: mixed_vs_fp64(torch, dev, L, _lib)),
-                        ("serving", lambda: serving_run(torch, dev, args.serve_seconds, (500, 2000, 5000)))):
+                        ("serving", lambda: serving_run(torch, dev, args.serve_seconds))):
             try:
                 extras[key] = fn()
             except Exception as e:  # noqa: BLE001
                 extras[key] = {"error": f"{type(e).__name__}: {e}"}
             torch.cuda.empty_cache()
+        extras["mixed_vs_fp64_summary"] = mixed_summary(extras.get("mixed_vs_fp64"))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (PCG64 default_rng, seed %d + rank)" % SEED,
-            "config": {"workload": WORKLOAD, "count": cnt, "parallelism": f"replicas{world}",
-                       "l2": "inputs (%.2f GB of A) larger than L2; no flush" % (8 * plan.a_elems / 1e9),
-                       "graph": True, "autotuned_chains": chains, "autotuned_lookahead": lookahead,
-                       "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls],
-                       **({"orders_only": list(args.orders)} if args.orders else {})},
+            "config": {**bench_config(cnt, world), **({"orders_only": list(args.orders)} if args.orders else {})},
+            "plan": {"graph": True, "autotuned_chains": chains, "autotuned_lookahead": lookahead,
+                     "classes": [f"{c[0]}<= {c[1]}: {c[2]}" for c in cls]},
             "p50_ms": float(np.percentile(per_step, 50)), "p99_ms": float(np.percentile(per_step, 99)),
             "gflops": flops_step * world / (ms_step * 1e-3) / 1e9,
             "max_backward_error_sample": worst,
@@ -614,9 +663,13 @@ def run_b200(args):
             "gpu_launches": args.steps * nlaunch,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
-            "hbm_peak_gbs": measured_peaks().get("hbm_gbs"),
+            "cpu_baseline_1thread": cpu_1t,
+            "hbm_peak_gbs": hbm,
             **extras,
         }
+        # the compact mixed-vs-FP64 figures last: the end of the line is what log tails keep
+        if "mixed_vs_fp64_summary" in line:
+            line["mixed_vs_fp64_summary"] = line.pop("mixed_vs_fp64_summary")
         print(json.dumps(line), flush=True)
     plan.close()
     if world > 1:

@@ -161,18 +161,21 @@ int nppb_d_getrs_batched(int64_t count, int32_t n, int32_t nrhs, const double* d
 
 /* Allocation-free solve. No counterpart in the reference: NumPP's CUDA
  * backend allocates per call (src/backend/cuda_backend.cu:126-146,189-206).
- * For callers that must not allocate device memory while they run (code in a
- * CUDA graph being captured, hosts whose device memory is reserved up front,
- * fixed-pool allocators): X = A^-1 B for a uniform batch on device buffers,
- * with no cudaMalloc / cudaFree or allocating call. Orders above 32 use a
- * fixed 32 MiB scratch array inside the library, so count * (8*n*n + 8616)
- * bytes must fit in 32 MiB (NPPB_E_RANGE otherwise, before any GPU work);
- * orders up to 32 need no scratch. The first call on each device looks up the
- * array's device address, so make that first call before any stream capture;
- * each device that has set it up keeps the 32 MiB until the process exits.
- * Every call shares the array: calls that overlap on the GPU (other streams,
- * other threads) race and must be ordered by the caller. info as for the
- * other solves; dX must not alias dB. */
+ * For callers that must not allocate device memory while they run (hosts
+ * whose device memory is reserved up front, fixed-pool allocators where a
+ * cudaMalloc would fail or stall): X = A^-1 B for a uniform batch on device
+ * buffers, with no cudaMalloc / cudaFree or allocating call. Orders above 32
+ * use a fixed 32 MiB scratch array inside the library, so
+ * count * (8*n*n + 8616) bytes must fit in 32 MiB (NPPB_E_RANGE otherwise,
+ * before any GPU work); orders up to 32 need no scratch. The array belongs to
+ * the library's module: its 32 MiB are reserved on every device where the
+ * module is loaded (each context under eager module loading, the first use
+ * under lazy loading) until the process exits. The first call on each device
+ * looks up the array's device address, so make that first call before any
+ * stream capture. Every call shares the array: calls that overlap on the GPU
+ * (other streams, other threads) race and must be ordered by the caller.
+ * Always the single-level step schedule (NPPB_BLOCKED_MIN_N is ignored).
+ * info as for the other solves; dX must not alias dB. */
 int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                  const double* dB, double* dX, int32_t* dinfo, void* stream);
 
@@ -253,8 +256,10 @@ int nppb_server_destroy(nppb_server* srv);
 
 /* ---- uneven batches ------------------------------------------------------ */
 /* A plan packs `count` systems of different orders n[i] and right-hand-side
- * counts nrhs[i] into size classes, one persistent launch per class, and
- * replays them as one CUDA graph. System i's matrix starts at element
+ * counts nrhs[i] into size classes (one warp-kernel launch per class of
+ * orders <= 32; one chain of panel / row-move / update / substitution
+ * launches per class above, chains on parallel graph branches) and replays
+ * them as one CUDA graph. System i's matrix starts at element
  * a_off[i] of the packed A array, its right-hand side / solution at b_off[i]
  * of B / X, and its inverse (when inv_off[i] >= 0) at inv_off[i] of Inv.
  * Per-system outputs (sign, logabsdet, det, info) are indexed by i.

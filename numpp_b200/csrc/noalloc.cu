@@ -1,20 +1,33 @@
 // Allocation-free batched solve: nppb_d_solve_batched_noalloc.
 //
-// For callers that cannot allocate device memory while they run: code inside a
-// CUDA graph being captured, real-time or embedded hosts that pre-reserve all
-// memory, and allocators with fixed pools where a cudaMalloc would fail or
-// stall. The solve of a uniform batch needs an LU workspace and per-system
-// step state for orders above 32; here they live in one file-scope device
-// array of fixed size instead of being allocated per call.
+// For callers that cannot allocate device memory while they run: real-time or
+// embedded hosts that reserve all device memory up front, and fixed-pool
+// allocators where a cudaMalloc would fail or stall mid-run. The solve of a
+// uniform batch needs an LU workspace and per-system step state for orders
+// above 32; here they live in one file-scope device array of fixed size
+// instead of being allocated per call. The array belongs to the library's
+// module, so its 32 MiB are reserved on every device where that module is
+// loaded (each context under eager module loading; the first use under lazy
+// loading) until the process exits.
 //
 // The array is a host-side symbol in host code, not a device address: its
 // device address is fetched once per device with cudaGetSymbolAddress (the
-// first call on each device does that, with the device current) and only that
-// address is passed to the kernels.
+// first call on each device does that, with the device current, so make that
+// first call before any stream capture) and only that address is passed to
+// the kernels. Every call shares the array and it keeps the last call's
+// contents; nothing in it needs to start at zero (every call writes the LU
+// workspace and the step state before reading them). Calls that overlap on the
+// GPU race on it.
+//
+// This solve always takes the single-level step kernels (it ignores
+// NPPB_BLOCKED_MIN_N, whose two-level schedule needs a per-call history
+// buffer), so with that variable set its results can differ from the
+// allocating solve's in the last bits.
 #include <cuda_runtime.h>
 
 #include <cstddef>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "../../include/numpp_b200.h"
@@ -24,7 +37,7 @@
 namespace nppb {
 namespace {
 
-constexpr size_t kNoAllocBytes = size_t(32) << 20;  // 32 MiB on every device that sets it up
+constexpr size_t kNoAllocBytes = size_t(32) << 20;  // 32 MiB on every device that loads the module
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -57,10 +70,10 @@ int scratch_address(void** out) {
 
 using namespace nppb;
 
-extern "C" int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA,
-                                            const double* dB, double* dX, int32_t* dinfo,
-                                            void* stream) {
-  clear_error();
+namespace {
+
+int solve_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA, const double* dB, double* dX,
+                  int32_t* dinfo, void* stream) {
   if (count < 0 || n < 0 || nrhs < 0) {
     set_error("negative count, order or nrhs");
     return NPPB_E_ARG;
@@ -115,4 +128,18 @@ extern "C" int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nr
   }
   if (e != cudaSuccess) return cuda_status(e, "allocation-free solve launch");
   return NPPB_OK;
+}
+
+}  // namespace
+
+extern "C" int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const double* dA,
+                                            const double* dB, double* dX, int32_t* dinfo,
+                                            void* stream) {
+  try {  // error text is a std::string: no exception may leave the C ABI
+    clear_error();
+    return solve_noalloc(count, n, nrhs, dA, dB, dX, dinfo, stream);
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return NPPB_E_NOMEM;
+  }
 }

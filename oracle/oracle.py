@@ -24,11 +24,14 @@ def _ptr(a, t=_dp):
     return a.ctypes.data_as(t) if a is not None else None
 
 
-def build_oracle() -> None:
-    """Compile liboracle.so (and the reference library when its sources exist)."""
+def build_oracle(ref_src: str | None = None) -> None:
+    """Compile liboracle.so, and the reference library when the NumPP source
+    tree is named (``ref_src``, else the NUMPP_REF_SRC environment variable)
+    and present; without one the reference build is skipped."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
-    if os.path.isdir(os.environ.get("NUMPP_REF_SRC", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    src = ref_src or os.environ.get("NUMPP_REF_SRC")
+    if src and os.path.isdir(src):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={src}"], check=True)
 
 
 class Oracle:
