@@ -182,34 +182,42 @@ int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const d
 /* ---- mixed precision: FP32 factors, FP64 iterative refinement ---------- */
 /* No counterpart in the reference (NumPP solves in double only,
  * src/linalg/linalg.cpp:92-103). X = A^-1 B for a uniform batch: power-of-two
- * row/column equilibration, LU in FP32 on the step-wise kernels, then FP64
- * refinement (R = B - A X in FP64, correction solved with the FP32 factors,
- * added in FP64) until the normwise backward error
- * eta = max|R| / (||A||_inf max|X| + max|B|) <= tol. A system whose eta stops
- * halving is stalled; stalled systems, FP32 zero pivots and systems still
- * refining after max_iter corrections are refactored and solved in FP64.
- * Per system: berr (final eta), ferr (max|X - Xtrue| / max|Xtrue|, when Xtrue
- * is given), iters (corrections applied), fallback (1 = the FP64 solve ran),
- * info (of the FP64 solve, when it ran). Orders <= 32 always take the FP64
- * warp kernel (fallback = 1). The device form synchronises `stream` (it reads
- * convergence counts back between corrections).
- * Trailing products of the FP32 factorisation: by default on the tensor
- * cores as error-compensated TF32 (each operand split into two TF32 parts,
- * three products: close to FP32 accuracy); NPPB_MIXED_TF32 / NPPB_MIXED_BF16:
- * one tensor-core product from operands rounded to TF32 / BF16;
- * NPPB_MIXED_FP32_FMA: FP32 fused multiply-adds. FP32 accumulation in every
- * case; the panels, the stored factors and the correction solves stay FP32.
- * The TF32 products run on the warp-level mma.sync instructions, or with
- * NPPB_MIXED_TCGEN05 on tcgen05 with TMEM accumulators (same products; the
- * mma.sync form measured faster here: the update is bound by memory, not by
- * the tensor core). BF16 always uses mma.sync. */
+ * row/column equilibration, an LU in FP32, then FP64 refinement (R = B - A X
+ * in FP64, correction solved with the FP32 factors, added in FP64) until the
+ * normwise backward error eta = max|R| / (||A||_inf max|X| + max|B|) <= tol.
+ * A system whose eta stops halving is stalled; stalled systems, FP32 zero
+ * pivots and systems still refining after max_iter corrections are
+ * refactored and solved in FP64. Per system: berr (final eta), ferr
+ * (max|X - Xtrue| / max|Xtrue|, when Xtrue is given), iters (corrections
+ * applied), fallback (1 = the FP64 solve ran), info (of the FP64 solve, when
+ * it ran). Orders <= 32 always take the FP64 warp kernel (fallback = 1). The
+ * device form synchronises `stream` (it reads convergence counts back between
+ * corrections).
+ * The FP32 factorisation, by default: the equilibrated matrix mixed by a
+ * depth-2 random butterfly transform on both sides, padded to a multiple of
+ * 128 with an identity block, and factored in 128-column blocks with partial
+ * pivoting among each diagonal block's own rows; each block's two triangular
+ * solves (by the inverses of its diagonal factors) and its trailing update
+ * run as tcgen05 GEMMs with error-compensated TF32 products (each operand
+ * split into two TF32 parts, three products: close to FP32 accuracy) and TMEM
+ * accumulators, operands staged by TMA. The refinement works on the original
+ * matrix: the transform and the restricted pivoting change which factors
+ * precondition the corrections, not the system solved.
+ * With NPPB_MIXED_PIVOTED (or any of TF32 / BF16 / FP32_FMA / TCGEN05): LU
+ * with partial pivoting on the step-wise kernels; trailing products as
+ * error-compensated TF32 (default), one TF32 or BF16 product (NPPB_MIXED_TF32
+ * / NPPB_MIXED_BF16), or FP32 fused multiply-adds (NPPB_MIXED_FP32_FMA); the
+ * TF32 products on mma.sync, or with NPPB_MIXED_TCGEN05 on tcgen05 with TMEM
+ * accumulators. FP32 accumulation in every case; the stored factors and the
+ * correction solves stay FP32. */
 enum {
   NPPB_MIXED_NO_EQUILIBRATE = 1,
   NPPB_MIXED_NO_FALLBACK = 2,
   NPPB_MIXED_TF32 = 4,
   NPPB_MIXED_BF16 = 8,
   NPPB_MIXED_FP32_FMA = 16,
-  NPPB_MIXED_TCGEN05 = 32
+  NPPB_MIXED_TCGEN05 = 32,
+  NPPB_MIXED_PIVOTED = 64
 };
 int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                const double* dB, double* dX, const double* dXtrue, double tol,

@@ -326,6 +326,12 @@ cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, floa
   k_equil_apply<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, cs, A32, st);
   return cudaGetLastError();
 }
+cudaError_t mixed_equil_scan(const double* A, int count, int n, int equil, double* rs, double* cmax,
+                             RefineState* st, cudaStream_t s) {
+  const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
+  k_equil_rows<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, st);
+  return cudaGetLastError();
+}
 cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,
                             RefineState* st, cudaStream_t s) {
   k_scale_rhs<<<count, MT, 0, s>>>(B, n, nrhs, rs, B32, st);

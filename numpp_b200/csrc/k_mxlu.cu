@@ -1,0 +1,949 @@
+// Randomised blocked LU in FP32 on tcgen05 (the mixed solve's factorisation)
+// and its triangular solves. See mxlu.hpp for the algorithm.
+//
+// Kernels, per system of a uniform batch padded to order N (multiple of 128):
+//  k_mx_build      M = U^T (Dr A Dc) V in FP64, rounded once to FP32. A depth-2
+//                  butterfly restricted to the rows {r, r+N/4, r+N/2, r+3N/4}
+//                  is a 4x4 matrix, so each thread maps one 4x4 quad of A to
+//                  one quad of M.
+//  k_mx_transpose  the first block's panel row, transposed (A12^T).
+//  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
+//                  among its own rows, with L^-1 P and U^-T from the same row
+//                  operations (one CTA, 4 threads per row, the row in
+//                  registers, one barrier per column).
+//  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
+//                  by TMA in 128-byte-swizzled boxes (two stages of 32-column
+//                  chunks), split into TF32 hi / lo in shared memory, one
+//                  thread issues tcgen05.mma.kind::tf32 (M = N = 128) into a
+//                  TMEM accumulator, tcgen05.ld epilogue against the C tile
+//                  (loaded by TMA behind the products), TMA store.
+//  k_mx_trsv       forward and back substitution by 128-row blocks with the
+//                  stored diagonal-block inverses, one CTA per system and
+//                  right-hand-side chunk, the right-hand sides in shared memory.
+//  k_mx_rhs_in / k_mx_apply   U^T applied to a right-hand side, V and the
+//                  column scales applied to a solution (FP64 accumulation).
+// Every wait on an mbarrier is bounded (a second of %globaltimer): past it the
+// CTA counts a timeout, skips its stores, releases its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <mutex>
+
+#include "mxlu.hpp"
+
+namespace nppb {
+namespace {
+
+// ---------------------------------------------------------------------------
+// Random butterflies.
+
+__device__ __forceinline__ uint32_t mx_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x85ebca6bu;
+  x ^= x >> 13;
+  x *= 0xc2b2ae35u;
+  x ^= x >> 16;
+  return x;
+}
+
+// Diagonal entry i of butterfly factor `stage`: exp(u / 10), u uniform in
+// [-1/2, 1/2) (the distribution of the RBT papers), from a counter hash so that
+// every kernel reproduces the same transform.
+__device__ __forceinline__ double rbt_d(uint32_t stage, uint32_t i) {
+  const uint32_t h = mx_hash(mx_hash(i * 2u + 1u) ^ (0x9e3779b9u * (stage + 1u)));
+  const double u = (double)(h >> 8) * (1.0 / 16777216.0) - 0.5;
+  return exp(0.1 * u);
+}
+
+// The depth-2 butterfly W = D2 B_N (B_N = 2^-1/2 [R S; R -S], D2 = two such
+// blocks of order N/2) restricted to the quad {r, r+q, r+2q, r+3q}, q = N/4.
+// side 0: the left transform U, side 1: the right transform V.
+__device__ void rbt_quad(int side, int r, int q, double Q[4][4]) {
+  const uint32_t b = 6u * (uint32_t)side;
+  const double R0 = rbt_d(b, r), S0 = rbt_d(b + 1, r), R1 = rbt_d(b, r + q), S1 = rbt_d(b + 1, r + q);
+  const double Ra = rbt_d(b + 2, r), Sa = rbt_d(b + 3, r), Rb = rbt_d(b + 4, r), Sb = rbt_d(b + 5, r);
+  Q[0][0] = 0.5 * Ra * R0;  Q[0][1] = 0.5 * Sa * R1;  Q[0][2] = 0.5 * Ra * S0;  Q[0][3] = 0.5 * Sa * S1;
+  Q[1][0] = 0.5 * Ra * R0;  Q[1][1] = -0.5 * Sa * R1; Q[1][2] = 0.5 * Ra * S0;  Q[1][3] = -0.5 * Sa * S1;
+  Q[2][0] = 0.5 * Rb * R0;  Q[2][1] = 0.5 * Sb * R1;  Q[2][2] = -0.5 * Rb * S0; Q[2][3] = -0.5 * Sb * S1;
+  Q[3][0] = 0.5 * Rb * R0;  Q[3][1] = -0.5 * Sb * R1; Q[3][2] = -0.5 * Rb * S0; Q[3][3] = 0.5 * Sb * S1;
+}
+
+__device__ __forceinline__ double pow2_scale(double m) {
+  if (!(m > 0.0) || !isfinite(m)) return 1.0;
+  return ldexp(1.0, -ilogb(m));
+}
+
+constexpr int BQX = 32, BQY = 8;
+
+__global__ void __launch_bounds__(BQX * BQY)
+k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const double* __restrict__ cmax, int equil,
+           double* __restrict__ cs, RefineState* __restrict__ st, float* __restrict__ M, int n, int N) {
+  __shared__ double Uq[BQY][4][4];
+  __shared__ double Vq[BQX][4][4];
+  const int s = blockIdx.z, q = N / 4;
+  const int tid = threadIdx.y * BQX + threadIdx.x;
+  if (tid < BQY) {
+    const int r = blockIdx.y * BQY + tid;
+    if (r < q) rbt_quad(0, r, q, Uq[tid]);
+  } else if (tid >= 32 && tid < 32 + BQX) {
+    const int c = blockIdx.x * BQX + tid - 32;
+    if (c < q) rbt_quad(1, c, q, Vq[tid - 32]);
+  }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+    st[s].eta = INFINITY;
+    st[s].prev = INFINITY;
+    st[s].status = kRefineActive;
+    st[s].iters = 0;
+  }
+  __syncthreads();
+  const int cq = blockIdx.x * BQX + threadIdx.x, rq = blockIdx.y * BQY + threadIdx.y;
+  if (cq >= q || rq >= q) return;
+  double csb[4], rsa[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int j = cq + b * q;
+    csb[b] = (j < n && equil) ? pow2_scale(cmax[(int64_t)s * n + j]) : 1.0;
+    if (j < n && blockIdx.y == 0 && threadIdx.y == 0) cs[(int64_t)s * n + j] = csb[b];
+    const int i = rq + b * q;
+    rsa[b] = i < n ? rs[(int64_t)s * n + i] : 1.0;
+  }
+  const double* As = A + (int64_t)s * n * n;
+  double a[4][4];
+#pragma unroll
+  for (int x = 0; x < 4; ++x) {
+    const int i = rq + x * q;
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      const int j = cq + y * q;
+      a[x][y] = (i < n && j < n) ? rsa[x] * As[(int64_t)i * n + j] * csb[y] : (i == j ? 1.0 : 0.0);
+    }
+  }
+  double t[4][4];  // A V
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      double v = 0.0;
+#pragma unroll
+      for (int z = 0; z < 4; ++z) v = fma(a[x][z], Vq[threadIdx.x][z][y], v);
+      t[x][y] = v;
+    }
+  float* Ms = M + (int64_t)s * N * N;
+#pragma unroll
+  for (int x = 0; x < 4; ++x)
+#pragma unroll
+    for (int y = 0; y < 4; ++y) {
+      double v = 0.0;  // (U^T A V)[x][y]
+#pragma unroll
+      for (int z = 0; z < 4; ++z) v = fma(Uq[threadIdx.y][z][x], t[z][y], v);
+      Ms[(int64_t)(rq + x * q) * N + cq + y * q] = (float)v;
+    }
+}
+
+// T[buf][s][j][r] = M[s][K + r][j] for r < 128, K + 128 <= j < N.
+__global__ void __launch_bounds__(256)
+k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K, int count, int buf) {
+  __shared__ float t[32][33];
+  const int s = blockIdx.z, j0 = K + kMxNB + blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const float* Ms = M + (int64_t)s * N * N;
+  for (int y = threadIdx.y; y < 32; y += 8) t[y][threadIdx.x] = Ms[(int64_t)(K + r0 + y) * N + j0 + threadIdx.x];
+  __syncthreads();
+  float* Tz = T + ((int64_t)buf * count + s) * N * kMxNB;
+  for (int y = threadIdx.y; y < 32; y += 8) Tz[(int64_t)(j0 + y) * kMxNB + r0 + threadIdx.x] = t[threadIdx.x][y];
+}
+
+// ---------------------------------------------------------------------------
+// Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
+// (L^-1 P) and U^-T.
+//
+// Thread t owns physical row i = t / 4 of the block (original order), columns
+// j = ph + 4q (ph = t % 4, q = 0..31): the row of A (becoming multipliers and
+// U) and the row's L^-1 in position space, both in registers; and row p = i
+// (a position) of the running U^-T in shared memory (thread-private column of
+// Yu). Step k: each warp proposes its largest |A[i][k]| among rows not yet
+// chosen (lowest row on ties) and publishes that row; after one barrier every
+// thread picks the block's winner, which takes position k; every row not yet
+// chosen takes l = A[i][k] / U[k][k] and updates A[i][k+1:] -= l U[k][k+1:],
+// Linv[i][:k] -= l Linv_w[:k], Linv[i][k] = -l (Gauss elimination of [A | I]
+// in position space gives L^-1). U^-T runs one step behind: row k-1 of it is
+// Y[k-1] / U[k-1][k-1] once step k-1's update is in, published before step
+// k's barrier and applied after it, Y[p] -= U[k-1][p] U^-T[k-1] for p >= k.
+// Out: the packed LU of P A11 in M, L^-1 P (the permutation folded into the
+// stored inverse, so that U12 = (L^-1 P) A12 and the forward substitution
+// need no row exchanges), U^-1 and U^-T.
+constexpr int DT = 512, DW = DT / 32;
+constexpr size_t kDiagSmem = sizeof(float) * (32 * DT + kMxNB * kMxNB + 2 * kMxNB) +
+                             sizeof(uint32_t) * (2 * DW * 2) + sizeof(int) * kMxNB;
+
+struct DiagCtx {
+  float* Yu;
+  float* big;
+  float* xrow;
+  uint32_t* keys;
+  int* fail;
+  int tid, i, ph, lane, warp;
+};
+
+// Step KK of the diagonal factorisation (a compile-time column, so that every
+// register index below is static).
+template <int KK>
+__device__ __forceinline__ void diag_step(const DiagCtx& c, float (&a)[32], float (&l)[32], bool& chosen, int& pos,
+                                          float& ukp, float& rpiv) {
+  constexpr int kq = KK >> 2, kph = KK & 3, b = KK & 1;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int tid = c.tid, i = c.i, ph = c.ph;
+  float* cand = c.big + b * (DW * 256);
+  float* xr = c.xrow + b * kMxNB;
+  float* Yu = c.Yu;
+  // finish row KK-1 of U^-T and publish it
+  if (KK > 0 && i == KK - 1) {
+    constexpr int pq = (KK - 1) >> 2, pph = (KK - 1) & 3;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      if (q < pq || (q == pq && ph <= pph)) {
+        const float x = Yu[q * DT + tid] * rpiv;
+        Yu[q * DT + tid] = x;
+        xr[ph * 32 + q] = x;
+      }
+    }
+  }
+  // this warp's candidate: the largest |A[i][KK]| among rows not chosen yet
+  const float aik = __shfl_sync(FULL, a[kq], (c.lane & ~3) | kph);
+  const uint32_t key = chosen ? 0u : __float_as_uint(fabsf(aik)) + 1u;
+  const uint32_t wmax = __reduce_max_sync(FULL, key);
+  const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)i : 0xffffffffu);
+  if ((uint32_t)i == wrow) {
+    float4* ca = reinterpret_cast<float4*>(cand + c.warp * 256 + ph * 32);
+    float4* cl = reinterpret_cast<float4*>(cand + c.warp * 256 + kMxNB + ph * 32);
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      ca[v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
+      if (4 * v <= kq) cl[v] = make_float4(l[4 * v], l[4 * v + 1], l[4 * v + 2], l[4 * v + 3]);
+    }
+    if (ph == 0) {
+      c.keys[(b * DW + c.warp) * 2] = wmax;
+      c.keys[(b * DW + c.warp) * 2 + 1] = wrow;
+    }
+  }
+  __syncthreads();
+  // the block's winner: largest key, lowest row on ties
+  uint32_t bk = 0u, br = 0xffffffffu;
+  int bw = 0;
+#pragma unroll
+  for (int w = 0; w < DW; ++w) {
+    const uint32_t kw = c.keys[(b * DW + w) * 2], rw = c.keys[(b * DW + w) * 2 + 1];
+    if (kw > bk || (kw == bk && rw < br)) {
+      bk = kw;
+      br = rw;
+      bw = w;
+    }
+  }
+  const float* wa = cand + bw * 256;
+  const float* wl = wa + kMxNB;
+  const float piv = wa[kph * 32 + kq];
+  if (tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
+  // U^-T, one step behind: positions p >= KK take row KK-1
+  if (KK > 0 && i >= KK) {
+    constexpr int pq = (KK - 1) >> 2, pph = (KK - 1) & 3;
+#pragma unroll
+    for (int q = 0; q < 32; ++q)
+      if (q < pq || (q == pq && ph <= pph)) Yu[q * DT + tid] = fmaf(-ukp, xr[ph * 32 + q], Yu[q * DT + tid]);
+  }
+  ukp = wa[(i & 3) * 32 + (i >> 2)];  // U[KK][i], for position i's update at the next step
+  rpiv = 1.0f / piv;
+  if ((uint32_t)i == br) {
+    chosen = true;
+    pos = KK;
+    if (ph == kph) l[kq] = 1.f;
+  } else if (!chosen) {
+    const float lik = aik / piv;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+      if (q > kq || (q == kq && ph > kph)) a[q] = fmaf(-lik, wa[ph * 32 + q], a[q]);
+      if (q < kq || (q == kq && ph < kph)) l[q] = fmaf(-lik, wl[ph * 32 + q], l[q]);
+      if (q == kq && ph == kph) {
+        a[q] = lik;
+        l[q] = -lik;
+      }
+    }
+  }
+}
+
+template <int KK>
+struct DiagSteps {
+  static __device__ __forceinline__ void run(const DiagCtx& c, float (&a)[32], float (&l)[32], bool& chosen,
+                                             int& pos, float& ukp, float& rpiv) {
+    diag_step<KK>(c, a, l, chosen, pos, ukp, rpiv);
+    DiagSteps<KK + 1>::run(c, a, l, chosen, pos, ukp, rpiv);
+  }
+};
+template <>
+struct DiagSteps<kMxNB> {
+  static __device__ __forceinline__ void run(const DiagCtx&, float (&)[32], float (&)[32], bool&, int&, float&,
+                                             float&) {}
+};
+
+__global__ void __launch_bounds__(DT, 1)
+k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
+          int32_t* __restrict__ info, int N, int k) {
+  extern __shared__ __align__(16) float dsm[];
+  float* Yu = dsm;                              // [32][DT]
+  float* big = Yu + 32 * DT;                    // loop: [2][DW][256] candidate rows; after: [128][128] L^-1 by position
+  float* xrow = big + kMxNB * kMxNB;            // [2][128]: finished row of U^-T, [ph][q] layout
+  uint32_t* keys = reinterpret_cast<uint32_t*>(xrow + 2 * kMxNB);  // [2][DW][2]: key, row
+  int* posOf = reinterpret_cast<int*>(keys + 4 * DW);             // [128]
+  __shared__ int fail;
+  const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x;
+  const int i = tid >> 2, ph = tid & 3;
+  float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
+  float a[32], l[32];
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    a[q] = Mb[(int64_t)i * N + ph + 4 * q];
+    l[q] = 0.f;
+    Yu[q * DT + tid] = (i == ph + 4 * q) ? 1.f : 0.f;
+  }
+  bool chosen = false;
+  int pos = 0;
+  float ukp = 0.f, rpiv = 1.f;
+  if (tid == 0) fail = 0;
+  __syncthreads();
+  const DiagCtx ctx{Yu, big, xrow, keys, &fail, tid, i, ph, tid & 31, tid >> 5};
+  DiagSteps<0>::run(ctx, a, l, chosen, pos, ukp, rpiv);
+  if (i == kMxNB - 1) {  // the last row of U^-T
+#pragma unroll
+    for (int q = 0; q < 32; ++q) Yu[q * DT + tid] *= rpiv;
+  }
+  __syncthreads();  // the candidate buffers are free: L^-1 by position goes there
+  if (ph == 0) posOf[i] = pos;
+#pragma unroll
+  for (int q = 0; q < 32; ++q) {
+    big[pos * kMxNB + ph + 4 * q] = l[q];
+    Mb[(int64_t)pos * N + ph + 4 * q] = a[q];
+  }
+  __syncthreads();
+  float* Lb = Linv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
+  float* Ub = Uinv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
+  float* UTb = UinvT + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
+  for (int idx = tid; idx < kMxNB * kMxNB; idx += DT) {
+    const int r = idx >> 7, c = idx & 127;
+    Lb[idx] = big[r * kMxNB + posOf[c]];              // (L^-1 P)[r][c]
+    UTb[idx] = Yu[(c >> 2) * DT + 4 * r + (c & 3)];   // U^-T[r][c]
+    Ub[idx] = Yu[(r >> 2) * DT + 4 * c + (r & 3)];    // U^-1[r][c] = U^-T[c][r]
+  }
+  if (tid == 0 && fail && info[s] == 0) info[s] = K + fail;
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 GEMM: one 128 x 128 tile of C, K = 128, per CTA.
+
+constexpr int GT = 256;
+constexpr int BOX = 128 * 128;  // bytes of one 128-row x 32-float swizzled box
+constexpr size_t kGemmSmem = 1024 + 12 * (size_t)BOX + 128;
+
+struct MxGemmArgs {
+  int ax, ay, az;  // A box origin of tile (mt = 0, chunk 0): x = K column, y = row, z = plane offset
+  int bx, by, bz;  // B (stored as B^T: row = output column) of tile (nt = 0)
+  int cx, cy, cz;  // C tile (0, 0)
+  int split3;
+  // optional transposed copy of each result element (r, c) of tile (mt, nt):
+  // tr + s * tr_sys + (tr_r0 + 128 mt + r) * tr_row + (tr_c0 + 128 nt + c) * tr_col
+  float* tr;
+  int64_t tr_sys, tr_col, tr_row;
+  int tr_c0, tr_r0, tr_mt0_only;
+};
+
+__device__ int g_mx_timeouts = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for phase `parity` of an mbarrier (one second).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done = 0;
+  const uint64_t t0 = global_ns();
+  while (true) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (global_ns() - t0 > 1000000000ull) return false;
+  }
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load(uint32_t dst, const CUtensorMap* map, uint32_t bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];\n" ::
+          "r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(bar), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_store(const CUtensorMap* map, uint32_t src, int x, int y, int z) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];\n" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(src), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+
+// K-major operand, 128-byte swizzle: 8-row groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
+}
+
+// kind::tf32, FP32 accumulator, A and B K-major, N = 128, M = 128
+constexpr uint32_t MX_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((128u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void mx_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(MX_IDESC), "r"(acc));
+}
+
+__device__ __forceinline__ void mx_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void mx_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(r[e]);
+}
+
+__device__ __forceinline__ float tf32_hi(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// In place x -> tf32(x) and lo = x - tf32(x) for one 16 KB box.
+__device__ __forceinline__ void split_box(float* raw, float* lo, int tid) {
+  float4* r4 = reinterpret_cast<float4*>(raw);
+  float4* l4 = reinterpret_cast<float4*>(lo);
+#pragma unroll 4
+  for (int e = tid; e < BOX / 16; e += GT) {
+    const float4 x = r4[e];
+    float4 h;
+    h.x = tf32_hi(x.x);
+    h.y = tf32_hi(x.y);
+    h.z = tf32_hi(x.z);
+    h.w = tf32_hi(x.w);
+    r4[e] = h;
+    l4[e] = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+  }
+}
+
+template <int SUB>
+__global__ void __launch_bounds__(GT, 1)
+k_mx_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
+          const __grid_constant__ CUtensorMap mC, const MxGemmArgs g) {
+  extern __shared__ __align__(1024) unsigned char gsm_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+  // stage st (0, 1): A hi at base + st*4*BOX, B hi + BOX, A lo + 2 BOX, B lo + 3 BOX; C tile: 4 boxes
+  unsigned char* Cs = base + 8 * BOX;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(base + 12 * BOX);  // full[2], freed[2], cfull, done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 6);
+  int* abort_flag = reinterpret_cast<int*>(bars + 7);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nt = blockIdx.x, mt = blockIdx.y, s = blockIdx.z;
+  const uint32_t bar0 = smem_u32(bars);
+  auto full = [&](int st) { return bar0 + 8u * st; };
+  auto freed = [&](int st) { return bar0 + 16u + 8u * st; };
+  const uint32_t cfull = bar0 + 32u, done = bar0 + 40u;
+
+  if (warp == 0) {  // the whole warp, converged: TMEM for the 128 x 128 FP32 accumulator
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;\n" ::"r"(smem_u32(tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    for (int b = 0; b < 6; ++b) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar0 + 8u * b));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
+    *abort_flag = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const uint32_t tmem = *tslot;
+
+  const int ay = g.ay + 128 * mt, az = g.az + s;
+  const int by = g.by + 128 * nt, bz = g.bz + s;
+  const int cx = g.cx + 128 * nt, cy = g.cy + 128 * mt, cz = g.cz + s;
+  auto stage = [&](int st) { return base + (size_t)st * 4 * BOX; };
+  if (tid == 0) {
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      mbar_expect_tx(full(c), 2 * BOX);
+      tma_load(smem_u32(stage(c)), &mA, full(c), g.ax + 32 * c, ay, az);
+      tma_load(smem_u32(stage(c) + BOX), &mB, full(c), g.bx + 32 * c, by, bz);
+    }
+    if (SUB) {
+      mbar_expect_tx(cfull, 4 * BOX);
+#pragma unroll
+      for (int b = 0; b < 4; ++b) tma_load(smem_u32(Cs + b * BOX), &mC, cfull, cx + 32 * b, cy, cz);
+    }
+  }
+  bool ok = true;
+#pragma unroll 1
+  for (int c = 0; c < 4; ++c) {
+    const int st = c & 1;
+    const uint32_t par = (uint32_t)(c >> 1) & 1u;
+    unsigned char* sb = stage(st);
+    if (!mbar_wait(full(st), par)) ok = false;
+    if (g.split3) {
+      split_box(reinterpret_cast<float*>(sb), reinterpret_cast<float*>(sb + 2 * BOX), tid);
+      split_box(reinterpret_cast<float*>(sb + BOX), reinterpret_cast<float*>(sb + 3 * BOX), tid);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const uint64_t dA = sw128_desc(smem_u32(sb)), dB = sw128_desc(smem_u32(sb + BOX));
+      const uint64_t dAl = sw128_desc(smem_u32(sb + 2 * BOX)), dBl = sw128_desc(smem_u32(sb + 3 * BOX));
+#pragma unroll
+      for (int ks = 0; ks < 4; ++ks) {
+        const uint64_t o = (uint64_t)(2 * ks);  // 32 bytes along K, in 16-byte units
+        const uint32_t acc0 = (c | ks) != 0;
+        if (g.split3) {
+          mx_mma(tmem, dAl + o, dB + o, acc0);  // small terms first
+          mx_mma(tmem, dA + o, dBl + o, 1u);
+          mx_mma(tmem, dA + o, dB + o, 1u);
+        } else {
+          mx_mma(tmem, dA + o, dB + o, acc0);
+        }
+      }
+      mx_commit(freed(st));
+      if (c + 2 < 4) {
+        // the stage is reloaded once the products reading it are done
+        if (!mbar_wait(freed(st), par)) {
+          ok = false;
+        } else {
+          mbar_expect_tx(full(st), 2 * BOX);
+          tma_load(smem_u32(sb), &mA, full(st), g.ax + 32 * (c + 2), ay, az);
+          tma_load(smem_u32(sb + BOX), &mB, full(st), g.bx + 32 * (c + 2), by, bz);
+        }
+      }
+    }
+  }
+  if (tid == 0) mx_commit(done);
+  if (!mbar_wait(done, 0)) ok = false;
+  if (SUB && !mbar_wait(cfull, 0)) ok = false;
+  if (!ok) {
+    *abort_flag = 1;
+    atomicAdd(&g_mx_timeouts, 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  __syncthreads();
+  const bool live = *abort_flag == 0;
+  {
+    const int qw = warp & 3, hf = warp >> 2, r = 32 * qw + lane;
+    float acc[64];
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mx_ld16(tmem + ((uint32_t)(32 * qw) << 16) + (uint32_t)(64 * hf + 16 * i), acc + 16 * i);
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::);
+    const bool tr = live && g.tr != nullptr && (!g.tr_mt0_only || mt == 0);
+    float* trp = tr ? g.tr + (int64_t)s * g.tr_sys + (int64_t)(g.tr_r0 + 128 * mt + r) * g.tr_row +
+                          (int64_t)(g.tr_c0 + 128 * nt) * g.tr_col
+                    : nullptr;
+#pragma unroll
+    for (int cc = 0; cc < 16; ++cc) {
+      const int c = 64 * hf + 4 * cc, b = c >> 5, ch = ((c & 31) >> 2) ^ (r & 7);
+      float4* p = reinterpret_cast<float4*>(Cs + b * BOX + r * 128 + ch * 16);
+      float4 v;
+      if (SUB) {
+        v = *p;
+        v.x -= acc[4 * cc];
+        v.y -= acc[4 * cc + 1];
+        v.z -= acc[4 * cc + 2];
+        v.w -= acc[4 * cc + 3];
+      } else {
+        v = make_float4(acc[4 * cc], acc[4 * cc + 1], acc[4 * cc + 2], acc[4 * cc + 3]);
+      }
+      *p = v;
+      if (tr) {
+        float* t = trp + (int64_t)c * g.tr_col;
+        t[0] = v.x;
+        t[g.tr_col] = v.y;
+        t[2 * g.tr_col] = v.z;
+        t[3 * g.tr_col] = v.w;
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (tid == 0 && live) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) tma_store(&mC, smem_u32(Cs + b * BOX), cx + 32 * b, cy, cz);
+    asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory");
+  }
+  if (warp == 0) {
+    __syncwarp();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;\n" ::"r"(tmem));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Triangular solves with the block factors: one CTA per (system, chunk of W
+// right-hand sides); the chunk sits in shared memory (N x W floats).
+
+constexpr int ST = 1024;  // threads: 32 warps
+
+// tmp[i][w] = sum_m D[i][m] y[m][w], i < 128 (D row-major 128 x 128)
+template <int W>
+__device__ __forceinline__ void block_apply(const float* __restrict__ D, const float* ys, float* tmp, int warp,
+                                            int lane) {
+  float yv[4][W];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int w = 0; w < W; ++w) yv[e][w] = ys[(4 * lane + e) * W + w];
+#pragma unroll
+  for (int rr = 0; rr < 4; ++rr) {
+    const int i = warp + 32 * rr;
+    const float4 d = *reinterpret_cast<const float4*>(D + i * kMxNB + 4 * lane);
+    float sum[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) sum[w] = d.x * yv[0][w] + d.y * yv[1][w] + d.z * yv[2][w] + d.w * yv[3][w];
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+#pragma unroll
+      for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
+    if (lane == 0)
+#pragma unroll
+      for (int w = 0; w < W; ++w) tmp[i * W + w] = sum[w];
+  }
+}
+
+// ys[i] -= M[i][K:K+128] . ys[K:K+128] for rows r0 <= i < r1 (warp per row, RU rows in flight)
+template <int W>
+__device__ __forceinline__ void panel_apply(const float* __restrict__ Ms, int N, int K, int r0, int r1, float* ys,
+                                            int warp, int lane) {
+  constexpr int RU = W <= 2 ? 8 : (W == 4 ? 4 : 2);
+  float yv[4][W];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int w = 0; w < W; ++w) yv[e][w] = ys[(K + 4 * lane + e) * W + w];
+  for (int i0 = r0 + warp; i0 < r1; i0 += 32 * RU) {
+    float4 m[RU];
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int i = i0 + 32 * u;
+      m[u] = i < r1 ? __ldcs(reinterpret_cast<const float4*>(Ms + (int64_t)i * N + K + 4 * lane))
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      const int i = i0 + 32 * u;
+      float sum[W];
+#pragma unroll
+      for (int w = 0; w < W; ++w)
+        sum[w] = m[u].x * yv[0][w] + m[u].y * yv[1][w] + m[u].z * yv[2][w] + m[u].w * yv[3][w];
+#pragma unroll
+      for (int o = 16; o; o >>= 1)
+#pragma unroll
+        for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
+      if (lane == 0 && i < r1)
+#pragma unroll
+        for (int w = 0; w < W; ++w) ys[i * W + w] -= sum[w];
+    }
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(ST, 1)
+k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const float* __restrict__ Uinv,
+          float* __restrict__ Y, int N, int nrhs, const RefineState* __restrict__ st, int only_active) {
+  extern __shared__ float ys[];  // [N][W], then tmp [128][W]
+  float* tmp = ys + (int64_t)N * W;
+  const int s = blockIdx.x, c0 = blockIdx.y * W;
+  if (only_active && st[s].status != kRefineActive) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float* Ms = M + (int64_t)s * N * N;
+  float* Ys = Y + (int64_t)s * N * nrhs;
+  for (int idx = tid; idx < N * W; idx += ST) {
+    const int i = idx / W, w = idx % W;
+    ys[idx] = c0 + w < nrhs ? Ys[(int64_t)i * nrhs + c0 + w] : 0.f;
+  }
+  __syncthreads();
+  const int nb = N / kMxNB;
+  const float* Ls = Linv + (int64_t)s * N * kMxNB;
+  const float* Us = Uinv + (int64_t)s * N * kMxNB;
+  for (int k = 0; k < nb; ++k) {  // L y = P c, block by block
+    const int K = k * kMxNB;
+    block_apply<W>(Ls + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
+    __syncthreads();
+    for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];
+    __syncthreads();
+    panel_apply<W>(Ms, N, K, K + kMxNB, N, ys, warp, lane);
+    __syncthreads();
+  }
+  for (int k = nb - 1; k >= 0; --k) {  // U x = y
+    const int K = k * kMxNB;
+    block_apply<W>(Us + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
+    __syncthreads();
+    for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];
+    __syncthreads();
+    panel_apply<W>(Ms, N, K, 0, K, ys, warp, lane);
+    __syncthreads();
+  }
+  for (int idx = tid; idx < N * W; idx += ST) {
+    const int i = idx / W, w = idx % W;
+    if (c0 + w < nrhs) Ys[(int64_t)i * nrhs + c0 + w] = ys[idx];
+  }
+}
+
+// Y = U^T pad(R): thread per (row quad, right-hand side).
+__global__ void __launch_bounds__(256)
+k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, int nrhs,
+            const RefineState* __restrict__ st, int only_active) {
+  const int s = blockIdx.y;
+  if (only_active && st[s].status != kRefineActive) return;
+  const int q = N / 4;
+  const int idx = blockIdx.x * 256 + threadIdx.x;
+  if (idx >= q * nrhs) return;
+  const int r = idx / nrhs, col = idx % nrhs;
+  double U[4][4];
+  rbt_quad(0, r, q, U);
+  double x[4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = r + a * q;
+    x[a] = i < n ? (double)R[((int64_t)s * n + i) * nrhs + col] : 0.0;
+  }
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) v = fma(U[b][a], x[b], v);
+    Y[((int64_t)s * N + r + a * q) * nrhs + col] = (float)v;
+  }
+}
+
+// X (=|+=) cs * (V Y)[0:n] in FP64: thread per (column quad, right-hand side).
+__global__ void __launch_bounds__(256)
+k_mx_apply(const float* __restrict__ Y, double* __restrict__ X, const double* __restrict__ cs, int n, int N,
+           int nrhs, const RefineState* __restrict__ st, int init) {
+  const int s = blockIdx.y;
+  if (!init && st[s].status != kRefineActive) return;
+  const int q = N / 4;
+  const int idx = blockIdx.x * 256 + threadIdx.x;
+  if (idx >= q * nrhs) return;
+  const int c = idx / nrhs, col = idx % nrhs;
+  double V[4][4];
+  rbt_quad(1, c, q, V);
+  double y[4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) y[b] = (double)Y[((int64_t)s * N + c + b * q) * nrhs + col];
+#pragma unroll
+  for (int a = 0; a < 4; ++a) {
+    const int i = c + a * q;
+    if (i >= n) continue;
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) v = fma(V[a][b], y[b], v);
+    double* x = X + ((int64_t)s * n + i) * nrhs + col;
+    const double d = cs[(int64_t)s * n + i] * v;
+    *x = init ? d : *x + d;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor maps and launches.
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// 3-D FP32 map {inner, rows, planes} (row-major planes), 32 x 128 boxes, 128-byte swizzle.
+bool make_map(CUtensorMap* m, const float* base, uint64_t inner, uint64_t rows, uint64_t planes) {
+  auto fn = encode_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {inner, rows, planes};
+  const cuuint64_t strides[2] = {inner * sizeof(float), inner * rows * sizeof(float)};
+  const cuuint32_t box[3] = {32, 128, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+}  // namespace
+
+size_t mx_workspace_bytes(int count, int n) {
+  const size_t N = (size_t)mx_padded(n), c = (size_t)count;
+  return align256(4 * c * N * N) + align256(4 * 2 * c * N * kMxNB) + 3 * align256(4 * c * N * kMxNB) +
+         align256(4 * c);
+}
+
+void mx_carve(MxBufs& b, void* base, int count, int n) {
+  const size_t N = (size_t)mx_padded(n), c = (size_t)count;
+  unsigned char* p = static_cast<unsigned char*>(base);
+  b.count = count;
+  b.n = n;
+  b.N = (int)N;
+  b.M = reinterpret_cast<float*>(p);
+  p += align256(4 * c * N * N);
+  b.T = reinterpret_cast<float*>(p);
+  p += align256(4 * 2 * c * N * kMxNB);
+  b.Linv = reinterpret_cast<float*>(p);
+  p += align256(4 * c * N * kMxNB);
+  b.Uinv = reinterpret_cast<float*>(p);
+  p += align256(4 * c * N * kMxNB);
+  b.UinvT = reinterpret_cast<float*>(p);
+  p += align256(4 * c * N * kMxNB);
+  b.info = reinterpret_cast<int32_t*>(p);
+}
+
+cudaError_t mx_prepare() {
+  cudaError_t e = cudaFuncSetAttribute(k_mx_gemm<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
+  const int tsm = (int)(sizeof(float) * ((size_t)4096 * 8 + kMxNB * 8));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
+  return e;
+}
+
+int mx_timeouts_take() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_mx_timeouts, sizeof(int)) != cudaSuccess) return -1;
+  const int z = 0;
+  if (cudaMemcpyToSymbol(g_mx_timeouts, &z, sizeof(int)) != cudaSuccess) return -1;
+  return v;
+}
+
+cudaError_t mx_build(const double* A, const double* rs, const double* cmax, int equil, double* cs, RefineState* st,
+                     const MxBufs& b, cudaStream_t s) {
+  const int q = b.N / 4;
+  const dim3 grid((unsigned)((q + BQX - 1) / BQX), (unsigned)((q + BQY - 1) / BQY), (unsigned)b.count);
+  k_mx_build<<<grid, dim3(BQX, BQY), 0, s>>>(A, rs, cmax, equil, cs, st, b.M, b.n, b.N);
+  return cudaGetLastError();
+}
+
+cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
+  const int N = b.N, count = b.count, nb = N / kMxNB;
+  CUtensorMap mM, mT, mL, mUT;
+  if (!make_map(&mM, b.M, N, N, count) || !make_map(&mT, b.T, kMxNB, N, 2 * (uint64_t)count) ||
+      !make_map(&mL, b.Linv, kMxNB, N, count) || !make_map(&mUT, b.UinvT, kMxNB, N, count))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(b.info, 0, sizeof(int32_t) * count, s);
+  if (e != cudaSuccess) return e;
+  if (nb > 1) {
+    k_mx_transpose<<<dim3((unsigned)((N - kMxNB) / 32), kMxNB / 32, (unsigned)count), dim3(32, 8), 0, s>>>(
+        b.M, b.T, N, 0, count, 0);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  int buf = 0;
+  for (int k = 0; k < nb; ++k) {
+    const int K = k * kMxNB, tiles = nb - k - 1;
+    k_mx_diag<<<count, DT, kDiagSmem, s>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.info, N, k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (tiles == 0) break;
+    MxGemmArgs g{};
+    g.split3 = b.split3;
+    // L21 = A21 U11^-1: B^T = U11^-T (block k of UinvT)
+    g.ax = K; g.ay = K + kMxNB; g.az = 0;
+    g.bx = 0; g.by = K; g.bz = 0;
+    g.cx = K; g.cy = K + kMxNB; g.cz = 0;
+    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mM, mUT, mM, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // U12^T = A12^T (L11^-1 P)^T: B^T = L11^-1 P (block k of Linv); U12 also written back into M's panel row
+    g.ax = 0; g.ay = K + kMxNB; g.az = buf * count;
+    g.bx = 0; g.by = K; g.bz = 0;
+    g.cx = 0; g.cy = K + kMxNB; g.cz = buf * count;
+    g.tr = b.M; g.tr_sys = (int64_t)N * N; g.tr_col = N; g.tr_row = 1; g.tr_c0 = K; g.tr_r0 = K + kMxNB;
+    g.tr_mt0_only = 0;
+    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mT, mL, mT, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // A22 -= L21 U12; the first row tile also writes the next panel row, transposed, into the other T buffer
+    g.ax = K; g.ay = K + kMxNB; g.az = 0;
+    g.bx = 0; g.by = K + kMxNB; g.bz = buf * count;
+    g.cx = K + kMxNB; g.cy = K + kMxNB; g.cz = 0;
+    g.tr = b.T + (int64_t)(buf ^ 1) * count * N * kMxNB;
+    g.tr_sys = (int64_t)N * kMxNB; g.tr_col = kMxNB; g.tr_row = 1; g.tr_c0 = K + kMxNB; g.tr_r0 = 0;
+    g.tr_mt0_only = 1;
+    k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mM, mT, mM, g);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    buf ^= 1;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t mx_rhs_in(const float* R, float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b,
+                      cudaStream_t s) {
+  const int work = b.N / 4 * nrhs;
+  k_mx_rhs_in<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(R, Y, b.n, b.N, nrhs, st,
+                                                                                      only_active);
+  return cudaGetLastError();
+}
+
+cudaError_t mx_solve(float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, cudaStream_t s) {
+  const int W = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;
+  const dim3 grid((unsigned)b.count, (unsigned)((nrhs + W - 1) / W));
+  const size_t sm = sizeof(float) * ((size_t)b.N * W + kMxNB * W);
+  switch (W) {
+    case 1: k_mx_trsv<1><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
+    case 2: k_mx_trsv<2><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
+    case 4: k_mx_trsv<4><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
+    default: k_mx_trsv<8><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t mx_apply(const float* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
+                     const MxBufs& b, cudaStream_t s) {
+  const int work = b.N / 4 * nrhs;
+  k_mx_apply<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(Y, X, cs, b.n, b.N, nrhs, st,
+                                                                                     init);
+  return cudaGetLastError();
+}
+
+}  // namespace nppb

@@ -2,11 +2,15 @@
 //
 // No counterpart in the reference (NumPP solves in double only,
 // src/linalg/linalg.cpp:92-103). For a uniform batch of order n:
-//  1. equilibrate: power-of-two row/column scales, the scaled matrix in FP32;
-//  2. factor in FP32 on the step-wise kernels (pivots and row moves kept),
-//     the first solution riding along as augmented columns; the trailing
-//     products on the tensor cores (error-compensated TF32 by default, or
-//     plain TF32 / BF16 operands) or in FP32 FMA;
+//  1. equilibrate: power-of-two row/column scales;
+//  2. factor in FP32. Default: the scaled matrix mixed by random butterflies
+//     on both sides and factored in 128-column blocks with pivoting inside
+//     each diagonal block, every block's triangular solves and trailing update
+//     as tcgen05 GEMMs with error-compensated TF32 products (k_mxlu.cu). With
+//     a pivoted flag: partial pivoting on the step-wise kernels (row moves
+//     kept), the first solution riding along as augmented columns, trailing
+//     products as error-compensated TF32, TF32, BF16 (mma.sync or tcgen05) or
+//     FP32 FMA;
 //  3. refine in FP64: R = B - A X, eta = normwise backward error; systems with
 //     eta <= tol stop, systems whose eta no longer halves are marked stalled;
 //     the others solve A d = R with the FP32 factors and add d in FP64;
@@ -23,6 +27,7 @@
 
 #include "../../include/numpp_b200.h"
 #include "mixed.hpp"
+#include "mxlu.hpp"
 #include "runtime.hpp"
 
 using namespace nppb;
@@ -49,7 +54,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   }
   const int arith = flags & (NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA);
   if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 |
-                 NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05)) ||
+                 NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05 | NPPB_MIXED_PIVOTED)) ||
       (arith & (arith - 1))) {
     set_error("unknown mixed flag bits, or more than one of TF32 / BF16 / FP32_FMA");
     return NPPB_E_ARG;
@@ -66,13 +71,21 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   if (!device()) return NPPB_E_NODEV;
   const int count = (int)count64;
   const size_t nn = (size_t)n * n, nb = (size_t)n * nrhs, c = (size_t)count;
-  DevMem a32, piv, rpos, sc32, b32, y32, rsm, csm, cmx, stm, info32, act;
-  NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
-  NPPB_CUDA(piv.alloc(sizeof(int32_t) * c * n, st), "workspace");
-  NPPB_CUDA(rpos.alloc(sizeof(int32_t) * c * n, st), "workspace");
-  NPPB_CUDA(sc32.alloc(sizeof(StepScratchT<float>) * c, st), "workspace");
+  const bool pivoted =
+      (flags & (NPPB_MIXED_PIVOTED | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05)) != 0;
+  const bool blocked = n > 32 && !pivoted;
+  DevMem a32, piv, rpos, sc32, b32, y32, rsm, csm, cmx, stm, info32, act, mxw;
+  if (!blocked) {
+    NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
+    NPPB_CUDA(piv.alloc(sizeof(int32_t) * c * n, st), "workspace");
+    NPPB_CUDA(rpos.alloc(sizeof(int32_t) * c * n, st), "workspace");
+    NPPB_CUDA(sc32.alloc(sizeof(StepScratchT<float>) * c, st), "workspace");
+    NPPB_CUDA(y32.alloc(sizeof(float) * c * nb, st), "workspace");
+  } else {
+    NPPB_CUDA(mxw.alloc(mx_workspace_bytes(count, n), st), "workspace");
+    NPPB_CUDA(y32.alloc(sizeof(float) * c * (size_t)mx_padded(n) * nrhs, st), "workspace");
+  }
   NPPB_CUDA(b32.alloc(sizeof(float) * c * nb, st), "workspace");
-  NPPB_CUDA(y32.alloc(sizeof(float) * c * nb, st), "workspace");
   NPPB_CUDA(rsm.alloc(sizeof(double) * c * n, st), "workspace");
   NPPB_CUDA(csm.alloc(sizeof(double) * c * n, st), "workspace");
   NPPB_CUDA(cmx.alloc(sizeof(double) * c * n, st), "workspace");
@@ -83,15 +96,58 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   NPPB_CUDA(act.alloc(sizeof(int), st), "workspace");
   RefineState* S = stm.as<RefineState>();
   const bool equil = !(flags & NPPB_MIXED_NO_EQUILIBRATE);
-  NPPB_CUDA(mixed_equilibrate(dA, count, n, equil ? 1 : 0, a32.as<float>(), rsm.as<double>(), csm.as<double>(),
-                              cmx.as<double>(), S, st),
-            "equilibrate");
+  if (blocked) {
+    NPPB_CUDA(mixed_equil_scan(dA, count, n, equil ? 1 : 0, rsm.as<double>(), cmx.as<double>(), S, st),
+              "equilibrate");
+  } else {
+    NPPB_CUDA(mixed_equilibrate(dA, count, n, equil ? 1 : 0, a32.as<float>(), rsm.as<double>(), csm.as<double>(),
+                                cmx.as<double>(), S, st),
+              "equilibrate");
+  }
   NPPB_CUDA(mixed_scale_rhs(dB, count, n, nrhs, rsm.as<double>(), b32.as<float>(), S, st), "scale rhs");
 
   std::vector<RefineState> hs(c);
   std::vector<int32_t> fallback(c, 0);
   bool any_fallback = false;
-  if (n > 32) {
+  if (blocked) {
+    MxBufs mb;
+    mx_carve(mb, mxw.as<void>(), count, n);
+    NPPB_CUDA(mx_build(dA, rsm.as<double>(), cmx.as<double>(), equil ? 1 : 0, csm.as<double>(), S, mb, st),
+              "butterfly transform");
+    NPPB_CUDA(mx_factor(mb, st), "FP32 block factorisation");
+    NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+    if (mx_timeouts_take() != 0) {
+      set_error("tensor-core block factorisation: a completion wait ran out");
+      return NPPB_E_CUDA;
+    }
+    NPPB_CUDA(mixed_mark_fp32_failures(mb.info, S, count, st), "mark");
+    float* Y = y32.as<float>();
+    NPPB_CUDA(mx_rhs_in(b32.as<float>(), Y, nrhs, S, 0, mb, st), "transform rhs");
+    NPPB_CUDA(mx_solve(Y, nrhs, S, 0, mb, st), "FP32 solve");
+    NPPB_CUDA(mx_apply(Y, dX, csm.as<double>(), nrhs, S, 1, mb, st), "apply");
+    int h_act = 0;
+    for (int it = 0;; ++it) {
+      NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
+      // the scaled residual lands in b32 (row order of A)
+      NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), nullptr, S, tol, it,
+                               1, act.as<int>(), st),
+                "residual");
+      NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
+      NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+      if (h_act == 0 || it >= max_iter) break;
+      NPPB_CUDA(mx_rhs_in(b32.as<float>(), Y, nrhs, S, 1, mb, st), "transform residual");
+      NPPB_CUDA(mx_solve(Y, nrhs, S, 1, mb, st), "FP32 correction solve");
+      NPPB_CUDA(mx_apply(Y, dX, csm.as<double>(), nrhs, S, 0, mb, st), "apply");
+    }
+    NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
+    NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+    for (size_t s = 0; s < c; ++s) {
+      if (hs[s].status != kRefineConverged && !(flags & NPPB_MIXED_NO_FALLBACK)) {
+        fallback[s] = 1;
+        any_fallback = true;
+      }
+    }
+  } else if (n > 32) {
     StepArgsT<float> sa{};
     sa.scratch = sc32.as<StepScratchT<float>>();
     sa.A = nullptr;  // factor the scaled FP32 matrix in place

@@ -29,6 +29,10 @@ struct RefineState {
 // st and cmax (count * n doubles of column maxima) must be zero on entry.
 cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, float* A32, double* rs,
                               double* cs, double* cmax, RefineState* st, cudaStream_t s);
+// The row pass of mixed_equilibrate alone: row scales rs, ||A||_inf into st,
+// column maxima of diag(rs)|A| into cmax (no FP32 copy of A).
+cudaError_t mixed_equil_scan(const double* A, int count, int n, int equil, double* rs, double* cmax,
+                             RefineState* st, cudaStream_t s);
 cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,
                             RefineState* st, cudaStream_t s);
 cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, int n, int nrhs,

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "../../include/numpp_b200.h"
+#include "mxlu.hpp"
 #include "nppb_step.hpp"
 
 namespace nppb {
@@ -113,7 +114,10 @@ void DevMem::release() {
   p_ = nullptr;
 }
 
-cudaError_t prepare_kernels() { return step_prepare(); }
+cudaError_t prepare_kernels() {
+  cudaError_t e = step_prepare();
+  return e == cudaSuccess ? mx_prepare() : e;
+}
 
 namespace {
 

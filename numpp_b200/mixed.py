@@ -11,14 +11,18 @@ _FACTOR = {"3xtf32": 0, "fp32": _lib.MIXED_FP32_FMA, "tf32": _lib.MIXED_TF32, "b
 
 
 def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equilibrate: bool = True,
-                fallback: bool = True, factor: str = "3xtf32", tcgen05: bool = False):
+                fallback: bool = True, factor: str = "3xtf32", tcgen05: bool = False, pivoted: bool = False):
     """X for a (count, n, n) / (count, n, nrhs) float64 batch; returns
     (X, report) with report = dict(berr, ferr, iters, fallback, info) per system.
-    factor: arithmetic of the factorisation's trailing products: "3xtf32"
-    (error-compensated TF32 tensor-core products, close to FP32), "tf32" or
-    "bf16" (one tensor-core product), "fp32" (FMA); FP32 panels and stored
-    factors in every case. tcgen05: TF32 products on the tcgen05 tensor
-    cores with TMEM accumulators instead of the warp-level mma.sync."""
+
+    Default: the blocked FP32 factorisation of the butterfly-transformed
+    matrix (pivoting inside each 128-row diagonal block, triangular solves and
+    trailing updates as tcgen05 GEMMs with error-compensated TF32 products).
+    pivoted=True, or any factor other than "3xtf32", or tcgen05=True: LU with
+    partial pivoting on the step-wise kernels, factor choosing the trailing
+    products: "3xtf32" (error-compensated TF32, close to FP32), "tf32" or
+    "bf16" (one tensor-core product), "fp32" (FMA); tcgen05: TF32 products on
+    the tcgen05 tensor cores with TMEM accumulators instead of mma.sync."""
     L = _lib.load()
     A = np.ascontiguousarray(A, np.float64)
     B = np.ascontiguousarray(B, np.float64)
@@ -31,7 +35,7 @@ def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equil
     fb = np.zeros(cnt, np.int32)
     Xt = None if X_true is None else np.ascontiguousarray(X_true, np.float64)
     flags = ((0 if equilibrate else _lib.MIXED_NO_EQUILIBRATE) | (0 if fallback else _lib.MIXED_NO_FALLBACK)
-             | _FACTOR[factor] | (_lib.MIXED_TCGEN05 if tcgen05 else 0))
+             | _FACTOR[factor] | (_lib.MIXED_TCGEN05 if tcgen05 else 0) | (_lib.MIXED_PIVOTED if pivoted else 0))
     P = _lib.ptr
     _check(L.nppb_solve_mixed_batched(cnt, n, k, P(A), P(B), P(X), P(Xt), tol, max_iter, flags, P(info),
                                       P(berr), P(ferr), P(iters), P(fb)))

@@ -10,6 +10,9 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ORACLE_SO = os.path.join(_HERE, "liboracle.so")
 _REF_SO = os.path.join(_HERE, "_ref", "libnumpp_ref.so")
+# NumPP's portable sources with the B200 front end and GPU vtable compiled in
+# (the drop-in; oracle/Makefile target `dropin`)
+DROPIN_SO = os.path.join(_HERE, "_ref", "dropin", "libnumpp_dropin.so")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -31,7 +34,7 @@ def build_oracle(ref_src: str | None = None) -> None:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     src = ref_src or os.environ.get("NUMPP_REF_SRC")
     if src and os.path.isdir(src):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "dropin", f"REF={src}"], check=True)
 
 
 class Oracle:
@@ -211,7 +214,17 @@ class RefLib:
                                         _dp, _dp, _dp, _dp, _i32p, C.c_int]
         L.ref_standard_normal2.argtypes = [C.c_uint64, C.c_int64, _dp, C.c_int64, _dp]
         L.ref_uniform.argtypes = [C.c_uint64, C.c_double, C.c_double, C.c_int64, _dp]
+        L.ref_last_backend.restype = C.c_int
         self.L = L
+
+    BACKEND_CPU, BACKEND_CUDA = 1, 6
+
+    def last_backend(self) -> int:
+        """numpp::last_backend() of the calling thread, as its enum value."""
+        return self.L.ref_last_backend()
+
+    def clear_last_backend(self):
+        self.L.ref_clear_last_backend()
 
     @staticmethod
     def _dt(a):

@@ -178,6 +178,12 @@ int ref_solve_grouped(int64_t count, const int32_t* n, const int32_t* nrhs, cons
   return 0;
 }
 
+// numpp::last_backend() (src/backend/backend.cpp:118-119), as its enum value
+// (numpp::Backend: Auto 0, Cpu 1, Blas 2, Device 3, Metal 4, Vulkan 5, Cuda 6,
+// OpenCL 7), and set_last_backend(Auto) to clear it between calls.
+int ref_last_backend(void) { return static_cast<int>(numpp::last_backend()); }
+void ref_clear_last_backend(void) { numpp::set_last_backend(numpp::Backend::Auto); }
+
 // numpp::random::default_rng(seed): n1 standard normals, then n2 more from the
 // same generator (the draw order of the uniform-batch workload: A, then b).
 int ref_standard_normal2(uint64_t seed, int64_t n1, double* out1, int64_t n2, double* out2) {
