@@ -185,9 +185,10 @@ int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const d
  * row/column equilibration, an LU in FP32, then FP64 refinement (R = B - A X
  * in FP64, correction solved with the FP32 factors, added in FP64) until the
  * normwise backward error eta = max|R| / (||A||_inf max|X| + max|B|) <= tol.
- * A system whose eta stops halving is stalled; stalled systems, FP32 zero
- * pivots and systems still refining after max_iter corrections are
- * refactored and solved in FP64. Per system: berr (final eta), ferr
+ * A system is stalled when its eta stops decreasing, or when the contraction
+ * it has shown cannot bring eta to tol within the corrections left; stalled
+ * systems, FP32 zero pivots and systems still refining after max_iter
+ * corrections are refactored and solved in FP64. Per system: berr (final eta), ferr
  * (max|X - Xtrue| / max|Xtrue|, when Xtrue is given), iters (corrections
  * applied), fallback (1 = the FP64 solve ran), info (of the FP64 solve, when
  * it ran). Orders <= 32 always take the FP64 warp kernel (fallback = 1). The

@@ -11,6 +11,8 @@
 //  k_residual     R = B - A X in FP64 and r * R in FP32 for the next correction
 //  k_refine_decide eta = max|R| / (||A||_inf max|X| + max|B|) (normwise
 //                 backward error) and the convergence / stall decision
+//                 (stalled: the contraction shown cannot reach tol in the
+//                 corrections left)
 //  k_ferr         forward error max|X - Xtrue| / max|Xtrue| when Xtrue is known
 #include <cfloat>
 #include <cmath>
@@ -245,9 +247,13 @@ k_residual(const double* __restrict__ A, const double* __restrict__ B, const dou
 
 // eta = max|R| / (||A||_inf max|X| + max|B|) per system; with decide, the
 // convergence / stall decision and the count of systems still refining.
+// A system is stalled when eta stops decreasing (or is NaN), or when the
+// contraction it has shown, rho = eta / previous eta, cannot bring eta down
+// to tol within the corrections left (log(tol / eta) / log(rho) of them):
+// slow but steady convergence continues, hopeless refinement stops at once.
 // Clears the running maxima for the next residual pass.
-__global__ void k_refine_decide(RefineState* __restrict__ st, int count, double tol, int iter, int decide,
-                                int* __restrict__ active) {
+__global__ void k_refine_decide(RefineState* __restrict__ st, int count, double tol, int iter, int max_iter,
+                                int decide, int* __restrict__ active) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= count) return;
   RefineState& q = st[s];
@@ -260,10 +266,15 @@ __global__ void k_refine_decide(RefineState* __restrict__ st, int count, double 
   q.eta = eta;
   if (!decide) return;
   q.iters = iter;
+  bool stalled = false;
+  if (!(eta <= tol) && iter > 0) {
+    const double rho = eta / q.prev;
+    stalled = !(rho < 1.0) || log(tol / eta) / log(rho) > (double)(max_iter - iter);
+  }
   if (eta <= tol) {
     q.status = kRefineConverged;
-  } else if (iter > 0 && !(eta <= 0.5 * q.prev)) {
-    q.status = kRefineStalled;  // not halving any more (or NaN): refinement has stalled
+  } else if (stalled || !(eta == eta)) {
+    q.status = kRefineStalled;
   } else {
     atomicAdd(active, 1);
   }
@@ -344,7 +355,7 @@ cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, 
 }
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
                            const double* rs, float* R32, const int32_t* rpos, RefineState* st, double tol,
-                           int iter, int decide, int* active, cudaStream_t s) {
+                           int iter, int max_iter, int decide, int* active, cudaStream_t s) {
   const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
   if (nrhs == 1) k_residual<1><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
   else if (nrhs == 2) k_residual<2><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
@@ -352,7 +363,7 @@ cudaError_t mixed_residual(const double* A, const double* B, const double* X, in
   else k_residual<8><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  k_refine_decide<<<(count + 255) / 256, 256, 0, s>>>(st, count, tol, iter, decide, active);
+  k_refine_decide<<<(count + 255) / 256, 256, 0, s>>>(st, count, tol, iter, max_iter, decide, active);
   return cudaGetLastError();
 }
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,

@@ -187,20 +187,26 @@ struct DiagCtx {
   int tid, i, ph, lane, warp;
 };
 
-// Step KK of the diagonal factorisation (a compile-time column, so that every
-// register index below is static).
-template <int KK>
-__device__ __forceinline__ void diag_step(const DiagCtx& c, float (&a)[32], float (&l)[32], bool& chosen, int& pos,
-                                          float& ukp, float& rpiv) {
-  constexpr int kq = KK >> 2, kph = KK & 3, b = KK & 1;
+// Step KK = 4 kq + KPH of the diagonal factorisation. kq is a runtime value
+// (one compact loop body, which the instruction cache holds) and KPH a
+// compile-time phase; registers are indexed by compile-time q only (runtime
+// comparisons with kq select), and 4-column groups that the step cannot touch
+// are skipped by warp-uniform branches.
+template <int KPH>
+__device__ __forceinline__ void diag_step(const DiagCtx& c, int kq, float (&a)[32], float (&l)[32], bool& chosen,
+                                          int& pos, float& ukp, float& rpiv) {
+  constexpr int b = KPH & 1;  // 4 kq is even: the buffer parity of step KK
   constexpr unsigned FULL = 0xffffffffu;
+  const int KK = 4 * kq + KPH;
   const int tid = c.tid, i = c.i, ph = c.ph;
   float* cand = c.big + b * (DW * 256);
   float* xr = c.xrow + b * kMxNB;
   float* Yu = c.Yu;
+  // previous column (KK - 1) as (group pq, phase pph)
+  const int pq = KPH ? kq : kq - 1;
+  constexpr int pph = KPH ? KPH - 1 : 3;
   // finish row KK-1 of U^-T and publish it
   if (KK > 0 && i == KK - 1) {
-    constexpr int pq = (KK - 1) >> 2, pph = (KK - 1) & 3;
 #pragma unroll
     for (int q = 0; q < 32; ++q) {
       if (q < pq || (q == pq && ph <= pph)) {
@@ -211,7 +217,10 @@ __device__ __forceinline__ void diag_step(const DiagCtx& c, float (&a)[32], floa
     }
   }
   // this warp's candidate: the largest |A[i][KK]| among rows not chosen yet
-  const float aik = __shfl_sync(FULL, a[kq], (c.lane & ~3) | kph);
+  float akq = a[0];
+#pragma unroll
+  for (int q = 1; q < 32; ++q) akq = q == kq ? a[q] : akq;
+  const float aik = __shfl_sync(FULL, akq, (c.lane & ~3) | KPH);
   const uint32_t key = chosen ? 0u : __float_as_uint(fabsf(aik)) + 1u;
   const uint32_t wmax = __reduce_max_sync(FULL, key);
   const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)i : 0xffffffffu);
@@ -229,62 +238,65 @@ __device__ __forceinline__ void diag_step(const DiagCtx& c, float (&a)[32], floa
     }
   }
   __syncthreads();
-  // the block's winner: largest key, lowest row on ties
-  uint32_t bk = 0u, br = 0xffffffffu;
-  int bw = 0;
-#pragma unroll
-  for (int w = 0; w < DW; ++w) {
-    const uint32_t kw = c.keys[(b * DW + w) * 2], rw = c.keys[(b * DW + w) * 2 + 1];
-    if (kw > bk || (kw == bk && rw < br)) {
-      bk = kw;
-      br = rw;
-      bw = w;
-    }
-  }
-  const float* wa = cand + bw * 256;
+  // the block's winner: largest key, lowest row on ties (rows of warp w are 8w..8w+7)
+  const uint32_t kw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2] : 0u;
+  const uint32_t rw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2 + 1] : 0xffffffffu;
+  const uint32_t bk = __reduce_max_sync(FULL, kw);
+  const uint32_t br = __reduce_min_sync(FULL, kw == bk ? rw : 0xffffffffu);
+  const float* wa = cand + (br >> 3) * 256;
   const float* wl = wa + kMxNB;
-  const float piv = wa[kph * 32 + kq];
+  const float piv = wa[KPH * 32 + kq];
   if (tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
   // U^-T, one step behind: positions p >= KK take row KK-1
   if (KK > 0 && i >= KK) {
-    constexpr int pq = (KK - 1) >> 2, pph = (KK - 1) & 3;
 #pragma unroll
-    for (int q = 0; q < 32; ++q)
-      if (q < pq || (q == pq && ph <= pph)) Yu[q * DT + tid] = fmaf(-ukp, xr[ph * 32 + q], Yu[q * DT + tid]);
+    for (int g = 0; g < 8; ++g) {
+      if (4 * g <= pq) {
+        const float4 x4 = *reinterpret_cast<const float4*>(xr + ph * 32 + 4 * g);
+        const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int q = 4 * g + e;
+          if (q < pq || (q == pq && ph <= pph)) Yu[q * DT + tid] = fmaf(-ukp, xv[e], Yu[q * DT + tid]);
+        }
+      }
+    }
   }
   ukp = wa[(i & 3) * 32 + (i >> 2)];  // U[KK][i], for position i's update at the next step
   rpiv = 1.0f / piv;
   if ((uint32_t)i == br) {
     chosen = true;
     pos = KK;
-    if (ph == kph) l[kq] = 1.f;
+#pragma unroll
+    for (int q = 0; q < 32; ++q)
+      if (q == kq && ph == KPH) l[q] = 1.f;
   } else if (!chosen) {
     const float lik = aik / piv;
 #pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      if (q > kq || (q == kq && ph > kph)) a[q] = fmaf(-lik, wa[ph * 32 + q], a[q]);
-      if (q < kq || (q == kq && ph < kph)) l[q] = fmaf(-lik, wl[ph * 32 + q], l[q]);
-      if (q == kq && ph == kph) {
-        a[q] = lik;
-        l[q] = -lik;
+    for (int g = 0; g < 8; ++g) {
+      if (4 * g + 3 >= kq) {  // columns >= KK of A
+        const float4 w4 = *reinterpret_cast<const float4*>(wa + ph * 32 + 4 * g);
+        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int q = 4 * g + e;
+          if (q > kq || (q == kq && ph > KPH)) a[q] = fmaf(-lik, wv[e], a[q]);
+          if (q == kq && ph == KPH) a[q] = lik;
+        }
+      }
+      if (4 * g <= kq) {  // columns <= KK of L^-1
+        const float4 w4 = *reinterpret_cast<const float4*>(wl + ph * 32 + 4 * g);
+        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int q = 4 * g + e;
+          if (q < kq || (q == kq && ph < KPH)) l[q] = fmaf(-lik, wv[e], l[q]);
+          if (q == kq && ph == KPH) l[q] = -lik;
+        }
       }
     }
   }
 }
-
-template <int KK>
-struct DiagSteps {
-  static __device__ __forceinline__ void run(const DiagCtx& c, float (&a)[32], float (&l)[32], bool& chosen,
-                                             int& pos, float& ukp, float& rpiv) {
-    diag_step<KK>(c, a, l, chosen, pos, ukp, rpiv);
-    DiagSteps<KK + 1>::run(c, a, l, chosen, pos, ukp, rpiv);
-  }
-};
-template <>
-struct DiagSteps<kMxNB> {
-  static __device__ __forceinline__ void run(const DiagCtx&, float (&)[32], float (&)[32], bool&, int&, float&,
-                                             float&) {}
-};
 
 __global__ void __launch_bounds__(DT, 1)
 k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
@@ -312,7 +324,13 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   if (tid == 0) fail = 0;
   __syncthreads();
   const DiagCtx ctx{Yu, big, xrow, keys, &fail, tid, i, ph, tid & 31, tid >> 5};
-  DiagSteps<0>::run(ctx, a, l, chosen, pos, ukp, rpiv);
+#pragma unroll 1
+  for (int kq = 0; kq < 32; ++kq) {
+    diag_step<0>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
+    diag_step<1>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
+    diag_step<2>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
+    diag_step<3>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
+  }
   if (i == kMxNB - 1) {  // the last row of U^-T
 #pragma unroll
     for (int q = 0; q < 32; ++q) Yu[q * DT + tid] *= rpiv;
@@ -681,6 +699,18 @@ __device__ __forceinline__ void panel_apply(const float* __restrict__ Ms, int N,
   }
 }
 
+// Bring rows [r0, r1) x columns [c0, c0 + 128) of M (4 lines of 128 bytes a
+// row) and a 128 x 128 block inverse into L2 ahead of the block step that
+// reads them: those loads do not depend on the solution being computed, so
+// the next step finds them in L2 instead of waiting on HBM.
+__device__ __forceinline__ void prefetch_step(const float* Ms, int N, int c0, int r0, int r1, const float* D,
+                                              int tid) {
+  const int lines = (r1 > r0 ? r1 - r0 : 0) * 4;
+  for (int idx = tid; idx < lines; idx += ST)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(Ms + (int64_t)(r0 + (idx >> 2)) * N + c0 + 32 * (idx & 3)));
+  for (int idx = tid; idx < kMxNB * kMxNB / 32; idx += ST) asm volatile("prefetch.global.L2 [%0];" ::"l"(D + 32 * idx));
+}
+
 template <int W>
 __global__ void __launch_bounds__(ST, 1)
 k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const float* __restrict__ Uinv,
@@ -702,6 +732,8 @@ k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const flo
   const float* Us = Uinv + (int64_t)s * N * kMxNB;
   for (int k = 0; k < nb; ++k) {  // L y = P c, block by block
     const int K = k * kMxNB;
+    if (k + 1 < nb) prefetch_step(Ms, N, K + kMxNB, K + 2 * kMxNB, N, Ls + (int64_t)(K + kMxNB) * kMxNB, tid);
+    else prefetch_step(Ms, N, K, 0, K, Us + (int64_t)K * kMxNB, tid);  // the back substitution's first step
     block_apply<W>(Ls + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
     __syncthreads();
     for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];
@@ -711,6 +743,7 @@ k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const flo
   }
   for (int k = nb - 1; k >= 0; --k) {  // U x = y
     const int K = k * kMxNB;
+    if (k > 0) prefetch_step(Ms, N, K - kMxNB, 0, K - kMxNB, Us + (int64_t)(K - kMxNB) * kMxNB, tid);
     block_apply<W>(Us + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
     __syncthreads();
     for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];

@@ -130,7 +130,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
       NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
       // the scaled residual lands in b32 (row order of A)
       NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), nullptr, S, tol, it,
-                               1, act.as<int>(), st),
+                               max_iter, 1, act.as<int>(), st),
                 "residual");
       NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
       NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
@@ -180,7 +180,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
       NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
       // the scaled residual lands in y32 already in pivoted row order
       NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), y32.as<float>(), rpos.as<int32_t>(), S,
-                               tol, it, 1, act.as<int>(), st),
+                               tol, it, max_iter, 1, act.as<int>(), st),
                 "residual");
       NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
       NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
@@ -238,7 +238,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     for (size_t q = 0; q < k; ++q) hinfo[idx[q]] = cinfo[q];
   }
   // final backward error of every system, whatever path produced it
-  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, 0, 0,
+  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, 0, max_iter, 0,
                            act.as<int>(), st),
             "residual");
   if (dFerr && dXtrue) NPPB_CUDA(mixed_ferr(dX, dXtrue, count, n, nrhs, dFerr, st), "forward error");

@@ -37,11 +37,12 @@ cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const d
                             RefineState* st, cudaStream_t s);
 cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, int n, int nrhs,
                         const RefineState* st, int init, cudaStream_t s);
-// decide = 1: update status / iters and count the still-active systems into *active.
+// decide = 1: update status / iters and count the still-active systems into *active
+// (a system is stalled when its contraction cannot reach tol in max_iter - iter corrections).
 // R32 (optional): r * R in FP32, row i stored at row rpos[i] (the pivoted order) when rpos is given.
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
                            const double* rs, float* R32, const int32_t* rpos, RefineState* st, double tol,
-                           int iter, int decide, int* active, cudaStream_t s);
+                           int iter, int max_iter, int decide, int* active, cudaStream_t s);
 // rpos[s*n + i] = position of row i after the swaps of ipiv (s*n .. s*n+n-1).
 cudaError_t mixed_row_positions(const int32_t* ipiv, int count, int n, int32_t* rpos, cudaStream_t s);
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,
