@@ -8,9 +8,9 @@
 //                  one quad of M.
 //  k_mx_transpose  the first block's panel row, transposed (A12^T).
 //  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
-//                  among its own rows, with L^-1 P and U^-T from the same row
-//                  operations (one CTA, 4 threads per row, the row in
-//                  registers, one barrier per column).
+//                  among its own rows (one CTA, 4 threads per row, the row in
+//                  registers, one barrier per column), then L^-1 P, U^-1 and
+//                  U^-T by blocked inversion in shared memory.
 //  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
 //                  by TMA in 128-byte-swizzled boxes (two stages of 32-column
 //                  chunks), split into TF32 hi / lo in shared memory, one
@@ -157,66 +157,46 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 
 // ---------------------------------------------------------------------------
 // Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
-// (L^-1 P) and U^-T.
+// then (L^-1 P), U^-1 and U^-T.
 //
-// Thread t owns physical row i = t / 4 of the block (original order), columns
-// j = ph + 4q (ph = t % 4, q = 0..31): the row of A (becoming multipliers and
-// U) and the row's L^-1 in position space, both in registers; and row p = i
-// (a position) of the running U^-T in shared memory (thread-private column of
-// Yu). Step k: each warp proposes its largest |A[i][k]| among rows not yet
-// chosen (lowest row on ties) and publishes that row; after one barrier every
-// thread picks the block's winner, which takes position k; every row not yet
-// chosen takes l = A[i][k] / U[k][k] and updates A[i][k+1:] -= l U[k][k+1:],
-// Linv[i][:k] -= l Linv_w[:k], Linv[i][k] = -l (Gauss elimination of [A | I]
-// in position space gives L^-1). U^-T runs one step behind: row k-1 of it is
-// Y[k-1] / U[k-1][k-1] once step k-1's update is in, published before step
-// k's barrier and applied after it, Y[p] -= U[k-1][p] U^-T[k-1] for p >= k.
+// LU: thread t owns physical row i = t / 4 of the block (original order),
+// columns j = ph + 4q (ph = t % 4, q = 0..31), in registers. Step k: each
+// warp proposes its largest |A[i][k]| among rows not yet chosen (lowest row
+// on ties) and publishes that row; after one barrier every thread picks the
+// block's winner, which takes position k, and every row not yet chosen takes
+// l = A[i][k] / U[k][k] and updates A[i][k+1:] -= l U[k][k+1:]. The step
+// index k = 4 kq + phase has a runtime kq and a compile-time phase (a compact
+// loop the instruction cache holds); 4-column groups right of k are updated
+// without predicates, the one group holding k with them.
+// Inverses, from the packed factors in shared memory (position order): the
+// eight 32 x 32 diagonal blocks of L and U inverted by one warp each (lane =
+// column, substitution down / up the block), then two levels of block
+// products, [L00 0; L10 L11]^-1 = [L00^-1 0; -L11^-1 L10 L00^-1 L11^-1] and
+// [U00 U01; 0 U11]^-1 = [U00^-1 -U00^-1 U01 U11^-1; 0 U11^-1], as 32^3 and
+// 64^3 shared-memory GEMMs (temporaries in the quadrants the results leave
+// zero, and at the last level in the factors' diagonal quadrants).
 // Out: the packed LU of P A11 in M, L^-1 P (the permutation folded into the
 // stored inverse, so that U12 = (L^-1 P) A12 and the forward substitution
 // need no row exchanges), U^-1 and U^-T.
 constexpr int DT = 512, DW = DT / 32;
-constexpr size_t kDiagSmem = sizeof(float) * (32 * DT + kMxNB * kMxNB + 2 * kMxNB) +
-                             sizeof(uint32_t) * (2 * DW * 2) + sizeof(int) * kMxNB;
+constexpr int DLD = 132;  // leading dimension of the shared 128 x 128 arrays (16-byte rows, 4-bank row offset)
+constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(uint32_t) * (2 * DW * 2) +
+                             sizeof(int) * kMxNB;
 
 struct DiagCtx {
-  float* Yu;
-  float* big;
-  float* xrow;
+  float* cand;  // [2][DW][128] candidate rows
   uint32_t* keys;
   int* fail;
   int tid, i, ph, lane, warp;
 };
 
-// Step KK = 4 kq + KPH of the diagonal factorisation. kq is a runtime value
-// (one compact loop body, which the instruction cache holds) and KPH a
-// compile-time phase; registers are indexed by compile-time q only (runtime
-// comparisons with kq select), and 4-column groups that the step cannot touch
-// are skipped by warp-uniform branches.
 template <int KPH>
-__device__ __forceinline__ void diag_step(const DiagCtx& c, int kq, float (&a)[32], float (&l)[32], bool& chosen,
-                                          int& pos, float& ukp, float& rpiv) {
+__device__ __forceinline__ void lu_step(const DiagCtx& c, int kq, float (&a)[32], bool& chosen, int& pos) {
   constexpr int b = KPH & 1;  // 4 kq is even: the buffer parity of step KK
   constexpr unsigned FULL = 0xffffffffu;
   const int KK = 4 * kq + KPH;
-  const int tid = c.tid, i = c.i, ph = c.ph;
-  float* cand = c.big + b * (DW * 256);
-  float* xr = c.xrow + b * kMxNB;
-  float* Yu = c.Yu;
-  // previous column (KK - 1) as (group pq, phase pph)
-  const int pq = KPH ? kq : kq - 1;
-  constexpr int pph = KPH ? KPH - 1 : 3;
-  // finish row KK-1 of U^-T and publish it
-  if (KK > 0 && i == KK - 1) {
-#pragma unroll
-    for (int q = 0; q < 32; ++q) {
-      if (q < pq || (q == pq && ph <= pph)) {
-        const float x = Yu[q * DT + tid] * rpiv;
-        Yu[q * DT + tid] = x;
-        xr[ph * 32 + q] = x;
-      }
-    }
-  }
-  // this warp's candidate: the largest |A[i][KK]| among rows not chosen yet
+  const int i = c.i, ph = c.ph;
+  float* cand = c.cand + b * (DW * kMxNB);
   float akq = a[0];
 #pragma unroll
   for (int q = 1; q < 32; ++q) akq = q == kq ? a[q] : akq;
@@ -225,13 +205,9 @@ __device__ __forceinline__ void diag_step(const DiagCtx& c, int kq, float (&a)[3
   const uint32_t wmax = __reduce_max_sync(FULL, key);
   const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)i : 0xffffffffu);
   if ((uint32_t)i == wrow) {
-    float4* ca = reinterpret_cast<float4*>(cand + c.warp * 256 + ph * 32);
-    float4* cl = reinterpret_cast<float4*>(cand + c.warp * 256 + kMxNB + ph * 32);
+    float4* ca = reinterpret_cast<float4*>(cand + c.warp * kMxNB + ph * 32);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      ca[v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
-      if (4 * v <= kq) cl[v] = make_float4(l[4 * v], l[4 * v + 1], l[4 * v + 2], l[4 * v + 3]);
-    }
+    for (int v = 0; v < 8; ++v) ca[v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
     if (ph == 0) {
       c.keys[(b * DW + c.warp) * 2] = wmax;
       c.keys[(b * DW + c.warp) * 2 + 1] = wrow;
@@ -243,39 +219,24 @@ __device__ __forceinline__ void diag_step(const DiagCtx& c, int kq, float (&a)[3
   const uint32_t rw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2 + 1] : 0xffffffffu;
   const uint32_t bk = __reduce_max_sync(FULL, kw);
   const uint32_t br = __reduce_min_sync(FULL, kw == bk ? rw : 0xffffffffu);
-  const float* wa = cand + (br >> 3) * 256;
-  const float* wl = wa + kMxNB;
-  const float piv = wa[KPH * 32 + kq];
-  if (tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
-  // U^-T, one step behind: positions p >= KK take row KK-1
-  if (KK > 0 && i >= KK) {
-#pragma unroll
-    for (int g = 0; g < 8; ++g) {
-      if (4 * g <= pq) {
-        const float4 x4 = *reinterpret_cast<const float4*>(xr + ph * 32 + 4 * g);
-        const float xv[4] = {x4.x, x4.y, x4.z, x4.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int q = 4 * g + e;
-          if (q < pq || (q == pq && ph <= pph)) Yu[q * DT + tid] = fmaf(-ukp, xv[e], Yu[q * DT + tid]);
-        }
-      }
-    }
-  }
-  ukp = wa[(i & 3) * 32 + (i >> 2)];  // U[KK][i], for position i's update at the next step
-  rpiv = 1.0f / piv;
+  const float* wa = cand + (br >> 3) * kMxNB + ph * 32;
+  const float piv = cand[(br >> 3) * kMxNB + KPH * 32 + kq];
+  if (c.tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
   if ((uint32_t)i == br) {
     chosen = true;
     pos = KK;
-#pragma unroll
-    for (int q = 0; q < 32; ++q)
-      if (q == kq && ph == KPH) l[q] = 1.f;
   } else if (!chosen) {
     const float lik = aik / piv;
 #pragma unroll
     for (int g = 0; g < 8; ++g) {
-      if (4 * g + 3 >= kq) {  // columns >= KK of A
-        const float4 w4 = *reinterpret_cast<const float4*>(wa + ph * 32 + 4 * g);
+      if (4 * g > kq) {
+        const float4 w4 = *reinterpret_cast<const float4*>(wa + 4 * g);
+        a[4 * g] = fmaf(-lik, w4.x, a[4 * g]);
+        a[4 * g + 1] = fmaf(-lik, w4.y, a[4 * g + 1]);
+        a[4 * g + 2] = fmaf(-lik, w4.z, a[4 * g + 2]);
+        a[4 * g + 3] = fmaf(-lik, w4.w, a[4 * g + 3]);
+      } else if (4 * g + 3 >= kq) {
+        const float4 w4 = *reinterpret_cast<const float4*>(wa + 4 * g);
         const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -284,73 +245,138 @@ __device__ __forceinline__ void diag_step(const DiagCtx& c, int kq, float (&a)[3
           if (q == kq && ph == KPH) a[q] = lik;
         }
       }
-      if (4 * g <= kq) {  // columns <= KK of L^-1
-        const float4 w4 = *reinterpret_cast<const float4*>(wl + ph * 32 + 4 * g);
-        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int q = 4 * g + e;
-          if (q < kq || (q == kq && ph < KPH)) l[q] = fmaf(-lik, wv[e], l[q]);
-          if (q == kq && ph == KPH) l[q] = -lik;
-        }
-      }
     }
   }
+}
+
+// Inverse of one 32 x 32 diagonal block of the packed factors at (o, o), one
+// warp, lane = column: unit lower (L) by substitution down, upper (U) up.
+__device__ __forceinline__ void inv_lower32(const float* LU, float* Li, int o, int lane) {
+  float x[32];
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    float s = r == lane ? 1.f : 0.f;
+#pragma unroll
+    for (int m = 0; m < r; ++m) s = fmaf(-LU[(o + r) * DLD + o + m], x[m], s);
+    x[r] = s;
+  }
+#pragma unroll
+  for (int r = 0; r < 32; ++r) Li[(o + r) * DLD + o + lane] = x[r];
+}
+__device__ __forceinline__ void inv_upper32(const float* LU, float* Ui, int o, int lane) {
+  float x[32];
+#pragma unroll
+  for (int r = 31; r >= 0; --r) {
+    float s = r == lane ? 1.f : 0.f;
+#pragma unroll
+    for (int m = r + 1; m < 32; ++m) s = fmaf(-LU[(o + r) * DLD + o + m], x[m], s);
+    x[r] = s / LU[(o + r) * DLD + o + r];
+  }
+#pragma unroll
+  for (int r = 0; r < 32; ++r) Ui[(o + r) * DLD + o + lane] = x[r];
+}
+
+// C = alpha A B for S x S blocks of the shared arrays (leading dimension DLD),
+// thread t of a group of (S/TM) * (S/4) threads computing TM x 4 outputs.
+template <int S, int TM>
+__device__ __forceinline__ void sgemm(const float* A, const float* B, float* C, float alpha, int t) {
+  constexpr int CG = S / 4;
+  const int r0 = (t / CG) * TM, c0 = (t % CG) * 4;
+  float acc[TM][4];
+#pragma unroll
+  for (int r = 0; r < TM; ++r)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[r][j] = 0.f;
+#pragma unroll 8
+  for (int k = 0; k < S; ++k) {
+    const float4 bv = *reinterpret_cast<const float4*>(B + k * DLD + c0);
+#pragma unroll
+    for (int r = 0; r < TM; ++r) {
+      const float av = A[(r0 + r) * DLD + k];
+      acc[r][0] = fmaf(av, bv.x, acc[r][0]);
+      acc[r][1] = fmaf(av, bv.y, acc[r][1]);
+      acc[r][2] = fmaf(av, bv.z, acc[r][2]);
+      acc[r][3] = fmaf(av, bv.w, acc[r][3]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < TM; ++r)
+    *reinterpret_cast<float4*>(C + (r0 + r) * DLD + c0) =
+        make_float4(alpha * acc[r][0], alpha * acc[r][1], alpha * acc[r][2], alpha * acc[r][3]);
 }
 
 __global__ void __launch_bounds__(DT, 1)
 k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
           int32_t* __restrict__ info, int N, int k) {
   extern __shared__ __align__(16) float dsm[];
-  float* Yu = dsm;                              // [32][DT]
-  float* big = Yu + 32 * DT;                    // loop: [2][DW][256] candidate rows; after: [128][128] L^-1 by position
-  float* xrow = big + kMxNB * kMxNB;            // [2][128]: finished row of U^-T, [ph][q] layout
-  uint32_t* keys = reinterpret_cast<uint32_t*>(xrow + 2 * kMxNB);  // [2][DW][2]: key, row
+  float* LU = dsm;                       // [128][DLD] packed factors, position order
+  float* Li = LU + kMxNB * DLD;          // [128][DLD] L^-1 (position order); the loop's candidate rows first
+  float* Ui = Li + kMxNB * DLD;          // [128][DLD] U^-1
+  uint32_t* keys = reinterpret_cast<uint32_t*>(Ui + kMxNB * DLD);  // [2][DW][2]: key, row
   int* posOf = reinterpret_cast<int*>(keys + 4 * DW);             // [128]
   __shared__ int fail;
-  const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x;
+  const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int i = tid >> 2, ph = tid & 3;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
-  float a[32], l[32];
+  float a[32];
 #pragma unroll
-  for (int q = 0; q < 32; ++q) {
-    a[q] = Mb[(int64_t)i * N + ph + 4 * q];
-    l[q] = 0.f;
-    Yu[q * DT + tid] = (i == ph + 4 * q) ? 1.f : 0.f;
-  }
+  for (int q = 0; q < 32; ++q) a[q] = Mb[(int64_t)i * N + ph + 4 * q];
   bool chosen = false;
   int pos = 0;
-  float ukp = 0.f, rpiv = 1.f;
   if (tid == 0) fail = 0;
   __syncthreads();
-  const DiagCtx ctx{Yu, big, xrow, keys, &fail, tid, i, ph, tid & 31, tid >> 5};
+  const DiagCtx ctx{Li, keys, &fail, tid, i, ph, lane, warp};
 #pragma unroll 1
   for (int kq = 0; kq < 32; ++kq) {
-    diag_step<0>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
-    diag_step<1>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
-    diag_step<2>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
-    diag_step<3>(ctx, kq, a, l, chosen, pos, ukp, rpiv);
+    lu_step<0>(ctx, kq, a, chosen, pos);
+    lu_step<1>(ctx, kq, a, chosen, pos);
+    lu_step<2>(ctx, kq, a, chosen, pos);
+    lu_step<3>(ctx, kq, a, chosen, pos);
   }
-  if (i == kMxNB - 1) {  // the last row of U^-T
-#pragma unroll
-    for (int q = 0; q < 32; ++q) Yu[q * DT + tid] *= rpiv;
-  }
-  __syncthreads();  // the candidate buffers are free: L^-1 by position goes there
+  // the packed factors by position: to M (the stored factorisation) and to shared memory
   if (ph == 0) posOf[i] = pos;
 #pragma unroll
   for (int q = 0; q < 32; ++q) {
-    big[pos * kMxNB + ph + 4 * q] = l[q];
     Mb[(int64_t)pos * N + ph + 4 * q] = a[q];
+    LU[pos * DLD + ph + 4 * q] = a[q];
   }
+  __syncthreads();  // the candidate rows are dead: zero both inverses
+  for (int idx = tid; idx < 2 * kMxNB * DLD; idx += DT) Li[idx] = 0.f;
   __syncthreads();
+  // level 1: the eight 32 x 32 diagonal blocks
+  if (warp < 4) inv_lower32(LU, Li, 32 * warp, lane);
+  else if (warp < 8) inv_upper32(LU, Ui, 32 * (warp - 4), lane);
+  __syncthreads();
+  // level 2: 64 x 64 diagonal quadrants; four chains of 128 threads
+  {
+    const int ch = tid >> 7, t = tid & 127, p = ch & 1, o = 64 * p;
+    float* tL = Li + (32 * p) * DLD + 64;        // temporaries in Li's upper-right quadrant
+    float* tU = Ui + (64 + 32 * p) * DLD;        //   ... and Ui's lower-left quadrant
+    if (ch < 2) sgemm<32, 2>(LU + (o + 32) * DLD + o, Li + o * DLD + o, tL, 1.f, t);
+    else sgemm<32, 2>(LU + o * DLD + o + 32, Ui + (o + 32) * DLD + o + 32, tU, 1.f, t);
+    __syncthreads();
+    if (ch < 2) sgemm<32, 2>(Li + (o + 32) * DLD + o + 32, tL, Li + (o + 32) * DLD + o, -1.f, t);
+    else sgemm<32, 2>(Ui + o * DLD + o, tU, Ui + o * DLD + o + 32, -1.f, t);
+    __syncthreads();
+  }
+  // level 3: the off-diagonal quadrants; two chains of 256 threads, temporaries in LU's diagonal quadrants
+  {
+    const int ch = tid >> 8, t = tid & 255;
+    if (ch == 0) sgemm<64, 4>(LU + 64 * DLD, Li, LU, 1.f, t);
+    else sgemm<64, 4>(LU + 64, Ui + 64 * DLD + 64, LU + 64 * DLD + 64, 1.f, t);
+    __syncthreads();
+    if (ch == 0) sgemm<64, 4>(Li + 64 * DLD + 64, LU, Li + 64 * DLD, -1.f, t);
+    else sgemm<64, 4>(Ui, LU + 64 * DLD + 64, Ui + 64, -1.f, t);
+    __syncthreads();
+  }
   float* Lb = Linv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   float* Ub = Uinv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   float* UTb = UinvT + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   for (int idx = tid; idx < kMxNB * kMxNB; idx += DT) {
-    const int r = idx >> 7, c = idx & 127;
-    Lb[idx] = big[r * kMxNB + posOf[c]];              // (L^-1 P)[r][c]
-    UTb[idx] = Yu[(c >> 2) * DT + 4 * r + (c & 3)];   // U^-T[r][c]
-    Ub[idx] = Yu[(r >> 2) * DT + 4 * c + (r & 3)];    // U^-1[r][c] = U^-T[c][r]
+    const int r = idx >> 7, c = idx & 127, pc = posOf[c];
+    Lb[idx] = pc <= r ? Li[r * DLD + pc] : 0.f;      // (L^-1 P)[r][c]
+    Ub[idx] = c >= r ? Ui[r * DLD + c] : 0.f;        // U^-1[r][c]
+    UTb[idx] = r >= c ? Ui[c * DLD + r] : 0.f;       // U^-T[r][c]
   }
   if (tid == 0 && fail && info[s] == 0) info[s] = K + fail;
 }
