@@ -8,7 +8,7 @@
 //                  one quad of M.
 //  k_mx_transpose  the first block's panel row, transposed (A12^T).
 //  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
-//                  among its own rows (one CTA, 4 threads per row, the row in
+//                  among its own rows (one CTA, 2 threads per row, the row in
 //                  registers, one barrier per column), then L^-1 P, U^-1 and
 //                  U^-T by blocked inversion in shared memory.
 //  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
@@ -22,7 +22,7 @@
 //                  right-hand-side chunk, the right-hand sides in shared memory.
 //  k_mx_rhs_in / k_mx_apply   U^T applied to a right-hand side, V and the
 //                  column scales applied to a solution (FP64 accumulation).
-// Every wait on an mbarrier is bounded (a second of %globaltimer): past it the
+// Every wait on an mbarrier is bounded (about a second of SM clock): past it the
 // CTA counts a timeout, skips its stores, releases its TMEM and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -159,15 +159,18 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
 // then (L^-1 P), U^-1 and U^-T.
 //
-// LU: thread t owns physical row i = t / 4 of the block (original order),
-// columns j = ph + 4q (ph = t % 4, q = 0..31), in registers. Step k: each
+// LU: thread t owns physical row i = t / 2 of the block (original order),
+// columns j = ph + 2q (ph = t % 2, q = 0..63), in registers. Step k: each
 // warp proposes its largest |A[i][k]| among rows not yet chosen (lowest row
 // on ties) and publishes that row; after one barrier every thread picks the
 // block's winner, which takes position k, and every row not yet chosen takes
 // l = A[i][k] / U[k][k] and updates A[i][k+1:] -= l U[k][k+1:]. The step
-// index k = 4 kq + phase has a runtime kq and a compile-time phase (a compact
-// loop the instruction cache holds); 4-column groups right of k are updated
-// without predicates, the one group holding k with them.
+// index k = 2 kq + phase has a runtime kq and a compile-time phase (a compact
+// loop); 4-column groups right of k are updated without predicates, the one
+// group holding k with them, and the value in the next step's column is
+// picked out of that group (a 4-way select, not a 64-way one). Candidate rows
+// sit in shared memory as [16-byte piece][owner thread], so the two owners
+// write and every reader reads consecutive pieces (no bank conflicts).
 // Inverses, from the packed factors in shared memory (position order): the
 // eight 32 x 32 diagonal blocks of L and U inverted by one warp each (lane =
 // column, substitution down / up the block), then two levels of block
@@ -178,65 +181,69 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // Out: the packed LU of P A11 in M, L^-1 P (the permutation folded into the
 // stored inverse, so that U12 = (L^-1 P) A12 and the forward substitution
 // need no row exchanges), U^-1 and U^-T.
-constexpr int DT = 512, DW = DT / 32;
+constexpr int DT = 256, DW = DT / 32;
 constexpr int DLD = 132;  // leading dimension of the shared 128 x 128 arrays (16-byte rows, 4-bank row offset)
 constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(uint32_t) * (2 * DW * 2) +
                              sizeof(int) * kMxNB;
 
 struct DiagCtx {
-  float* cand;  // [2][DW][128] candidate rows
+  float* cand;  // [2][DW][128] candidate rows, piece v of owner ph at (2 v + ph) * 4
   uint32_t* keys;
   int* fail;
   int tid, i, ph, lane, warp;
 };
 
+__device__ __forceinline__ float sel4(float a0, float a1, float a2, float a3, int e) {
+  return e == 0 ? a0 : e == 1 ? a1 : e == 2 ? a2 : a3;
+}
+
 template <int KPH>
-__device__ __forceinline__ void lu_step(const DiagCtx& c, int kq, float (&a)[32], bool& chosen, int& pos) {
-  constexpr int b = KPH & 1;  // 4 kq is even: the buffer parity of step KK
+__device__ __forceinline__ void lu_step(const DiagCtx& c, int kq, float (&a)[64], float& cur, bool& chosen,
+                                        int& pos) {
+  constexpr int b = KPH;  // 2 kq is even: the buffer parity of step KK is the phase
   constexpr unsigned FULL = 0xffffffffu;
-  const int KK = 4 * kq + KPH;
+  const int KK = 2 * kq + KPH;
   const int i = c.i, ph = c.ph;
   float* cand = c.cand + b * (DW * kMxNB);
-  float akq = a[0];
-#pragma unroll
-  for (int q = 1; q < 32; ++q) akq = q == kq ? a[q] : akq;
-  const float aik = __shfl_sync(FULL, akq, (c.lane & ~3) | KPH);
+  const float aik = __shfl_sync(FULL, cur, (c.lane & ~1) | KPH);
   const uint32_t key = chosen ? 0u : __float_as_uint(fabsf(aik)) + 1u;
   const uint32_t wmax = __reduce_max_sync(FULL, key);
   const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)i : 0xffffffffu);
   if ((uint32_t)i == wrow) {
-    float4* ca = reinterpret_cast<float4*>(cand + c.warp * kMxNB + ph * 32);
+    float4* ca = reinterpret_cast<float4*>(cand + c.warp * kMxNB) + ph;
 #pragma unroll
-    for (int v = 0; v < 8; ++v) ca[v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
+    for (int v = 0; v < 16; ++v) ca[2 * v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
     if (ph == 0) {
       c.keys[(b * DW + c.warp) * 2] = wmax;
       c.keys[(b * DW + c.warp) * 2 + 1] = wrow;
     }
   }
   __syncthreads();
-  // the block's winner: largest key, lowest row on ties (rows of warp w are 8w..8w+7)
+  // the block's winner: largest key, lowest row on ties (rows of warp w are 16w..16w+15)
   const uint32_t kw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2] : 0u;
   const uint32_t rw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2 + 1] : 0xffffffffu;
   const uint32_t bk = __reduce_max_sync(FULL, kw);
   const uint32_t br = __reduce_min_sync(FULL, kw == bk ? rw : 0xffffffffu);
-  const float* wa = cand + (br >> 3) * kMxNB + ph * 32;
-  const float piv = cand[(br >> 3) * kMxNB + KPH * 32 + kq];
+  const float* wrow_s = cand + (br >> 4) * kMxNB;
+  const float piv = wrow_s[((kq >> 2) * 2 + KPH) * 4 + (kq & 3)];
   if (c.tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
+  const int qn = KPH ? kq + 1 : kq;  // this thread's q of column KK + 1
   if ((uint32_t)i == br) {
     chosen = true;
     pos = KK;
   } else if (!chosen) {
     const float lik = aik / piv;
+    const float4* wa = reinterpret_cast<const float4*>(wrow_s) + ph;
 #pragma unroll
-    for (int g = 0; g < 8; ++g) {
+    for (int g = 0; g < 16; ++g) {
       if (4 * g > kq) {
-        const float4 w4 = *reinterpret_cast<const float4*>(wa + 4 * g);
+        const float4 w4 = wa[2 * g];
         a[4 * g] = fmaf(-lik, w4.x, a[4 * g]);
         a[4 * g + 1] = fmaf(-lik, w4.y, a[4 * g + 1]);
         a[4 * g + 2] = fmaf(-lik, w4.z, a[4 * g + 2]);
         a[4 * g + 3] = fmaf(-lik, w4.w, a[4 * g + 3]);
       } else if (4 * g + 3 >= kq) {
-        const float4 w4 = *reinterpret_cast<const float4*>(wa + 4 * g);
+        const float4 w4 = wa[2 * g];
         const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
@@ -245,6 +252,7 @@ __device__ __forceinline__ void lu_step(const DiagCtx& c, int kq, float (&a)[32]
           if (q == kq && ph == KPH) a[q] = lik;
         }
       }
+      if (4 * g <= qn && qn < 4 * g + 4) cur = sel4(a[4 * g], a[4 * g + 1], a[4 * g + 2], a[4 * g + 3], qn & 3);
     }
   }
 }
@@ -316,57 +324,56 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   int* posOf = reinterpret_cast<int*>(keys + 4 * DW);             // [128]
   __shared__ int fail;
   const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int i = tid >> 2, ph = tid & 3;
+  const int i = tid >> 1, ph = tid & 1;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
-  float a[32];
+  float a[64];
 #pragma unroll
-  for (int q = 0; q < 32; ++q) a[q] = Mb[(int64_t)i * N + ph + 4 * q];
+  for (int q = 0; q < 64; ++q) a[q] = Mb[(int64_t)i * N + ph + 2 * q];
+  float cur = a[0];
   bool chosen = false;
   int pos = 0;
   if (tid == 0) fail = 0;
   __syncthreads();
   const DiagCtx ctx{Li, keys, &fail, tid, i, ph, lane, warp};
 #pragma unroll 1
-  for (int kq = 0; kq < 32; ++kq) {
-    lu_step<0>(ctx, kq, a, chosen, pos);
-    lu_step<1>(ctx, kq, a, chosen, pos);
-    lu_step<2>(ctx, kq, a, chosen, pos);
-    lu_step<3>(ctx, kq, a, chosen, pos);
+  for (int kq = 0; kq < 64; ++kq) {
+    lu_step<0>(ctx, kq, a, cur, chosen, pos);
+    lu_step<1>(ctx, kq, a, cur, chosen, pos);
   }
   // the packed factors by position: to M (the stored factorisation) and to shared memory
   if (ph == 0) posOf[i] = pos;
 #pragma unroll
-  for (int q = 0; q < 32; ++q) {
-    Mb[(int64_t)pos * N + ph + 4 * q] = a[q];
-    LU[pos * DLD + ph + 4 * q] = a[q];
+  for (int q = 0; q < 64; ++q) {
+    Mb[(int64_t)pos * N + ph + 2 * q] = a[q];
+    LU[pos * DLD + ph + 2 * q] = a[q];
   }
   __syncthreads();  // the candidate rows are dead: zero both inverses
   for (int idx = tid; idx < 2 * kMxNB * DLD; idx += DT) Li[idx] = 0.f;
   __syncthreads();
   // level 1: the eight 32 x 32 diagonal blocks
   if (warp < 4) inv_lower32(LU, Li, 32 * warp, lane);
-  else if (warp < 8) inv_upper32(LU, Ui, 32 * (warp - 4), lane);
+  else inv_upper32(LU, Ui, 32 * (warp - 4), lane);
   __syncthreads();
-  // level 2: 64 x 64 diagonal quadrants; four chains of 128 threads
+  // level 2: 64 x 64 diagonal quadrants; four chains of 64 threads
   {
-    const int ch = tid >> 7, t = tid & 127, p = ch & 1, o = 64 * p;
+    const int ch = tid >> 6, t = tid & 63, p = ch & 1, o = 64 * p;
     float* tL = Li + (32 * p) * DLD + 64;        // temporaries in Li's upper-right quadrant
     float* tU = Ui + (64 + 32 * p) * DLD;        //   ... and Ui's lower-left quadrant
-    if (ch < 2) sgemm<32, 2>(LU + (o + 32) * DLD + o, Li + o * DLD + o, tL, 1.f, t);
-    else sgemm<32, 2>(LU + o * DLD + o + 32, Ui + (o + 32) * DLD + o + 32, tU, 1.f, t);
+    if (ch < 2) sgemm<32, 4>(LU + (o + 32) * DLD + o, Li + o * DLD + o, tL, 1.f, t);
+    else sgemm<32, 4>(LU + o * DLD + o + 32, Ui + (o + 32) * DLD + o + 32, tU, 1.f, t);
     __syncthreads();
-    if (ch < 2) sgemm<32, 2>(Li + (o + 32) * DLD + o + 32, tL, Li + (o + 32) * DLD + o, -1.f, t);
-    else sgemm<32, 2>(Ui + o * DLD + o, tU, Ui + o * DLD + o + 32, -1.f, t);
+    if (ch < 2) sgemm<32, 4>(Li + (o + 32) * DLD + o + 32, tL, Li + (o + 32) * DLD + o, -1.f, t);
+    else sgemm<32, 4>(Ui + o * DLD + o, tU, Ui + o * DLD + o + 32, -1.f, t);
     __syncthreads();
   }
-  // level 3: the off-diagonal quadrants; two chains of 256 threads, temporaries in LU's diagonal quadrants
+  // level 3: the off-diagonal quadrants; two chains of 128 threads, temporaries in LU's diagonal quadrants
   {
-    const int ch = tid >> 8, t = tid & 255;
-    if (ch == 0) sgemm<64, 4>(LU + 64 * DLD, Li, LU, 1.f, t);
-    else sgemm<64, 4>(LU + 64, Ui + 64 * DLD + 64, LU + 64 * DLD + 64, 1.f, t);
+    const int ch = tid >> 7, t = tid & 127;
+    if (ch == 0) sgemm<64, 8>(LU + 64 * DLD, Li, LU, 1.f, t);
+    else sgemm<64, 8>(LU + 64, Ui + 64 * DLD + 64, LU + 64 * DLD + 64, 1.f, t);
     __syncthreads();
-    if (ch == 0) sgemm<64, 4>(Li + 64 * DLD + 64, LU, Li + 64 * DLD, -1.f, t);
-    else sgemm<64, 4>(Ui, LU + 64 * DLD + 64, Ui + 64, -1.f, t);
+    if (ch == 0) sgemm<64, 8>(Li + 64 * DLD + 64, LU, Li + 64 * DLD, -1.f, t);
+    else sgemm<64, 8>(Ui, LU + 64 * DLD + 64, Ui + 64, -1.f, t);
     __syncthreads();
   }
   float* Lb = Linv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
@@ -406,16 +413,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-__device__ __forceinline__ uint64_t global_ns() {
-  uint64_t t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Bounded wait for phase `parity` of an mbarrier (one second).
+// Bounded wait for phase `parity` of an mbarrier: about a second of the SM's
+// own cycle counter (cheap to read, unlike the global timer).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   uint32_t done = 0;
-  const uint64_t t0 = global_ns();
+  const long long t0 = clock64();
   while (true) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -425,7 +427,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (global_ns() - t0 > 1000000000ull) return false;
+    if (clock64() - t0 > (2ll << 30)) return false;
   }
 }
 

