@@ -8,9 +8,9 @@
 //                  one quad of M.
 //  k_mx_transpose  the first block's panel row, transposed (A12^T).
 //  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
-//                  among its own rows (one CTA, 2 threads per row, the row in
-//                  registers, one barrier per column), then L^-1 P, U^-1 and
-//                  U^-T by blocked inversion in shared memory.
+//                  among its own rows (one CTA, the block in shared memory,
+//                  two barriers per column), then L^-1 P, U^-1 and U^-T by
+//                  blocked inversion in shared memory.
 //  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
 //                  by TMA in 128-byte-swizzled boxes (two stages of 32-column
 //                  chunks), split into TF32 hi / lo in shared memory, one
@@ -159,103 +159,28 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
 // then (L^-1 P), U^-1 and U^-T.
 //
-// LU: thread t owns physical row i = t / 2 of the block (original order),
-// columns j = ph + 2q (ph = t % 2, q = 0..63), in registers. Step k: each
-// warp proposes its largest |A[i][k]| among rows not yet chosen (lowest row
-// on ties) and publishes that row; after one barrier every thread picks the
-// block's winner, which takes position k, and every row not yet chosen takes
-// l = A[i][k] / U[k][k] and updates A[i][k+1:] -= l U[k][k+1:]. The step
-// index k = 2 kq + phase has a runtime kq and a compile-time phase (a compact
-// loop); 4-column groups right of k are updated without predicates, the one
-// group holding k with them, and the value in the next step's column is
-// picked out of that group (a 4-way select, not a 64-way one). Candidate rows
-// sit in shared memory as [16-byte piece][owner thread], so the two owners
-// write and every reader reads consecutive pieces (no bank conflicts).
-// Inverses, from the packed factors in shared memory (position order): the
-// eight 32 x 32 diagonal blocks of L and U inverted by one warp each (lane =
-// column, substitution down / up the block), then two levels of block
-// products, [L00 0; L10 L11]^-1 = [L00^-1 0; -L11^-1 L10 L00^-1 L11^-1] and
-// [U00 U01; 0 U11]^-1 = [U00^-1 -U00^-1 U01 U11^-1; 0 U11^-1], as 32^3 and
-// 64^3 shared-memory GEMMs (temporaries in the quadrants the results leave
-// zero, and at the last level in the factors' diagonal quadrants).
+// LU, in shared memory (row-major, rows swapped as pivots are chosen, so the
+// factors end in position order). Step k: warp 0 finds the first largest
+// |A[i][k]|, i >= k, swaps rows k and p (whole rows: the multipliers already
+// left of k move with them, as in LAPACK's getf2) and scales the column below
+// the diagonal by 1 / A[k][k]; after a barrier all threads update the trailing
+// block A[k+1:, k+1:] -= A[k+1:, k] A[k, k+1:] in 16-byte pieces covering only
+// the active columns (the piece holding column k masked); a second barrier
+// closes the step. The permutation is tracked as the original row of each
+// position.
+// Inverses, from the packed factors: the eight 32 x 32 diagonal blocks of L
+// and U inverted by one warp each (lane = column, substitution down / up the
+// block), then two levels of block products, [L00 0; L10 L11]^-1 =
+// [L00^-1 0; -L11^-1 L10 L00^-1 L11^-1] and [U00 U01; 0 U11]^-1 =
+// [U00^-1 -U00^-1 U01 U11^-1; 0 U11^-1], as 32^3 and 64^3 shared-memory GEMMs
+// (temporaries in the quadrants the results leave zero, and at the last level
+// in the factors' diagonal quadrants).
 // Out: the packed LU of P A11 in M, L^-1 P (the permutation folded into the
 // stored inverse, so that U12 = (L^-1 P) A12 and the forward substitution
 // need no row exchanges), U^-1 and U^-T.
-constexpr int DT = 256, DW = DT / 32;
+constexpr int DT = 256;
 constexpr int DLD = 132;  // leading dimension of the shared 128 x 128 arrays (16-byte rows, 4-bank row offset)
-constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(uint32_t) * (2 * DW * 2) +
-                             sizeof(int) * kMxNB;
-
-struct DiagCtx {
-  float* cand;  // [2][DW][128] candidate rows, piece v of owner ph at (2 v + ph) * 4
-  uint32_t* keys;
-  int* fail;
-  int tid, i, ph, lane, warp;
-};
-
-__device__ __forceinline__ float sel4(float a0, float a1, float a2, float a3, int e) {
-  return e == 0 ? a0 : e == 1 ? a1 : e == 2 ? a2 : a3;
-}
-
-template <int KPH>
-__device__ __forceinline__ void lu_step(const DiagCtx& c, int kq, float (&a)[64], float& cur, bool& chosen,
-                                        int& pos) {
-  constexpr int b = KPH;  // 2 kq is even: the buffer parity of step KK is the phase
-  constexpr unsigned FULL = 0xffffffffu;
-  const int KK = 2 * kq + KPH;
-  const int i = c.i, ph = c.ph;
-  float* cand = c.cand + b * (DW * kMxNB);
-  const float aik = __shfl_sync(FULL, cur, (c.lane & ~1) | KPH);
-  const uint32_t key = chosen ? 0u : __float_as_uint(fabsf(aik)) + 1u;
-  const uint32_t wmax = __reduce_max_sync(FULL, key);
-  const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)i : 0xffffffffu);
-  if ((uint32_t)i == wrow) {
-    float4* ca = reinterpret_cast<float4*>(cand + c.warp * kMxNB) + ph;
-#pragma unroll
-    for (int v = 0; v < 16; ++v) ca[2 * v] = make_float4(a[4 * v], a[4 * v + 1], a[4 * v + 2], a[4 * v + 3]);
-    if (ph == 0) {
-      c.keys[(b * DW + c.warp) * 2] = wmax;
-      c.keys[(b * DW + c.warp) * 2 + 1] = wrow;
-    }
-  }
-  __syncthreads();
-  // the block's winner: largest key, lowest row on ties (rows of warp w are 16w..16w+15)
-  const uint32_t kw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2] : 0u;
-  const uint32_t rw = c.lane < DW ? c.keys[(b * DW + c.lane) * 2 + 1] : 0xffffffffu;
-  const uint32_t bk = __reduce_max_sync(FULL, kw);
-  const uint32_t br = __reduce_min_sync(FULL, kw == bk ? rw : 0xffffffffu);
-  const float* wrow_s = cand + (br >> 4) * kMxNB;
-  const float piv = wrow_s[((kq >> 2) * 2 + KPH) * 4 + (kq & 3)];
-  if (c.tid == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && *c.fail == 0) *c.fail = KK + 1;
-  const int qn = KPH ? kq + 1 : kq;  // this thread's q of column KK + 1
-  if ((uint32_t)i == br) {
-    chosen = true;
-    pos = KK;
-  } else if (!chosen) {
-    const float lik = aik / piv;
-    const float4* wa = reinterpret_cast<const float4*>(wrow_s) + ph;
-#pragma unroll
-    for (int g = 0; g < 16; ++g) {
-      if (4 * g > kq) {
-        const float4 w4 = wa[2 * g];
-        a[4 * g] = fmaf(-lik, w4.x, a[4 * g]);
-        a[4 * g + 1] = fmaf(-lik, w4.y, a[4 * g + 1]);
-        a[4 * g + 2] = fmaf(-lik, w4.z, a[4 * g + 2]);
-        a[4 * g + 3] = fmaf(-lik, w4.w, a[4 * g + 3]);
-      } else if (4 * g + 3 >= kq) {
-        const float4 w4 = wa[2 * g];
-        const float wv[4] = {w4.x, w4.y, w4.z, w4.w};
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int q = 4 * g + e;
-          if (q > kq || (q == kq && ph > KPH)) a[q] = fmaf(-lik, wv[e], a[q]);
-          if (q == kq && ph == KPH) a[q] = lik;
-        }
-      }
-      if (4 * g <= qn && qn < 4 * g + 4) cur = sel4(a[4 * g], a[4 * g + 1], a[4 * g + 2], a[4 * g + 3], qn & 3);
-    }
-  }
-}
+constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(int) * 2 * kMxNB;
 
 // Inverse of one 32 x 32 diagonal block of the packed factors at (o, o), one
 // warp, lane = column: unit lower (L) by substitution down, upper (U) up.
@@ -317,37 +242,89 @@ __global__ void __launch_bounds__(DT, 1)
 k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
           int32_t* __restrict__ info, int N, int k) {
   extern __shared__ __align__(16) float dsm[];
-  float* LU = dsm;                       // [128][DLD] packed factors, position order
-  float* Li = LU + kMxNB * DLD;          // [128][DLD] L^-1 (position order); the loop's candidate rows first
+  float* LU = dsm;                       // [128][DLD] the block, then its packed factors (position order)
+  float* Li = LU + kMxNB * DLD;          // [128][DLD] L^-1 (position order)
   float* Ui = Li + kMxNB * DLD;          // [128][DLD] U^-1
-  uint32_t* keys = reinterpret_cast<uint32_t*>(Ui + kMxNB * DLD);  // [2][DW][2]: key, row
-  int* posOf = reinterpret_cast<int*>(keys + 4 * DW);             // [128]
+  int* orig = reinterpret_cast<int*>(Ui + kMxNB * DLD);  // [128] original row of each position
+  int* posOf = orig + kMxNB;                             // [128] position of each original row
   __shared__ int fail;
   const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int i = tid >> 1, ph = tid & 1;
+  constexpr unsigned FULL = 0xffffffffu;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
-  float a[64];
-#pragma unroll
-  for (int q = 0; q < 64; ++q) a[q] = Mb[(int64_t)i * N + ph + 2 * q];
-  float cur = a[0];
-  bool chosen = false;
-  int pos = 0;
+  for (int idx = tid; idx < kMxNB * 32; idx += DT) {
+    const int r = idx >> 5, c = (idx & 31) * 4;
+    *reinterpret_cast<float4*>(LU + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
+  }
+  if (tid < kMxNB) orig[tid] = tid;
   if (tid == 0) fail = 0;
   __syncthreads();
-  const DiagCtx ctx{Li, keys, &fail, tid, i, ph, lane, warp};
 #pragma unroll 1
-  for (int kq = 0; kq < 64; ++kq) {
-    lu_step<0>(ctx, kq, a, cur, chosen, pos);
-    lu_step<1>(ctx, kq, a, cur, chosen, pos);
-  }
-  // the packed factors by position: to M (the stored factorisation) and to shared memory
-  if (ph == 0) posOf[i] = pos;
+  for (int kk = 0; kk < kMxNB; ++kk) {
+    if (warp == 0) {
+      // pivot: first largest |A[i][kk]| over i >= kk (lowest row on ties)
+      uint32_t best = 0u, brow = 0xffffffffu;
 #pragma unroll
-  for (int q = 0; q < 64; ++q) {
-    Mb[(int64_t)pos * N + ph + 2 * q] = a[q];
-    LU[pos * DLD + ph + 2 * q] = a[q];
+      for (int m = 0; m < 4; ++m) {
+        const int r = kk + lane + 32 * m;
+        if (r < kMxNB) {
+          const uint32_t key = __float_as_uint(fabsf(LU[r * DLD + kk])) + 1u;
+          if (key > best) {
+            best = key;
+            brow = (uint32_t)r;
+          }
+        }
+      }
+      const uint32_t wmax = __reduce_max_sync(FULL, best);
+      const int p = (int)__reduce_min_sync(FULL, best == wmax ? brow : 0xffffffffu);
+      if (p != kk) {  // swap whole rows kk and p
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+          const int c = lane + 32 * m;
+          const float t = LU[kk * DLD + c];
+          LU[kk * DLD + c] = LU[p * DLD + c];
+          LU[p * DLD + c] = t;
+        }
+        if (lane == 0) {
+          const int t = orig[kk];
+          orig[kk] = orig[p];
+          orig[p] = t;
+        }
+      }
+      __syncwarp();
+      const float piv = LU[kk * DLD + kk];
+      if (lane == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && fail == 0) fail = kk + 1;
+      const float rp = 1.0f / piv;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int r = kk + 1 + lane + 32 * m;
+        if (r < kMxNB) LU[r * DLD + kk] *= rp;
+      }
+    }
+    __syncthreads();
+    // trailing update in 16-byte pieces: rows kk+1.., pieces from the one holding column kk+1
+    const int c0 = (kk + 1) >> 2, np = 32 - c0, nr = kMxNB - 1 - kk;
+    for (int w = tid; w < nr * np; w += DT) {
+      const int r = kk + 1 + w / np, c = (c0 + w % np) * 4;
+      const float l = LU[r * DLD + kk];
+      const float4 u = *reinterpret_cast<const float4*>(LU + kk * DLD + c);
+      float4* ap = reinterpret_cast<float4*>(LU + r * DLD + c);
+      float4 v = *ap;
+      if (c > kk) {
+        v.x = fmaf(-l, u.x, v.x);
+      }
+      if (c + 1 > kk) v.y = fmaf(-l, u.y, v.y);
+      if (c + 2 > kk) v.z = fmaf(-l, u.z, v.z);
+      v.w = c + 3 > kk ? fmaf(-l, u.w, v.w) : v.w;
+      *ap = v;
+    }
+    __syncthreads();
   }
-  __syncthreads();  // the candidate rows are dead: zero both inverses
+  // the packed factors (position order) to M; the permutation
+  for (int idx = tid; idx < kMxNB * 32; idx += DT) {
+    const int r = idx >> 5, c = (idx & 31) * 4;
+    *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = *reinterpret_cast<const float4*>(LU + r * DLD + c);
+  }
+  if (tid < kMxNB) posOf[orig[tid]] = tid;
   for (int idx = tid; idx < 2 * kMxNB * DLD; idx += DT) Li[idx] = 0.f;
   __syncthreads();
   // level 1: the eight 32 x 32 diagonal blocks
