@@ -17,13 +17,17 @@
 //                  thread issues tcgen05.mma.kind::tf32 (M = N = 128) into a
 //                  TMEM accumulator, tcgen05.ld epilogue against the C tile
 //                  (loaded by TMA behind the products), TMA store.
-//  k_mx_trsv       forward and back substitution by 128-row blocks with the
-//                  stored diagonal-block inverses, one CTA per system and
-//                  right-hand-side chunk, the right-hand sides in shared memory.
+//  k_mx_trsv_c     forward and back substitution by 128-row blocks with the
+//                  stored diagonal-block inverses: a cluster of 1..8 CTAs per
+//                  system and right-hand-side chunk, each holding its blocks'
+//                  right-hand sides in shared memory, block solutions passed
+//                  through distributed shared memory (k_mx_trsv: the
+//                  single-CTA form).
 //  k_mx_rhs_in / k_mx_apply   U^T applied to a right-hand side, V and the
 //                  column scales applied to a solution (FP64 accumulation).
 // Every wait on an mbarrier is bounded (about a second of SM clock): past it the
 // CTA counts a timeout, skips its stores, releases its TMEM and returns.
+#include <cooperative_groups.h>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -58,13 +62,22 @@ __device__ __forceinline__ double rbt_d(uint32_t stage, uint32_t i) {
   return exp(0.1 * u);
 }
 
+// The butterflies' diagonals, computed once per call: tab[stage][i] =
+// rbt_d(stage, i) for the 12 stages and i < N / 2.
+__global__ void k_mx_rbt_table(double* __restrict__ tab, int half) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < 12 * half) tab[idx] = rbt_d((uint32_t)(idx / half), (uint32_t)(idx % half));
+}
+
 // The depth-2 butterfly W = D2 B_N (B_N = 2^-1/2 [R S; R -S], D2 = two such
 // blocks of order N/2) restricted to the quad {r, r+q, r+2q, r+3q}, q = N/4.
-// side 0: the left transform U, side 1: the right transform V.
-__device__ void rbt_quad(int side, int r, int q, double Q[4][4]) {
-  const uint32_t b = 6u * (uint32_t)side;
-  const double R0 = rbt_d(b, r), S0 = rbt_d(b + 1, r), R1 = rbt_d(b, r + q), S1 = rbt_d(b + 1, r + q);
-  const double Ra = rbt_d(b + 2, r), Sa = rbt_d(b + 3, r), Rb = rbt_d(b + 4, r), Sb = rbt_d(b + 5, r);
+// side 0: the left transform U, side 1: the right transform V; diagonals
+// from the table (rows of length 2q).
+__device__ __forceinline__ void rbt_quad(const double* __restrict__ tab, int side, int r, int q, double Q[4][4]) {
+  const double* t = tab + (size_t)(6 * side) * (2 * q);
+  const int h = 2 * q;
+  const double R0 = t[r], S0 = t[h + r], R1 = t[r + q], S1 = t[h + r + q];
+  const double Ra = t[2 * h + r], Sa = t[3 * h + r], Rb = t[4 * h + r], Sb = t[5 * h + r];
   Q[0][0] = 0.5 * Ra * R0;  Q[0][1] = 0.5 * Sa * R1;  Q[0][2] = 0.5 * Ra * S0;  Q[0][3] = 0.5 * Sa * S1;
   Q[1][0] = 0.5 * Ra * R0;  Q[1][1] = -0.5 * Sa * R1; Q[1][2] = 0.5 * Ra * S0;  Q[1][3] = -0.5 * Sa * S1;
   Q[2][0] = 0.5 * Rb * R0;  Q[2][1] = 0.5 * Sb * R1;  Q[2][2] = -0.5 * Rb * S0; Q[2][3] = -0.5 * Sb * S1;
@@ -80,17 +93,18 @@ constexpr int BQX = 32, BQY = 8;
 
 __global__ void __launch_bounds__(BQX * BQY)
 k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const double* __restrict__ cmax, int equil,
-           double* __restrict__ cs, RefineState* __restrict__ st, float* __restrict__ M, int n, int N) {
+           double* __restrict__ cs, RefineState* __restrict__ st, float* __restrict__ M, int n, int N,
+           const double* __restrict__ tab) {
   __shared__ double Uq[BQY][4][4];
   __shared__ double Vq[BQX][4][4];
   const int s = blockIdx.z, q = N / 4;
   const int tid = threadIdx.y * BQX + threadIdx.x;
   if (tid < BQY) {
     const int r = blockIdx.y * BQY + tid;
-    if (r < q) rbt_quad(0, r, q, Uq[tid]);
+    if (r < q) rbt_quad(tab, 0, r, q, Uq[tid]);
   } else if (tid >= 32 && tid < 32 + BQX) {
     const int c = blockIdx.x * BQX + tid - 32;
-    if (c < q) rbt_quad(1, c, q, Vq[tid - 32]);
+    if (c < q) rbt_quad(tab, 1, c, q, Vq[tid - 32]);
   }
   if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
     st[s].eta = INFINITY;
@@ -164,9 +178,9 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // |A[i][k]|, i >= k, swaps rows k and p (whole rows: the multipliers already
 // left of k move with them, as in LAPACK's getf2) and scales the column below
 // the diagonal by 1 / A[k][k]; after a barrier all threads update the trailing
-// block A[k+1:, k+1:] -= A[k+1:, k] A[k, k+1:] in 16-byte pieces covering only
-// the active columns (the piece holding column k masked); a second barrier
-// closes the step. The permutation is tracked as the original row of each
+// block A[k+1:, k+1:] -= A[k+1:, k] A[k, k+1:], lane = 16-byte column piece
+// (only the active ones; the piece holding column k masked), warps over the
+// rows; a second barrier closes the step. The permutation is tracked as the original row of each
 // position.
 // Inverses, from the packed factors: the eight 32 x 32 diagonal blocks of L
 // and U inverted by one warp each (lane = column, substitution down / up the
@@ -301,21 +315,23 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
       }
     }
     __syncthreads();
-    // trailing update in 16-byte pieces: rows kk+1.., pieces from the one holding column kk+1
-    const int c0 = (kk + 1) >> 2, np = 32 - c0, nr = kMxNB - 1 - kk;
-    for (int w = tid; w < nr * np; w += DT) {
-      const int r = kk + 1 + w / np, c = (c0 + w % np) * 4;
-      const float l = LU[r * DLD + kk];
-      const float4 u = *reinterpret_cast<const float4*>(LU + kk * DLD + c);
-      float4* ap = reinterpret_cast<float4*>(LU + r * DLD + c);
-      float4 v = *ap;
-      if (c > kk) {
-        v.x = fmaf(-l, u.x, v.x);
+    // trailing update: lane = 16-byte column piece, warp = row phase (rows kk+1+warp, +8, ...);
+    // pieces left of the one holding column kk+1 sit idle, the one holding column kk is masked
+    {
+      const int c = lane * 4;
+      if (c + 3 > kk) {
+        const float4 u = *reinterpret_cast<const float4*>(LU + kk * DLD + c);
+        for (int r = kk + 1 + warp; r < kMxNB; r += DT / 32) {
+          const float l = LU[r * DLD + kk];
+          float4* ap = reinterpret_cast<float4*>(LU + r * DLD + c);
+          float4 v = *ap;
+          if (c > kk) v.x = fmaf(-l, u.x, v.x);
+          if (c + 1 > kk) v.y = fmaf(-l, u.y, v.y);
+          if (c + 2 > kk) v.z = fmaf(-l, u.z, v.z);
+          v.w = fmaf(-l, u.w, v.w);
+          *ap = v;
+        }
       }
-      if (c + 1 > kk) v.y = fmaf(-l, u.y, v.y);
-      if (c + 2 > kk) v.z = fmaf(-l, u.z, v.z);
-      v.w = c + 3 > kk ? fmaf(-l, u.w, v.w) : v.w;
-      *ap = v;
     }
     __syncthreads();
   }
@@ -762,10 +778,131 @@ k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const flo
   }
 }
 
+// Cluster form of the triangular solves: C CTAs per (system, chunk of W
+// right-hand sides), C = 1, 2, 4 or 8. CTA r owns the 128-row blocks b with
+// b % C == r and keeps their right-hand sides in its shared memory. Block
+// step k: the owner computes y_k = D_k c_k (D_k the stored inverse of the
+// diagonal block), writes y_k into every CTA's shared memory (distributed
+// shared memory), and one cluster barrier publishes it; each CTA then
+// updates its own blocks, c_j -= M[block j][block k] y_k. y is
+// double-buffered: a CTA reaches step k's barrier only after finishing step
+// k-1's updates, so step k+1's owner may overwrite step k-1's buffer after it.
+constexpr int TS = 512;  // threads per CTA: 16 warps
+
+// tmp[i][w] = sum_m D[i][m] y[m][w] for the block's 128 rows, 16 warps
+template <int W>
+__device__ __forceinline__ void block_apply16(const float* __restrict__ D, const float* y, float* tmp, int warp,
+                                              int lane) {
+  float yv[4][W];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int w = 0; w < W; ++w) yv[e][w] = y[(4 * lane + e) * W + w];
+#pragma unroll
+  for (int rr = 0; rr < 8; ++rr) {
+    const int i = warp + 16 * rr;
+    const float4 d = *reinterpret_cast<const float4*>(D + i * kMxNB + 4 * lane);
+    float sum[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) sum[w] = d.x * yv[0][w] + d.y * yv[1][w] + d.z * yv[2][w] + d.w * yv[3][w];
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+#pragma unroll
+      for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
+    if (lane == 0)
+#pragma unroll
+      for (int w = 0; w < W; ++w) tmp[i * W + w] = sum[w];
+  }
+}
+
+// c[i] -= M[J + i][K:K+128] . y for the 128 rows of block J (local copy c), 16 warps
+template <int W>
+__device__ __forceinline__ void block_update16(const float* __restrict__ Ms, int N, int J, int K, const float* y,
+                                               float* c, int warp, int lane) {
+  float yv[4][W];
+#pragma unroll
+  for (int e = 0; e < 4; ++e)
+#pragma unroll
+    for (int w = 0; w < W; ++w) yv[e][w] = y[(4 * lane + e) * W + w];
+  float4 m[8];  // rows warp + 16 u: all eight loads in flight before the sums
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+    m[u] = __ldcs(reinterpret_cast<const float4*>(Ms + (int64_t)(J + warp + 16 * u) * N + K + 4 * lane));
+#pragma unroll
+  for (int u = 0; u < 8; ++u) {
+    const int i = warp + 16 * u;
+    float sum[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w)
+      sum[w] = m[u].x * yv[0][w] + m[u].y * yv[1][w] + m[u].z * yv[2][w] + m[u].w * yv[3][w];
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+#pragma unroll
+      for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
+    if (lane == 0)
+#pragma unroll
+      for (int w = 0; w < W; ++w) c[i * W + w] -= sum[w];
+  }
+}
+
+template <int W>
+__global__ void __launch_bounds__(TS, 1)
+k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const float* __restrict__ Uinv,
+            float* __restrict__ Y, int N, int nrhs, int C, const RefineState* __restrict__ st, int only_active) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ float tsm[];
+  const int rank = (int)cluster.block_rank();
+  const int s = blockIdx.x / C, c0 = blockIdx.y * W;
+  if (only_active && st[s].status != kRefineActive) return;  // every CTA of the cluster: same system, same answer
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nb = N / kMxNB, nbl = (nb - rank + C - 1) / C;  // blocks this CTA owns
+  float* cl = tsm;                                  // [nbl][128][W] owned right-hand sides
+  float* yb = cl + (size_t)((nb + C - 1) / C) * kMxNB * W;  // [2][128][W] broadcast block solutions
+  float* tmp = yb + 2 * kMxNB * W;                  // [128][W]
+  const float* Ms = M + (int64_t)s * N * N;
+  float* Ys = Y + (int64_t)s * N * nrhs;
+  for (int idx = tid; idx < nbl * kMxNB * W; idx += TS) {
+    const int lb = idx / (kMxNB * W), rem = idx % (kMxNB * W), i = (lb * C + rank) * kMxNB + rem / W, w = rem % W;
+    cl[idx] = c0 + w < nrhs ? Ys[(int64_t)i * nrhs + c0 + w] : 0.f;
+  }
+  const float* Ls = Linv + (int64_t)s * N * kMxNB;
+  const float* Us = Uinv + (int64_t)s * N * kMxNB;
+  for (int pass = 0; pass < 2; ++pass) {  // L y = P c, then U x = y
+    for (int t = 0; t < nb; ++t) {
+      const int k = pass == 0 ? t : nb - 1 - t, K = k * kMxNB, buf = (pass * nb + t) & 1;
+      float* yk = yb + buf * kMxNB * W;
+      __syncthreads();  // this CTA's updates of the previous step are in
+      if (k % C == rank) {
+        float* ck = cl + (k / C) * kMxNB * W;
+        block_apply16<W>((pass == 0 ? Ls : Us) + (int64_t)K * kMxNB, ck, tmp, warp, lane);
+        __syncthreads();
+        for (int q = 0; q < C; ++q) {
+          float* dst = cluster.map_shared_rank(yk, q);
+          for (int idx = tid; idx < kMxNB * W; idx += TS) dst[idx] = tmp[idx];
+        }
+        for (int idx = tid; idx < kMxNB * W; idx += TS) ck[idx] = tmp[idx];
+      }
+      cluster.sync();  // y_k in every CTA
+      for (int lb = 0; lb < nbl; ++lb) {
+        const int j = lb * C + rank;
+        if (pass == 0 ? j > k : j < k)
+          block_update16<W>(Ms, N, j * kMxNB, K, yk, cl + lb * kMxNB * W, warp, lane);
+      }
+    }
+  }
+  __syncthreads();
+  for (int idx = tid; idx < nbl * kMxNB * W; idx += TS) {
+    const int lb = idx / (kMxNB * W), rem = idx % (kMxNB * W), i = (lb * C + rank) * kMxNB + rem / W, w = rem % W;
+    if (c0 + w < nrhs) Ys[(int64_t)i * nrhs + c0 + w] = cl[idx];
+  }
+  cluster.sync();  // no CTA leaves while a peer may still write into its shared memory
+}
+
 // Y = U^T pad(R): thread per (row quad, right-hand side).
 __global__ void __launch_bounds__(256)
 k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, int nrhs,
-            const RefineState* __restrict__ st, int only_active) {
+            const RefineState* __restrict__ st, int only_active, const double* __restrict__ tab) {
   const int s = blockIdx.y;
   if (only_active && st[s].status != kRefineActive) return;
   const int q = N / 4;
@@ -773,7 +910,7 @@ k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, in
   if (idx >= q * nrhs) return;
   const int r = idx / nrhs, col = idx % nrhs;
   double U[4][4];
-  rbt_quad(0, r, q, U);
+  rbt_quad(tab, 0, r, q, U);
   double x[4];
 #pragma unroll
   for (int a = 0; a < 4; ++a) {
@@ -792,7 +929,7 @@ k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, in
 // X (=|+=) cs * (V Y)[0:n] in FP64: thread per (column quad, right-hand side).
 __global__ void __launch_bounds__(256)
 k_mx_apply(const float* __restrict__ Y, double* __restrict__ X, const double* __restrict__ cs, int n, int N,
-           int nrhs, const RefineState* __restrict__ st, int init) {
+           int nrhs, const RefineState* __restrict__ st, int init, const double* __restrict__ tab) {
   const int s = blockIdx.y;
   if (!init && st[s].status != kRefineActive) return;
   const int q = N / 4;
@@ -800,7 +937,7 @@ k_mx_apply(const float* __restrict__ Y, double* __restrict__ X, const double* __
   if (idx >= q * nrhs) return;
   const int c = idx / nrhs, col = idx % nrhs;
   double V[4][4];
-  rbt_quad(1, c, q, V);
+  rbt_quad(tab, 1, c, q, V);
   double y[4];
 #pragma unroll
   for (int b = 0; b < 4; ++b) y[b] = (double)Y[((int64_t)s * N + c + b * q) * nrhs + col];
@@ -854,7 +991,7 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 size_t mx_workspace_bytes(int count, int n) {
   const size_t N = (size_t)mx_padded(n), c = (size_t)count;
   return align256(4 * c * N * N) + align256(4 * 2 * c * N * kMxNB) + 3 * align256(4 * c * N * kMxNB) +
-         align256(4 * c);
+         align256(4 * c) + align256(sizeof(double) * 12 * (N / 2));
 }
 
 void mx_carve(MxBufs& b, void* base, int count, int n) {
@@ -874,6 +1011,8 @@ void mx_carve(MxBufs& b, void* base, int count, int n) {
   b.UinvT = reinterpret_cast<float*>(p);
   p += align256(4 * c * N * kMxNB);
   b.info = reinterpret_cast<int32_t*>(p);
+  p += align256(4 * c);
+  b.rbt = reinterpret_cast<double*>(p);
 }
 
 cudaError_t mx_prepare() {
@@ -882,6 +1021,11 @@ cudaError_t mx_prepare() {
     e = cudaFuncSetAttribute(k_mx_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
+  const int csm = (int)(sizeof(float) * ((size_t)4096 * 8 + 3 * kMxNB * 8));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   const int tsm = (int)(sizeof(float) * ((size_t)4096 * 8 + kMxNB * 8));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
@@ -900,9 +1044,12 @@ int mx_timeouts_take() {
 
 cudaError_t mx_build(const double* A, const double* rs, const double* cmax, int equil, double* cs, RefineState* st,
                      const MxBufs& b, cudaStream_t s) {
-  const int q = b.N / 4;
+  const int q = b.N / 4, half = b.N / 2;
+  k_mx_rbt_table<<<(12 * half + 255) / 256, 256, 0, s>>>(b.rbt, half);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((q + BQX - 1) / BQX), (unsigned)((q + BQY - 1) / BQY), (unsigned)b.count);
-  k_mx_build<<<grid, dim3(BQX, BQY), 0, s>>>(A, rs, cmax, equil, cs, st, b.M, b.n, b.N);
+  k_mx_build<<<grid, dim3(BQX, BQY), 0, s>>>(A, rs, cmax, equil, cs, st, b.M, b.n, b.N, b.rbt);
   return cudaGetLastError();
 }
 
@@ -959,28 +1106,60 @@ cudaError_t mx_rhs_in(const float* R, float* Y, int nrhs, const RefineState* st,
                       cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
   k_mx_rhs_in<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(R, Y, b.n, b.N, nrhs, st,
-                                                                                      only_active);
+                                                                                      only_active, b.rbt);
   return cudaGetLastError();
+}
+
+// Cluster size of the triangular solves: enough CTAs per system to cover the
+// GPU's SMs when the batch is small, at most 8 (the portable cluster size) and
+// no more than the blocks.
+int trsv_cluster(int count, int chunks, int nb) {
+  int sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaGetLastError();
+  int c = 1;
+  while (c < 8 && 2 * c <= nb && (int64_t)count * chunks * 2 * c <= sms) c *= 2;
+  return c;
+}
+
+template <int W>
+cudaError_t launch_trsv_c(float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, int C,
+                          cudaStream_t s) {
+  const int nb = b.N / kMxNB;
+  const size_t sm = sizeof(float) * ((size_t)((nb + C - 1) / C) * kMxNB * W + 3 * kMxNB * W);
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)(b.count * C), (unsigned)((nrhs + W - 1) / W));
+  cfg.blockDim = dim3(TS);
+  cfg.dynamicSmemBytes = sm;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)C;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_mx_trsv_c<W>, (const float*)b.M, (const float*)b.Linv, (const float*)b.Uinv, Y,
+                            b.N, nrhs, C, st, only_active);
 }
 
 cudaError_t mx_solve(float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, cudaStream_t s) {
   const int W = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;
-  const dim3 grid((unsigned)b.count, (unsigned)((nrhs + W - 1) / W));
-  const size_t sm = sizeof(float) * ((size_t)b.N * W + kMxNB * W);
+  const int C = trsv_cluster(b.count, (nrhs + W - 1) / W, b.N / kMxNB);
   switch (W) {
-    case 1: k_mx_trsv<1><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
-    case 2: k_mx_trsv<2><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
-    case 4: k_mx_trsv<4><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
-    default: k_mx_trsv<8><<<grid, ST, sm, s>>>(b.M, b.Linv, b.Uinv, Y, b.N, nrhs, st, only_active); break;
+    case 1: return launch_trsv_c<1>(Y, nrhs, st, only_active, b, C, s);
+    case 2: return launch_trsv_c<2>(Y, nrhs, st, only_active, b, C, s);
+    case 4: return launch_trsv_c<4>(Y, nrhs, st, only_active, b, C, s);
+    default: return launch_trsv_c<8>(Y, nrhs, st, only_active, b, C, s);
   }
-  return cudaGetLastError();
 }
 
 cudaError_t mx_apply(const float* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
                      const MxBufs& b, cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
   k_mx_apply<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(Y, X, cs, b.n, b.N, nrhs, st,
-                                                                                     init);
+                                                                                     init, b.rbt);
   return cudaGetLastError();
 }
 

@@ -44,10 +44,11 @@ struct MxBufs {
   float* Uinv = nullptr;   // count x N x 128: U_kk^-1
   float* UinvT = nullptr;  // count x N x 128: U_kk^-T
   int32_t* info = nullptr; // count: 0, or 1 + first column whose pivot was zero / not finite
+  double* rbt = nullptr;   // 12 x N/2: the butterflies' random diagonals (computed by mx_build)
   int split3 = 1;          // error-compensated TF32 (1) or plain TF32 (0) products
 };
 
-// Device bytes of the factorisation's buffers for a batch (M, T, Linv, Uinv, UinvT, info).
+// Device bytes of the factorisation's buffers for a batch (M, T, Linv, Uinv, UinvT, info, rbt).
 size_t mx_workspace_bytes(int count, int n);
 // Carve the buffers out of one allocation of mx_workspace_bytes (256-byte aligned).
 void mx_carve(MxBufs& b, void* base, int count, int n);
