@@ -35,6 +35,7 @@
 #include <cstring>
 #include <limits>
 #include <mutex>
+#include <vector>
 
 #include "mxlu.hpp"
 
@@ -89,7 +90,7 @@ __device__ __forceinline__ double pow2_scale(double m) {
   return ldexp(1.0, -ilogb(m));
 }
 
-constexpr int BQX = 32, BQY = 8;
+constexpr int BQX = 128, BQY = 2;  // a block reads 1 KB runs of each of its rows
 
 __global__ void __launch_bounds__(BQX * BQY)
 k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const double* __restrict__ cmax, int equil,
@@ -393,6 +394,10 @@ struct MxGemmArgs {
   int bx, by, bz;  // B (stored as B^T: row = output column) of tile (nt = 0)
   int cx, cy, cz;  // C tile (0, 0)
   int split3;
+  // tile of this CTA: cross = 1: blockIdx.x < tiles -> (0, blockIdx.x), else
+  // (blockIdx.x - tiles + 1, 0) (the next block's panel row and column);
+  // cross = 0: (blockIdx.y + toff, blockIdx.x + toff)
+  int cross, tiles, toff;
   // optional transposed copy of each result element (r, c) of tile (mt, nt):
   // tr + s * tr_sys + (tr_r0 + 128 mt + r) * tr_row + (tr_c0 + 128 nt + c) * tr_col
   float* tr;
@@ -512,7 +517,10 @@ k_mx_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 6);
   int* abort_flag = reinterpret_cast<int*>(bars + 7);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nt = blockIdx.x, mt = blockIdx.y, s = blockIdx.z;
+  const int s = blockIdx.z;
+  const bool in_row = !g.cross || (int)blockIdx.x < g.tiles;
+  const int nt = g.cross ? (in_row ? (int)blockIdx.x : 0) : (int)blockIdx.x + g.toff;
+  const int mt = g.cross ? (in_row ? 0 : (int)blockIdx.x - g.tiles + 1) : (int)blockIdx.y + g.toff;
   const uint32_t bar0 = smem_u32(bars);
   auto full = [&](int st) { return bar0 + 8u * st; };
   auto freed = [&](int st) { return bar0 + 16u + 8u * st; };
@@ -884,6 +892,16 @@ k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const f
         for (int idx = tid; idx < kMxNB * W; idx += TS) ck[idx] = tmp[idx];
       }
       cluster.sync();  // y_k in every CTA
+      if (t + 1 < nb) {  // the next step's panel rows of this CTA's blocks into L2, behind this step's loads
+        const int kn = pass == 0 ? k + 1 : k - 1;
+        for (int idx = tid; idx < nbl * kMxNB * 4; idx += TS) {
+          const int lb = idx / (kMxNB * 4), j = lb * C + rank;
+          if (pass == 0 ? j > kn : j < kn) {
+            const int row = j * kMxNB + (idx / 4) % kMxNB;
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(Ms + (int64_t)row * N + kn * kMxNB + 32 * (idx & 3)));
+          }
+        }
+      }
       for (int lb = 0; lb < nbl; ++lb) {
         const int j = lb * C + rank;
         if (pass == 0 ? j > k : j < k)
@@ -1053,12 +1071,63 @@ cudaError_t mx_build(const double* A, const double* rs, const double* cmax, int 
   return cudaGetLastError();
 }
 
+namespace {
+
+// Streams and events of the look-ahead (per thread and device, made on first use).
+struct MxStreams {
+  cudaStream_t panel = nullptr;  // the next block's diagonal factor and triangular solves, highest priority
+  cudaStream_t side = nullptr;   // the bulk of the trailing update
+  cudaEvent_t ev[4] = {};
+};
+
+MxStreams* mx_streams() {
+  struct Holder {
+    std::vector<MxStreams> per_dev;
+    ~Holder() {
+      for (auto& m : per_dev) {
+        for (cudaStream_t t : {m.panel, m.side})
+          if (t) cudaStreamDestroy(t);
+        for (cudaEvent_t e : m.ev)
+          if (e) cudaEventDestroy(e);
+      }
+    }
+  };
+  thread_local Holder h;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  if ((int)h.per_dev.size() <= dev) h.per_dev.resize(dev + 1);
+  MxStreams& m = h.per_dev[dev];
+  if (!m.side) {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    bool ok = cudaStreamCreateWithPriority(&m.panel, cudaStreamNonBlocking, greatest) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking) == cudaSuccess;
+    for (cudaEvent_t& e : m.ev) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      return nullptr;
+    }
+  }
+  return &m;
+}
+
+}  // namespace
+
+// Blocked factorisation with look-ahead. On the panel stream: block k's
+// diagonal factor and triangular solves, then the cross of its trailing
+// update that block k+1 needs (the first row and column of 128 x 128 tiles);
+// on the side stream, once block k's triangular solves are done, the rest of
+// its trailing update. Block k+1's diagonal factor and solves therefore run
+// beside the bulk of block k's update; block k+1's trailing update waits for
+// it. Every element sees the same operations in the same order either way.
 cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
   const int N = b.N, count = b.count, nb = N / kMxNB;
   CUtensorMap mM, mT, mL, mUT;
   if (!make_map(&mM, b.M, N, N, count) || !make_map(&mT, b.T, kMxNB, N, 2 * (uint64_t)count) ||
       !make_map(&mL, b.Linv, kMxNB, N, count) || !make_map(&mUT, b.UinvT, kMxNB, N, count))
     return cudaErrorInvalidValue;
+  MxStreams* ms = mx_streams();
+  cudaStream_t ps = ms ? ms->panel : s, ss = ms ? ms->side : s;
   cudaError_t e = cudaMemsetAsync(b.info, 0, sizeof(int32_t) * count, s);
   if (e != cudaSuccess) return e;
   if (nb > 1) {
@@ -1066,10 +1135,16 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
         b.M, b.T, N, 0, count, 0);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
+  if (ms) {  // the panel stream starts behind everything queued on s
+    if ((e = cudaEventRecord(ms->ev[0], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(ps, ms->ev[0], 0)) != cudaSuccess) return e;
+  }
+  bool rest_pending = false;
   int buf = 0;
   for (int k = 0; k < nb; ++k) {
     const int K = k * kMxNB, tiles = nb - k - 1;
-    k_mx_diag<<<count, DT, kDiagSmem, s>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.info, N, k);
+    // block k's panel was last written by block k-1's cross, earlier on ps
+    k_mx_diag<<<count, DT, kDiagSmem, ps>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.info, N, k);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (tiles == 0) break;
     MxGemmArgs g{};
@@ -1078,7 +1153,7 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
     g.ax = K; g.ay = K + kMxNB; g.az = 0;
     g.bx = 0; g.by = K; g.bz = 0;
     g.cx = K; g.cy = K + kMxNB; g.cz = 0;
-    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mM, mUT, mM, g);
+    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mUT, mM, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // U12^T = A12^T (L11^-1 P)^T: B^T = L11^-1 P (block k of Linv); U12 also written back into M's panel row
     g.ax = 0; g.ay = K + kMxNB; g.az = buf * count;
@@ -1086,18 +1161,48 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
     g.cx = 0; g.cy = K + kMxNB; g.cz = buf * count;
     g.tr = b.M; g.tr_sys = (int64_t)N * N; g.tr_col = N; g.tr_row = 1; g.tr_c0 = K; g.tr_r0 = K + kMxNB;
     g.tr_mt0_only = 0;
-    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mT, mL, mT, g);
+    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mT, mL, mT, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // A22 -= L21 U12; the first row tile also writes the next panel row, transposed, into the other T buffer
+    // A22 -= L21 U12 over the trailing tiles; tile row 0 also writes the next panel row, transposed
     g.ax = K; g.ay = K + kMxNB; g.az = 0;
     g.bx = 0; g.by = K + kMxNB; g.bz = buf * count;
     g.cx = K + kMxNB; g.cy = K + kMxNB; g.cz = 0;
     g.tr = b.T + (int64_t)(buf ^ 1) * count * N * kMxNB;
     g.tr_sys = (int64_t)N * kMxNB; g.tr_col = kMxNB; g.tr_row = 1; g.tr_c0 = K + kMxNB; g.tr_r0 = 0;
     g.tr_mt0_only = 1;
-    k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, s>>>(mM, mT, mM, g);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    g.tiles = tiles;
+    if (ms && tiles > 1) {
+      // the bulk (tiles >= 1 in both directions) on the side stream once the solves are in;
+      // the previous bulk is ahead of it on the same stream
+      if ((e = cudaEventRecord(ms->ev[1], ps)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(ss, ms->ev[1], 0)) != cudaSuccess) return e;
+      MxGemmArgs gr = g;
+      gr.cross = 0;
+      gr.toff = 1;
+      k_mx_gemm<1><<<dim3((unsigned)(tiles - 1), (unsigned)(tiles - 1), (unsigned)count), GT, kGemmSmem, ss>>>(
+          mM, mT, mM, gr);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      // the cross on the panel stream; it touches tiles the previous bulk updated
+      if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
+      g.cross = 1;
+      k_mx_gemm<1><<<dim3((unsigned)(2 * tiles - 1), 1, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      if ((e = cudaEventRecord(ms->ev[2], ss)) != cudaSuccess) return e;
+      rest_pending = true;
+    } else {
+      if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
+      rest_pending = false;
+      g.cross = 0;
+      g.toff = 0;
+      k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     buf ^= 1;
+  }
+  if (ms) {  // s resumes behind both streams
+    if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ms->ev[3], ps)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(s, ms->ev[3], 0)) != cudaSuccess) return e;
   }
   return cudaSuccess;
 }

@@ -237,10 +237,12 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
     for (size_t q = 0; q < k; ++q) hinfo[idx[q]] = cinfo[q];
   }
-  // final backward error of every system, whatever path produced it
-  NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, 0, max_iter, 0,
-                           act.as<int>(), st),
-            "residual");
+  // final backward error of every system, whatever path produced it (the last
+  // residual of the refinement already is, unless some system fell back)
+  if (any_fallback || n <= 32)
+    NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, 0, max_iter,
+                             0, act.as<int>(), st),
+              "residual");
   if (dFerr && dXtrue) NPPB_CUDA(mixed_ferr(dX, dXtrue, count, n, nrhs, dFerr, st), "forward error");
   NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
   NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
