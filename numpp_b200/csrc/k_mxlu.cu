@@ -174,15 +174,20 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
 // then (L^-1 P), U^-1 and U^-T.
 //
-// LU, in shared memory (row-major, rows swapped as pivots are chosen, so the
-// factors end in position order). Step k: warp 0 finds the first largest
-// |A[i][k]|, i >= k, swaps rows k and p (whole rows: the multipliers already
-// left of k move with them, as in LAPACK's getf2) and scales the column below
-// the diagonal by 1 / A[k][k]; after a barrier all threads update the trailing
-// block A[k+1:, k+1:] -= A[k+1:, k] A[k, k+1:], lane = 16-byte column piece
-// (only the active ones; the piece holding column k masked), warps over the
-// rows; a second barrier closes the step. The permutation is tracked as the original row of each
-// position.
+// LU, in shared memory, blocked by 32-column panels. Rows never move: each
+// physical row of the block gets its position when it is chosen as a pivot
+// (pos_of / phys_of), so the multipliers left of a panel stay with their row
+// as in LAPACK's getrf. Panel p (columns 32p .. 32p+31), warps 0-3, thread =
+// physical row, its 32 panel values in registers; step j: each warp's first
+// largest |a[j]| over its rows not yet chosen (two warp reductions), the
+// winner of each warp publishes its key, row and panel values, one named
+// barrier over the four warps, then every thread takes the overall winner
+// (largest, lowest row on ties), and the rows not yet chosen scale a[j] by
+// 1 / pivot and update their panel values right of j. The candidate buffers
+// alternate between steps, so one barrier per step suffices. After the panel:
+// U12 = L11^-1 A12 over the panel's pivot rows (thread = column), and
+// A22 -= L21 U12 over the rows not yet chosen (4 x 4 register tiles).
+// The packed factors are then gathered into position order.
 // Inverses, from the packed factors: the eight 32 x 32 diagonal blocks of L
 // and U inverted by one warp each (lane = column, substitution down / up the
 // block), then two levels of block products, [L00 0; L10 L11]^-1 =
@@ -195,7 +200,16 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // need no row exchanges), U^-1 and U^-T.
 constexpr int DT = 256;
 constexpr int DLD = 132;  // leading dimension of the shared 128 x 128 arrays (16-byte rows, 4-bank row offset)
-constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(int) * 2 * kMxNB;
+// shared state of the LU besides the three 128 x DLD arrays
+struct DiagAux {
+  int pos_of[kMxNB];   // position of each physical row, -1 until chosen as a pivot
+  int phys_of[kMxNB];  // physical row of each position
+  int act[kMxNB];      // rows not yet chosen, after a panel
+  int4 cand[2][4];     // per warp: key, row, pivot value (bits) of its winner; two buffers
+  float crow[2][4][32];  // per warp: the winner's panel values
+  int fail;
+};
+constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(DiagAux);
 
 // Inverse of one 32 x 32 diagonal block of the packed factors at (o, o), one
 // warp, lane = column: unit lower (L) by substitution down, upper (U) up.
@@ -253,96 +267,177 @@ __device__ __forceinline__ void sgemm(const float* A, const float* B, float* C, 
         make_float4(alpha * acc[r][0], alpha * acc[r][1], alpha * acc[r][2], alpha * acc[r][3]);
 }
 
+// Panel p of the LU (columns c0 = 32p .. c0+31) on warps 0-3, thread t = physical row t.
+__device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int w = t >> 5;
+  const bool was_done = ax.pos_of[t] >= 0;
+  bool done = was_done;
+  int mypos = -1;
+  float a[32];
+  {
+    const float4* src = reinterpret_cast<const float4*>(LU + t * DLD + c0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const float4 v = src[q];
+      a[4 * q] = v.x;
+      a[4 * q + 1] = v.y;
+      a[4 * q + 2] = v.z;
+      a[4 * q + 3] = v.w;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int b = j & 1;
+    // this warp's first largest |a[j]| over rows not yet chosen (key 0: chosen)
+    const uint32_t key = done ? 0u : __float_as_uint(fabsf(a[j])) + 1u;
+    const uint32_t wmax = __reduce_max_sync(FULL, key);
+    const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)t : 0xffffffffu);
+    if ((uint32_t)t == wrow) {
+      ax.cand[b][w] = make_int4((int)wmax, t, __float_as_int(a[j]), 0);
+      float4* cr = reinterpret_cast<float4*>(ax.crow[b][w]);
+#pragma unroll
+      for (int q = (j + 1) >> 2; q < 8; ++q) cr[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
+    }
+    asm volatile("bar.sync 1, 128;\n" ::: "memory");
+    // the overall winner: largest key, lowest row on ties (warp w holds rows 32w .. 32w+31)
+    int4 best = ax.cand[b][0];
+    int bw = 0;
+#pragma unroll
+    for (int x = 1; x < 4; ++x) {
+      const int4 c = ax.cand[b][x];
+      if ((uint32_t)c.x > (uint32_t)best.x) {
+        best = c;
+        bw = x;
+      }
+    }
+    const float piv = __int_as_float(best.z);
+    if (t == best.y) {
+      done = true;
+      mypos = c0 + j;
+      if (!(fabsf(piv) > 0.f && isfinite(piv)) && ax.fail == 0) ax.fail = c0 + j + 1;
+    } else if (!done) {
+      const float l = a[j] * __frcp_rn(piv);
+      a[j] = l;
+      const float4* pr = reinterpret_cast<const float4*>(ax.crow[b][bw]);
+#pragma unroll
+      for (int q = (j + 1) >> 2; q < 8; ++q) {
+        const float4 u = pr[q];
+        if (4 * q > j) a[4 * q] = fmaf(-l, u.x, a[4 * q]);
+        if (4 * q + 1 > j) a[4 * q + 1] = fmaf(-l, u.y, a[4 * q + 1]);
+        if (4 * q + 2 > j) a[4 * q + 2] = fmaf(-l, u.z, a[4 * q + 2]);
+        a[4 * q + 3] = fmaf(-l, u.w, a[4 * q + 3]);
+      }
+    }
+  }
+  if (!was_done) {
+    float4* dst = reinterpret_cast<float4*>(LU + t * DLD + c0);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) dst[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
+  }
+  if (mypos >= 0) {
+    ax.pos_of[t] = mypos;
+    ax.phys_of[mypos] = t;
+  }
+}
+
 __global__ void __launch_bounds__(DT, 1)
 k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
           int32_t* __restrict__ info, int N, int k) {
   extern __shared__ __align__(16) float dsm[];
-  float* LU = dsm;                       // [128][DLD] the block, then its packed factors (position order)
-  float* Li = LU + kMxNB * DLD;          // [128][DLD] L^-1 (position order)
-  float* Ui = Li + kMxNB * DLD;          // [128][DLD] U^-1
-  int* orig = reinterpret_cast<int*>(Ui + kMxNB * DLD);  // [128] original row of each position
-  int* posOf = orig + kMxNB;                             // [128] position of each original row
-  __shared__ int fail;
+  float* W0 = dsm;                   // [128][DLD] the block by physical row; later L^-1
+  float* W1 = W0 + kMxNB * DLD;      // [128][DLD] the packed factors in position order
+  float* Ui = W1 + kMxNB * DLD;      // [128][DLD] U^-1
+  DiagAux& ax = *reinterpret_cast<DiagAux*>(Ui + kMxNB * DLD);
   const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   constexpr unsigned FULL = 0xffffffffu;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
   for (int idx = tid; idx < kMxNB * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
-    *reinterpret_cast<float4*>(LU + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
+    *reinterpret_cast<float4*>(W0 + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
   }
-  if (tid < kMxNB) orig[tid] = tid;
-  if (tid == 0) fail = 0;
+  if (tid < kMxNB) ax.pos_of[tid] = -1;
+  if (tid == 0) ax.fail = 0;
   __syncthreads();
 #pragma unroll 1
-  for (int kk = 0; kk < kMxNB; ++kk) {
-    if (warp == 0) {
-      // pivot: first largest |A[i][kk]| over i >= kk (lowest row on ties)
-      uint32_t best = 0u, brow = 0xffffffffu;
+  for (int p = 0; p < 4; ++p) {
+    const int c0 = 32 * p;
+    if (warp < 4) diag_panel(W0, ax, c0, tid);
+    __syncthreads();
+    if (p == 3) break;
+    const int W = kMxNB - c0 - 32;  // trailing columns (and rows not yet chosen)
+    if (tid < W) {
+      // U12 = L11^-1 A12 on the panel's pivot rows, thread = column
+      const int c = c0 + 32 + tid;
+      float u[32];
 #pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int r = kk + lane + 32 * m;
-        if (r < kMxNB) {
-          const uint32_t key = __float_as_uint(fabsf(LU[r * DLD + kk])) + 1u;
-          if (key > best) {
-            best = key;
-            brow = (uint32_t)r;
+      for (int j = 0; j < 32; ++j) u[j] = W0[ax.phys_of[c0 + j] * DLD + c];
+#pragma unroll
+      for (int j = 1; j < 32; ++j) {
+        const float* lr = W0 + ax.phys_of[c0 + j] * DLD + c0;
+#pragma unroll
+        for (int m = 0; m < j; ++m) u[j] = fmaf(-lr[m], u[m], u[j]);
+      }
+#pragma unroll
+      for (int j = 1; j < 32; ++j) W0[ax.phys_of[c0 + j] * DLD + c] = u[j];
+    } else if (warp == 4) {
+      // the rows not yet chosen, in physical order
+      int base = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int r = 32 * q + lane;
+        const bool nd = ax.pos_of[r] < 0;
+        const unsigned m = __ballot_sync(FULL, nd);
+        if (nd) ax.act[base + __popc(m & ((1u << lane) - 1u))] = r;
+        base += __popc(m);
+      }
+    }
+    __syncthreads();
+    // A22 -= L21 U12: 4 rows (of act) x 4 columns per task
+    {
+      const int ng = W >> 2, ntask = ng * ng;
+      for (int task = tid; task < ntask; task += DT) {
+        const int rg = task / ng, cc = c0 + 32 + 4 * (task - rg * ng);
+        float* rp[4];
+        float4 acc[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          rp[i] = W0 + ax.act[4 * rg + i] * DLD;
+          acc[i] = *reinterpret_cast<const float4*>(rp[i] + cc);
+        }
+#pragma unroll 8
+        for (int m = 0; m < 32; ++m) {
+          const float4 u = *reinterpret_cast<const float4*>(W0 + ax.phys_of[c0 + m] * DLD + cc);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float l = rp[i][c0 + m];
+            acc[i].x = fmaf(-l, u.x, acc[i].x);
+            acc[i].y = fmaf(-l, u.y, acc[i].y);
+            acc[i].z = fmaf(-l, u.z, acc[i].z);
+            acc[i].w = fmaf(-l, u.w, acc[i].w);
           }
         }
-      }
-      const uint32_t wmax = __reduce_max_sync(FULL, best);
-      const int p = (int)__reduce_min_sync(FULL, best == wmax ? brow : 0xffffffffu);
-      if (p != kk) {  // swap whole rows kk and p
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          const int c = lane + 32 * m;
-          const float t = LU[kk * DLD + c];
-          LU[kk * DLD + c] = LU[p * DLD + c];
-          LU[p * DLD + c] = t;
-        }
-        if (lane == 0) {
-          const int t = orig[kk];
-          orig[kk] = orig[p];
-          orig[p] = t;
-        }
-      }
-      __syncwarp();
-      const float piv = LU[kk * DLD + kk];
-      if (lane == 0 && !(fabsf(piv) > 0.f && isfinite(piv)) && fail == 0) fail = kk + 1;
-      const float rp = 1.0f / piv;
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int r = kk + 1 + lane + 32 * m;
-        if (r < kMxNB) LU[r * DLD + kk] *= rp;
-      }
-    }
-    __syncthreads();
-    // trailing update: lane = 16-byte column piece, warp = row phase (rows kk+1+warp, +8, ...);
-    // pieces left of the one holding column kk+1 sit idle, the one holding column kk is masked
-    {
-      const int c = lane * 4;
-      if (c + 3 > kk) {
-        const float4 u = *reinterpret_cast<const float4*>(LU + kk * DLD + c);
-        for (int r = kk + 1 + warp; r < kMxNB; r += DT / 32) {
-          const float l = LU[r * DLD + kk];
-          float4* ap = reinterpret_cast<float4*>(LU + r * DLD + c);
-          float4 v = *ap;
-          if (c > kk) v.x = fmaf(-l, u.x, v.x);
-          if (c + 1 > kk) v.y = fmaf(-l, u.y, v.y);
-          if (c + 2 > kk) v.z = fmaf(-l, u.z, v.z);
-          v.w = fmaf(-l, u.w, v.w);
-          *ap = v;
-        }
+        for (int i = 0; i < 4; ++i) *reinterpret_cast<float4*>(rp[i] + cc) = acc[i];
       }
     }
     __syncthreads();
   }
-  // the packed factors (position order) to M; the permutation
+  // the packed factors in position order: to W1 and M
   for (int idx = tid; idx < kMxNB * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
-    *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = *reinterpret_cast<const float4*>(LU + r * DLD + c);
+    const float4 v = *reinterpret_cast<const float4*>(W0 + ax.phys_of[r] * DLD + c);
+    *reinterpret_cast<float4*>(W1 + r * DLD + c) = v;
+    *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = v;
   }
-  if (tid < kMxNB) posOf[orig[tid]] = tid;
-  for (int idx = tid; idx < 2 * kMxNB * DLD; idx += DT) Li[idx] = 0.f;
+  __syncthreads();
+  float* LU = W1;
+  float* Li = W0;
+  const int* posOf = ax.pos_of;
+  for (int idx = tid; idx < kMxNB * DLD; idx += DT) {
+    Li[idx] = 0.f;
+    Ui[idx] = 0.f;
+  }
   __syncthreads();
   // level 1: the eight 32 x 32 diagonal blocks
   if (warp < 4) inv_lower32(LU, Li, 32 * warp, lane);
@@ -379,7 +474,7 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
     Ub[idx] = c >= r ? Ui[r * DLD + c] : 0.f;        // U^-1[r][c]
     UTb[idx] = r >= c ? Ui[c * DLD + r] : 0.f;       // U^-T[r][c]
   }
-  if (tid == 0 && fail && info[s] == 0) info[s] = K + fail;
+  if (tid == 0 && ax.fail && info[s] == 0) info[s] = K + ax.fail;
 }
 
 // ---------------------------------------------------------------------------
