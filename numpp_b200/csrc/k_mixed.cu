@@ -71,6 +71,7 @@ k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict_
   double arow = 0.0;
   for (int i = warp; i < rows; i += MT / 32) {
     double m = 0.0, sum = 0.0;
+#pragma unroll 8
     for (int j = lane; j < n; j += 32) {
       const double v = fabs(a[(int64_t)i * n + j]);
       m = fmax(m, v);
@@ -90,6 +91,7 @@ k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict_
   if (!equil) return;
   for (int j = tid; j < n; j += MT) {
     double m = 0.0;
+#pragma unroll 8
     for (int i = 0; i < rows; ++i) m = fmax(m, rsc[i] * fabs(a[(int64_t)i * n + j]));
     atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), m);
   }

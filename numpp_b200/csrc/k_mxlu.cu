@@ -90,30 +90,19 @@ __device__ __forceinline__ double pow2_scale(double m) {
   return ldexp(1.0, -ilogb(m));
 }
 
-constexpr int BQX = 128, BQY = 2;  // a block reads 1 KB runs of each of its rows
+constexpr int BQX = 128, BQY = 2;  // a block reads 1 KB runs of each of its rows; quads in registers
 
 __global__ void __launch_bounds__(BQX * BQY)
 k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const double* __restrict__ cmax, int equil,
            double* __restrict__ cs, RefineState* __restrict__ st, float* __restrict__ M, int n, int N,
            const double* __restrict__ tab) {
-  __shared__ double Uq[BQY][4][4];
-  __shared__ double Vq[BQX][4][4];
   const int s = blockIdx.z, q = N / 4;
-  const int tid = threadIdx.y * BQX + threadIdx.x;
-  if (tid < BQY) {
-    const int r = blockIdx.y * BQY + tid;
-    if (r < q) rbt_quad(tab, 0, r, q, Uq[tid]);
-  } else if (tid >= 32 && tid < 32 + BQX) {
-    const int c = blockIdx.x * BQX + tid - 32;
-    if (c < q) rbt_quad(tab, 1, c, q, Vq[tid - 32]);
-  }
-  if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) {
     st[s].eta = INFINITY;
     st[s].prev = INFINITY;
     st[s].status = kRefineActive;
     st[s].iters = 0;
   }
-  __syncthreads();
   const int cq = blockIdx.x * BQX + threadIdx.x, rq = blockIdx.y * BQY + threadIdx.y;
   if (cq >= q || rq >= q) return;
   double csb[4], rsa[4];
@@ -137,15 +126,21 @@ k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const do
     }
   }
   double t[4][4];  // A V
+  {
+    double Vq[4][4];  // this thread's column quad (consecutive threads: consecutive table entries)
+    rbt_quad(tab, 1, cq, q, Vq);
 #pragma unroll
-  for (int x = 0; x < 4; ++x)
+    for (int x = 0; x < 4; ++x)
 #pragma unroll
-    for (int y = 0; y < 4; ++y) {
-      double v = 0.0;
+      for (int y = 0; y < 4; ++y) {
+        double v = 0.0;
 #pragma unroll
-      for (int z = 0; z < 4; ++z) v = fma(a[x][z], Vq[threadIdx.x][z][y], v);
-      t[x][y] = v;
-    }
+        for (int z = 0; z < 4; ++z) v = fma(a[x][z], Vq[z][y], v);
+        t[x][y] = v;
+      }
+  }
+  double Uq[4][4];  // the row quad (one per warp: broadcast loads)
+  rbt_quad(tab, 0, rq, q, Uq);
   float* Ms = M + (int64_t)s * N * N;
 #pragma unroll
   for (int x = 0; x < 4; ++x)
@@ -153,7 +148,7 @@ k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const do
     for (int y = 0; y < 4; ++y) {
       double v = 0.0;  // (U^T A V)[x][y]
 #pragma unroll
-      for (int z = 0; z < 4; ++z) v = fma(Uq[threadIdx.y][z][x], t[z][y], v);
+      for (int z = 0; z < 4; ++z) v = fma(Uq[z][x], t[z][y], v);
       Ms[(int64_t)(rq + x * q) * N + cq + y * q] = (float)v;
     }
 }
