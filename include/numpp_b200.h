@@ -210,7 +210,14 @@ int nppb_d_solve_batched_noalloc(int64_t count, int32_t n, int32_t nrhs, const d
  * / NPPB_MIXED_BF16), or FP32 fused multiply-adds (NPPB_MIXED_FP32_FMA); the
  * TF32 products on mma.sync, or with NPPB_MIXED_TCGEN05 on tcgen05 with TMEM
  * accumulators. FP32 accumulation in every case; the stored factors and the
- * correction solves stay FP32. */
+ * correction solves stay FP32.
+ * With NPPB_MIXED_GMRES (default factorisation only): each correction is
+ * solved by GMRES on M^-1 A d = M^-1 R (Carson and Higham's GMRES-based
+ * refinement), M^-1 the FP32 factorisation applied to FP64 vectors with FP64
+ * accumulation, FP64 Krylov vectors and products with A, up to 30 Arnoldi
+ * steps per correction (to a relative residual of 1e-6); it reaches tol for
+ * conditioning the plain refinement stalls on (kappa up to about 1e8 with
+ * FP32 factors). iters then counts outer corrections. */
 enum {
   NPPB_MIXED_NO_EQUILIBRATE = 1,
   NPPB_MIXED_NO_FALLBACK = 2,
@@ -218,7 +225,8 @@ enum {
   NPPB_MIXED_BF16 = 8,
   NPPB_MIXED_FP32_FMA = 16,
   NPPB_MIXED_TCGEN05 = 32,
-  NPPB_MIXED_PIVOTED = 64
+  NPPB_MIXED_PIVOTED = 64,
+  NPPB_MIXED_GMRES = 128
 };
 int nppb_d_solve_mixed_batched(int64_t count, int32_t n, int32_t nrhs, const double* dA,
                                const double* dB, double* dX, const double* dXtrue, double tol,

@@ -18,6 +18,7 @@ DT_FLOAT32, DT_FLOAT64 = 10, 11
 WANT_LU, WANT_SOLVE, WANT_DET, WANT_SLOGDET, WANT_INV = 1, 2, 4, 8, 16
 MIXED_NO_EQUILIBRATE, MIXED_NO_FALLBACK, MIXED_TF32, MIXED_BF16, MIXED_FP32_FMA, MIXED_TCGEN05 = 1, 2, 4, 8, 16, 32
 MIXED_PIVOTED = 64
+MIXED_GMRES = 128
 
 _vp = C.c_void_p
 _i32 = C.c_int32

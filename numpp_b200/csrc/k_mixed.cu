@@ -132,7 +132,7 @@ k_scale_rhs(const double* __restrict__ B, int n, int nrhs, const double* __restr
   __shared__ double red[MT / 32];
   const int s = blockIdx.x, tid = threadIdx.x;
   const int64_t nb = (int64_t)n * nrhs;
-  const double* b = B + (int64_t)s * nb;
+  const double* b = B ? B + (int64_t)s * nb : nullptr;  // null: R = -A X (the product alone)
   double m = 0.0;
   for (int64_t idx = tid; idx < nb; idx += MT) {
     const double v = b[idx];
@@ -169,7 +169,8 @@ template <int RC>
 __global__ void __launch_bounds__(MT)
 k_residual(const double* __restrict__ A, const double* __restrict__ B, const double* __restrict__ X,
            int n, int nrhs, const double* __restrict__ rs, float* __restrict__ R32,
-           const int32_t* __restrict__ rpos, RefineState* __restrict__ st, int only_active) {
+           const int32_t* __restrict__ rpos, double* __restrict__ R64, RefineState* __restrict__ st,
+           int only_active, int stats) {
   constexpr int CB = XS / RC;
   __shared__ double xs[XS];
   __shared__ double red[MT / 32];
@@ -179,9 +180,9 @@ k_residual(const double* __restrict__ A, const double* __restrict__ B, const dou
   if (only_active && st[s].status != kRefineActive) return;
   const int64_t nb = (int64_t)n * nrhs;
   const double* a = A + (int64_t)s * n * n;
-  const double* b = B + (int64_t)s * nb;
+  const double* b = B ? B + (int64_t)s * nb : nullptr;  // null: R = -A X (the product alone)
   const double* x = X + (int64_t)s * nb;
-  const bool first = blockIdx.y == 0;
+  const bool first = stats && blockIdx.y == 0;
   double rmax = 0.0, xmax = 0.0;
   for (int k0 = 0; k0 < nrhs; k0 += RC) {
     const int kc = min(RC, nrhs - k0);
@@ -229,16 +230,18 @@ k_residual(const double* __restrict__ A, const double* __restrict__ B, const dou
       const int q = lane / RC, k = lane % RC;
       const int i = r0 + warp * RW + q;
       if (i < n && k < kc) {
-        const double r = b[(int64_t)i * nrhs + k0 + k] - ax_s[warp][q][k];
+        const double r = (b ? b[(int64_t)i * nrhs + k0 + k] : 0.0) - ax_s[warp][q][k];
         rmax = fmax(rmax, fabs(r));
         if (R32) {
           const int p = rpos ? rpos[(int64_t)s * n + i] : i;
           R32[(int64_t)s * nb + (int64_t)p * nrhs + k0 + k] = (float)(rs[(int64_t)s * n + i] * r);
         }
+        if (R64) R64[(int64_t)s * nb + (int64_t)i * nrhs + k0 + k] = rs[(int64_t)s * n + i] * r;
       }
     }
     __syncwarp();
   }
+  if (!stats) return;
   rmax = block_max(rmax, red);
   if (tid == 0) atomic_max_nonneg(&st[s].rmax_bits, rmax);
   if (first) {
@@ -355,18 +358,30 @@ cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, 
   k_apply<<<count, MT, 0, s>>>(X, Y, cs, n, nrhs, st, init);
   return cudaGetLastError();
 }
+namespace {
+cudaError_t launch_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
+                            const double* rs, float* R32, const int32_t* rpos, double* R64, RefineState* st,
+                            int only_active, int stats, cudaStream_t s) {
+  const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
+  if (nrhs == 1) k_residual<1><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, R64, st, only_active, stats);
+  else if (nrhs == 2) k_residual<2><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, R64, st, only_active, stats);
+  else if (nrhs <= 4) k_residual<4><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, R64, st, only_active, stats);
+  else k_residual<8><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, R64, st, only_active, stats);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
                            const double* rs, float* R32, const int32_t* rpos, RefineState* st, double tol,
-                           int iter, int max_iter, int decide, int* active, cudaStream_t s) {
-  const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
-  if (nrhs == 1) k_residual<1><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
-  else if (nrhs == 2) k_residual<2><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
-  else if (nrhs <= 4) k_residual<4><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
-  else k_residual<8><<<grid, MT, 0, s>>>(A, B, X, n, nrhs, rs, R32, rpos, st, decide);
-  cudaError_t e = cudaGetLastError();
+                           int iter, int max_iter, int decide, int* active, cudaStream_t s, double* R64) {
+  cudaError_t e = launch_residual(A, B, X, count, n, nrhs, rs, R32, rpos, R64, st, decide, 1, s);
   if (e != cudaSuccess) return e;
   k_refine_decide<<<(count + 255) / 256, 256, 0, s>>>(st, count, tol, iter, max_iter, decide, active);
   return cudaGetLastError();
+}
+cudaError_t mixed_matvec(const double* A, const double* X, int count, int n, int nrhs, const double* rs,
+                         double* R64, RefineState* st, cudaStream_t s) {
+  return launch_residual(A, nullptr, X, count, n, nrhs, rs, nullptr, nullptr, R64, st, 1, 0, s);
 }
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,
                        cudaStream_t s) {

@@ -9,8 +9,8 @@
 //  k_mx_transpose  the first block's panel row, transposed (A12^T).
 //  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
 //                  among its own rows (one CTA, the block in shared memory,
-//                  two barriers per column), then L^-1 P, U^-1 and U^-T by
-//                  blocked inversion in shared memory.
+//                  32-column panels factored by one warp in registers), then
+//                  L^-1 P, U^-1 and U^-T by blocked inversion in shared memory.
 //  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
 //                  by TMA in 128-byte-swizzled boxes (two stages of 32-column
 //                  chunks), split into TF32 hi / lo in shared memory, one
@@ -31,6 +31,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <limits>
@@ -172,16 +174,11 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // LU, in shared memory, blocked by 32-column panels. Rows never move: each
 // physical row of the block gets its position when it is chosen as a pivot
 // (pos_of / phys_of), so the multipliers left of a panel stay with their row
-// as in LAPACK's getrf. Panel p (columns 32p .. 32p+31), warps 0-3, thread =
-// physical row, its 32 panel values in registers; step j: each warp's first
-// largest |a[j]| over its rows not yet chosen (two warp reductions), the
-// winner of each warp publishes its key, row and panel values, one named
-// barrier over the four warps, then every thread takes the overall winner
-// (largest, lowest row on ties), and the rows not yet chosen scale a[j] by
-// 1 / pivot and update their panel values right of j. The candidate buffers
-// alternate between steps, so one barrier per step suffices. After the panel:
-// U12 = L11^-1 A12 over the panel's pivot rows (thread = column), and
-// A22 -= L21 U12 over the rows not yet chosen (4 x 4 register tiles).
+// as in LAPACK's getrf. Panel p (columns 32p .. 32p+31) is factored by one
+// warp with the panel in registers (diag_panel: no block-wide barrier inside
+// a panel). After the panel: U12 = L11^-1 A12 over the panel's pivot rows
+// (thread = column), and A22 -= L21 U12 over the rows not yet chosen (4 x 4
+// register tiles).
 // The packed factors are then gathered into position order.
 // Inverses, from the packed factors: the eight 32 x 32 diagonal blocks of L
 // and U inverted by one warp each (lane = column, substitution down / up the
@@ -200,9 +197,10 @@ struct DiagAux {
   int pos_of[kMxNB];   // position of each physical row, -1 until chosen as a pivot
   int phys_of[kMxNB];  // physical row of each position
   int act[kMxNB];      // rows not yet chosen, after a panel
-  int4 cand[2][4];     // per warp: key, row, pivot value (bits) of its winner; two buffers
-  float crow[2][4][32];  // per warp: the winner's panel values
-  int fail;
+  uint32_t keys[2][4];   // per warp: the key of its winner; two buffers (alternating steps)
+  float crow[2][4][32];  // per warp: its winner's panel values
+  float lcol[32][32];    // the panel's L11 columns below the diagonal (shifted to index 0)
+  int fail;  // 1 + first position whose pivot failed, INT_MAX if none
 };
 constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(DiagAux);
 
@@ -234,105 +232,144 @@ __device__ __forceinline__ void inv_upper32(const float* LU, float* Ui, int o, i
 }
 
 // C = alpha A B for S x S blocks of the shared arrays (leading dimension DLD),
-// thread t of a group of (S/TM) * (S/4) threads computing TM x 4 outputs.
+// thread t of a group of (S/TM) * (S/4) threads computing the 4 columns c0 ..
+// c0+3 of the TM rows g, g + S/TM, ... (adjacent threads: adjacent rows, so the
+// 16-byte loads of A along k and of B along c hit distinct banks).
 template <int S, int TM>
 __device__ __forceinline__ void sgemm(const float* A, const float* B, float* C, float alpha, int t) {
-  constexpr int CG = S / 4;
-  const int r0 = (t / CG) * TM, c0 = (t % CG) * 4;
+  constexpr int CG = S / 4, RG = S / TM;
+  const int g = t / CG, c0 = (t % CG) * 4;
   float acc[TM][4];
 #pragma unroll
   for (int r = 0; r < TM; ++r)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[r][j] = 0.f;
-#pragma unroll 8
-  for (int k = 0; k < S; ++k) {
-    const float4 bv = *reinterpret_cast<const float4*>(B + k * DLD + c0);
+#pragma unroll 2
+  for (int k = 0; k < S; k += 4) {
+    float4 bv[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) bv[i] = *reinterpret_cast<const float4*>(B + (k + i) * DLD + c0);
 #pragma unroll
     for (int r = 0; r < TM; ++r) {
-      const float av = A[(r0 + r) * DLD + k];
-      acc[r][0] = fmaf(av, bv.x, acc[r][0]);
-      acc[r][1] = fmaf(av, bv.y, acc[r][1]);
-      acc[r][2] = fmaf(av, bv.z, acc[r][2]);
-      acc[r][3] = fmaf(av, bv.w, acc[r][3]);
+      const float4 av = *reinterpret_cast<const float4*>(A + (g + RG * r) * DLD + k);
+      const float a4[4] = {av.x, av.y, av.z, av.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        acc[r][0] = fmaf(a4[i], bv[i].x, acc[r][0]);
+        acc[r][1] = fmaf(a4[i], bv[i].y, acc[r][1]);
+        acc[r][2] = fmaf(a4[i], bv[i].z, acc[r][2]);
+        acc[r][3] = fmaf(a4[i], bv[i].w, acc[r][3]);
+      }
     }
   }
 #pragma unroll
   for (int r = 0; r < TM; ++r)
-    *reinterpret_cast<float4*>(C + (r0 + r) * DLD + c0) =
+    *reinterpret_cast<float4*>(C + (g + RG * r) * DLD + c0) =
         make_float4(alpha * acc[r][0], alpha * acc[r][1], alpha * acc[r][2], alpha * acc[r][3]);
 }
 
-// Panel p of the LU (columns c0 = 32p .. c0+31) on warps 0-3, thread t = physical row t.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void st_shared_u32_if(bool c, uint32_t addr, uint32_t x) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.u32 p, %0, 0;\n @p st.shared.u32 [%1], %2;\n}\n" ::"r"((uint32_t)c),
+      "r"(addr), "r"(x)
+      : "memory");
+}
+// the 32 values v[0..31] to 128 bytes of shared memory at addr (16-byte aligned), if c
+__device__ __forceinline__ void st_shared_row_if(bool c, uint32_t addr, const float (&v)[32]) {
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.u32 p, %0, 0;\n @p st.shared.v4.f32 [%1], {%2, %3, %4, %5};\n}\n" ::"r"(
+            (uint32_t)c),
+        "r"(addr + 16u * q), "f"(v[4 * q]), "f"(v[4 * q + 1]), "f"(v[4 * q + 2]), "f"(v[4 * q + 3])
+        : "memory");
+}
+// 1 / x to about an ulp (the hardware approximation; subnormal x flushes to zero)
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Panel of the LU (columns c0 .. c0+31) on warps 0-3, thread t = physical row
+// t, in a rolled loop over the steps (the code stays small: this kernel is
+// otherwise bound by instruction fetch). At step j a row's 32 registers hold
+// its values in columns c0 + j .. c0 + j + 31 (shifted left by one every step
+// while the row is not chosen, so register indices are static). Step j: each
+// warp's largest key (magnitude with its 7 low mantissa bits dropped, plus
+// one) << 7 | (127 - row) over the rows not yet chosen by one warp reduction;
+// lane 0 publishes it and the warp's winner its values; one named barrier over
+// the four warps; the overall winner (the largest |a[j]| up to a relative
+// 2^-16, the lowest row among those) takes position c0 + j, and every row not
+// yet chosen stores l = a[j] / pivot and updates its values right of j. Keys
+// and rows sit in two alternating buffers, so one barrier per step suffices.
 __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t) {
   constexpr unsigned FULL = 0xffffffffu;
-  const int w = t >> 5;
-  const bool was_done = ax.pos_of[t] >= 0;
-  bool done = was_done;
-  int mypos = -1;
-  float a[32];
+  const int w = t >> 5, lane = t & 31;
+  const bool was = ax.pos_of[t] >= 0;
+  bool done = was;
+  int jd = 0;         // step at which this row was chosen
+  int bad = INT_MAX;  // 1 + position of this row if its pivot failed
+  float v[32];
   {
     const float4* src = reinterpret_cast<const float4*>(LU + t * DLD + c0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-      const float4 v = src[q];
-      a[4 * q] = v.x;
-      a[4 * q + 1] = v.y;
-      a[4 * q + 2] = v.z;
-      a[4 * q + 3] = v.w;
+      const float4 x = src[q];
+      v[4 * q] = x.x;
+      v[4 * q + 1] = x.y;
+      v[4 * q + 2] = x.z;
+      v[4 * q + 3] = x.w;
     }
   }
-#pragma unroll
+#pragma unroll 1
   for (int j = 0; j < 32; ++j) {
     const int b = j & 1;
-    // this warp's first largest |a[j]| over rows not yet chosen (key 0: chosen)
-    const uint32_t key = done ? 0u : __float_as_uint(fabsf(a[j])) + 1u;
-    const uint32_t wmax = __reduce_max_sync(FULL, key);
-    const uint32_t wrow = __reduce_min_sync(FULL, key == wmax ? (uint32_t)t : 0xffffffffu);
-    if ((uint32_t)t == wrow) {
-      ax.cand[b][w] = make_int4((int)wmax, t, __float_as_int(a[j]), 0);
-      float4* cr = reinterpret_cast<float4*>(ax.crow[b][w]);
-#pragma unroll
-      for (int q = (j + 1) >> 2; q < 8; ++q) cr[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
-    }
+    const uint32_t key =
+        done ? 0u : ((((__float_as_uint(fabsf(v[0])) >> 7) + 1u) << 7) | (uint32_t)(127 - t));
+    const uint32_t wkey = __reduce_max_sync(FULL, key);
+    // predicated stores, not a divergent branch (a one-lane branch around
+    // these stores costs several times their latency)
+    st_shared_u32_if(lane == 0, smem_addr(&ax.keys[b][w]), wkey);
+    st_shared_row_if(wkey != 0u && t == 127 - (int)(wkey & 127u), smem_addr(ax.crow[b][w]), v);
     asm volatile("bar.sync 1, 128;\n" ::: "memory");
-    // the overall winner: largest key, lowest row on ties (warp w holds rows 32w .. 32w+31)
-    int4 best = ax.cand[b][0];
-    int bw = 0;
+    const uint4 kk = *reinterpret_cast<const uint4*>(ax.keys[b]);
+    const uint32_t best = max(max(kk.x, kk.y), max(kk.z, kk.w));
+    const int prow = 127 - (int)(best & 127u);
+    const float* pr = ax.crow[b][prow >> 5];
+    // the winner's bookkeeping without a branch
+    const bool win = t == prow;
+    st_shared_u32_if(win, smem_addr(&ax.pos_of[t]), (uint32_t)(c0 + j));
+    st_shared_u32_if(win, smem_addr(&ax.phys_of[c0 + j]), (uint32_t)t);
+    // the approximate reciprocal below flushes subnormals: such a pivot fails too
+    if (win && !(fabsf(v[0]) >= FLT_MIN && isfinite(v[0]))) bad = min(bad, c0 + j + 1);
+    jd = win ? j : jd;
+    done = done || win;
+    if (!done) {
+      const float l = v[0] * rcp_approx(pr[0]);
+      LU[t * DLD + c0 + j] = l;
+      float u[32];
 #pragma unroll
-    for (int x = 1; x < 4; ++x) {
-      const int4 c = ax.cand[b][x];
-      if ((uint32_t)c.x > (uint32_t)best.x) {
-        best = c;
-        bw = x;
+      for (int q = 0; q < 8; ++q) {
+        const float4 x = reinterpret_cast<const float4*>(pr)[q];
+        u[4 * q] = x.x;
+        u[4 * q + 1] = x.y;
+        u[4 * q + 2] = x.z;
+        u[4 * q + 3] = x.w;
       }
-    }
-    const float piv = __int_as_float(best.z);
-    if (t == best.y) {
-      done = true;
-      mypos = c0 + j;
-      if (!(fabsf(piv) > 0.f && isfinite(piv)) && ax.fail == 0) ax.fail = c0 + j + 1;
-    } else if (!done) {
-      const float l = a[j] * __frcp_rn(piv);
-      a[j] = l;
-      const float4* pr = reinterpret_cast<const float4*>(ax.crow[b][bw]);
 #pragma unroll
-      for (int q = (j + 1) >> 2; q < 8; ++q) {
-        const float4 u = pr[q];
-        if (4 * q > j) a[4 * q] = fmaf(-l, u.x, a[4 * q]);
-        if (4 * q + 1 > j) a[4 * q + 1] = fmaf(-l, u.y, a[4 * q + 1]);
-        if (4 * q + 2 > j) a[4 * q + 2] = fmaf(-l, u.z, a[4 * q + 2]);
-        a[4 * q + 3] = fmaf(-l, u.w, a[4 * q + 3]);
-      }
+      for (int c = 0; c < 31; ++c) v[c] = fmaf(-l, u[c + 1], v[c + 1]);
+      v[31] = 0.f;
     }
   }
-  if (!was_done) {
-    float4* dst = reinterpret_cast<float4*>(LU + t * DLD + c0);
+  if (bad != INT_MAX) atomicMin(&ax.fail, bad);
+  if (done && !was) {  // the row's U values, columns c0 + jd .. c0 + 31
 #pragma unroll
-    for (int q = 0; q < 8; ++q) dst[q] = make_float4(a[4 * q], a[4 * q + 1], a[4 * q + 2], a[4 * q + 3]);
-  }
-  if (mypos >= 0) {
-    ax.pos_of[t] = mypos;
-    ax.phys_of[mypos] = t;
+    for (int c = 0; c < 32; ++c)
+      if (c < 32 - jd) LU[t * DLD + c0 + jd + c] = v[c];
   }
 }
 
@@ -352,7 +389,7 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
     *reinterpret_cast<float4*>(W0 + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
   }
   if (tid < kMxNB) ax.pos_of[tid] = -1;
-  if (tid == 0) ax.fail = 0;
+  if (tid == 0) ax.fail = INT_MAX;
   __syncthreads();
 #pragma unroll 1
   for (int p = 0; p < 4; ++p) {
@@ -362,19 +399,36 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
     if (p == 3) break;
     const int W = kMxNB - c0 - 32;  // trailing columns (and rows not yet chosen)
     if (tid < W) {
-      // U12 = L11^-1 A12 on the panel's pivot rows, thread = column
-      const int c = c0 + 32 + tid;
-      float u[32];
-#pragma unroll
-      for (int j = 0; j < 32; ++j) u[j] = W0[ax.phys_of[c0 + j] * DLD + c];
-#pragma unroll
-      for (int j = 1; j < 32; ++j) {
-        const float* lr = W0 + ax.phys_of[c0 + j] * DLD + c0;
-#pragma unroll
-        for (int m = 0; m < j; ++m) u[j] = fmaf(-lr[m], u[m], u[j]);
+      // U12 = L11^-1 A12 on the panel's pivot rows, thread = column, in a
+      // rolled loop: v[i] holds position c0 + j + i at step j (shifted like
+      // the panel); the columns of L11 below the diagonal are staged first,
+      // shifted: lcol[j][i] = L(c0 + j + 1 + i, c0 + j)
+      for (int idx = tid; idx < 32 * 32; idx += W) {
+        const int j = idx >> 5, i = idx & 31;
+        ax.lcol[j][i] = i < 31 - j ? W0[ax.phys_of[c0 + j + 1 + i] * DLD + c0 + j] : 0.f;
       }
+      asm volatile("bar.sync 2, %0;\n" ::"r"(W) : "memory");
+      const int c = c0 + 32 + tid;
+      float v[32];
 #pragma unroll
-      for (int j = 1; j < 32; ++j) W0[ax.phys_of[c0 + j] * DLD + c] = u[j];
+      for (int j = 0; j < 32; ++j) v[j] = W0[ax.phys_of[c0 + j] * DLD + c];
+#pragma unroll 1
+      for (int j = 0; j < 31; ++j) {
+        const float x = v[0];
+        W0[ax.phys_of[c0 + j] * DLD + c] = x;
+        float lc[32];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const float4 y = reinterpret_cast<const float4*>(ax.lcol[j])[q];
+          lc[4 * q] = y.x;
+          lc[4 * q + 1] = y.y;
+          lc[4 * q + 2] = y.z;
+          lc[4 * q + 3] = y.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 31; ++i) v[i] = fmaf(-lc[i], x, v[i + 1]);
+      }
+      W0[ax.phys_of[c0 + 31] * DLD + c] = v[0];
     } else if (warp == 4) {
       // the rows not yet chosen, in physical order
       int base = 0;
@@ -438,27 +492,36 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   if (warp < 4) inv_lower32(LU, Li, 32 * warp, lane);
   else inv_upper32(LU, Ui, 32 * (warp - 4), lane);
   __syncthreads();
-  // level 2: 64 x 64 diagonal quadrants; four chains of 64 threads
+  // level 2: 64 x 64 diagonal quadrants; four chains of 64 threads (one call
+  // site per level in a rolled loop over the two products: compact code)
   {
     const int ch = tid >> 6, t = tid & 63, p = ch & 1, o = 64 * p;
-    float* tL = Li + (32 * p) * DLD + 64;        // temporaries in Li's upper-right quadrant
-    float* tU = Ui + (64 + 32 * p) * DLD;        //   ... and Ui's lower-left quadrant
-    if (ch < 2) sgemm<32, 4>(LU + (o + 32) * DLD + o, Li + o * DLD + o, tL, 1.f, t);
-    else sgemm<32, 4>(LU + o * DLD + o + 32, Ui + (o + 32) * DLD + o + 32, tU, 1.f, t);
-    __syncthreads();
-    if (ch < 2) sgemm<32, 4>(Li + (o + 32) * DLD + o + 32, tL, Li + (o + 32) * DLD + o, -1.f, t);
-    else sgemm<32, 4>(Ui + o * DLD + o, tU, Ui + o * DLD + o + 32, -1.f, t);
-    __syncthreads();
+    const bool isL = ch < 2;
+    float* tmp = isL ? Li + (32 * p) * DLD + 64   // temporaries in Li's upper-right quadrant
+                     : Ui + (64 + 32 * p) * DLD;  //   ... and Ui's lower-left quadrant
+#pragma unroll 1
+    for (int ph = 0; ph < 2; ++ph) {
+      const float* A = ph == 0 ? (isL ? LU + (o + 32) * DLD + o : LU + o * DLD + o + 32)
+                               : (isL ? Li + (o + 32) * DLD + o + 32 : Ui + o * DLD + o);
+      const float* B = ph == 0 ? (isL ? Li + o * DLD + o : Ui + (o + 32) * DLD + o + 32) : tmp;
+      float* C = ph == 0 ? tmp : (isL ? Li + (o + 32) * DLD + o : Ui + o * DLD + o + 32);
+      sgemm<32, 4>(A, B, C, ph == 0 ? 1.f : -1.f, t);
+      __syncthreads();
+    }
   }
   // level 3: the off-diagonal quadrants; two chains of 128 threads, temporaries in LU's diagonal quadrants
   {
     const int ch = tid >> 7, t = tid & 127;
-    if (ch == 0) sgemm<64, 8>(LU + 64 * DLD, Li, LU, 1.f, t);
-    else sgemm<64, 8>(LU + 64, Ui + 64 * DLD + 64, LU + 64 * DLD + 64, 1.f, t);
-    __syncthreads();
-    if (ch == 0) sgemm<64, 8>(Li + 64 * DLD + 64, LU, Li + 64 * DLD, -1.f, t);
-    else sgemm<64, 8>(Ui, LU + 64 * DLD + 64, Ui + 64, -1.f, t);
-    __syncthreads();
+    const bool isL = ch == 0;
+    float* tmp = isL ? LU : LU + 64 * DLD + 64;
+#pragma unroll 1
+    for (int ph = 0; ph < 2; ++ph) {
+      const float* A = ph == 0 ? (isL ? LU + 64 * DLD : LU + 64) : (isL ? Li + 64 * DLD + 64 : Ui);
+      const float* B = ph == 0 ? (isL ? Li : Ui + 64 * DLD + 64) : tmp;
+      float* C = ph == 0 ? tmp : (isL ? Li + 64 * DLD : Ui + 64);
+      sgemm<64, 8>(A, B, C, ph == 0 ? 1.f : -1.f, t);
+      __syncthreads();
+    }
   }
   float* Lb = Linv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   float* Ub = Uinv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
@@ -469,7 +532,7 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
     Ub[idx] = c >= r ? Ui[r * DLD + c] : 0.f;        // U^-1[r][c]
     UTb[idx] = r >= c ? Ui[c * DLD + r] : 0.f;       // U^-T[r][c]
   }
-  if (tid == 0 && ax.fail && info[s] == 0) info[s] = K + ax.fail;
+  if (tid == 0 && ax.fail != INT_MAX && info[s] == 0) info[s] = K + ax.fail;
 }
 
 // ---------------------------------------------------------------------------
@@ -886,12 +949,13 @@ k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const flo
 // double-buffered: a CTA reaches step k's barrier only after finishing step
 // k-1's updates, so step k+1's owner may overwrite step k-1's buffer after it.
 constexpr int TS = 512;  // threads per CTA: 16 warps
+constexpr size_t kTrsv64Smem = 160 * 1024;  // shared-memory cap of the FP64-vector substitution
 
 // tmp[i][w] = sum_m D[i][m] y[m][w] for the block's 128 rows, 16 warps
-template <int W>
-__device__ __forceinline__ void block_apply16(const float* __restrict__ D, const float* y, float* tmp, int warp,
+template <int W, class VT>
+__device__ __forceinline__ void block_apply16(const float* __restrict__ D, const VT* y, VT* tmp, int warp,
                                               int lane) {
-  float yv[4][W];
+  VT yv[4][W];
 #pragma unroll
   for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -900,7 +964,7 @@ __device__ __forceinline__ void block_apply16(const float* __restrict__ D, const
   for (int rr = 0; rr < 8; ++rr) {
     const int i = warp + 16 * rr;
     const float4 d = *reinterpret_cast<const float4*>(D + i * kMxNB + 4 * lane);
-    float sum[W];
+    VT sum[W];
 #pragma unroll
     for (int w = 0; w < W; ++w) sum[w] = d.x * yv[0][w] + d.y * yv[1][w] + d.z * yv[2][w] + d.w * yv[3][w];
 #pragma unroll
@@ -914,10 +978,10 @@ __device__ __forceinline__ void block_apply16(const float* __restrict__ D, const
 }
 
 // c[i] -= M[J + i][K:K+128] . y for the 128 rows of block J (local copy c), 16 warps
-template <int W>
-__device__ __forceinline__ void block_update16(const float* __restrict__ Ms, int N, int J, int K, const float* y,
-                                               float* c, int warp, int lane) {
-  float yv[4][W];
+template <int W, class VT>
+__device__ __forceinline__ void block_update16(const float* __restrict__ Ms, int N, int J, int K, const VT* y,
+                                               VT* c, int warp, int lane) {
+  VT yv[4][W];
 #pragma unroll
   for (int e = 0; e < 4; ++e)
 #pragma unroll
@@ -929,7 +993,7 @@ __device__ __forceinline__ void block_update16(const float* __restrict__ Ms, int
 #pragma unroll
   for (int u = 0; u < 8; ++u) {
     const int i = warp + 16 * u;
-    float sum[W];
+    VT sum[W];
 #pragma unroll
     for (int w = 0; w < W; ++w)
       sum[w] = m[u].x * yv[0][w] + m[u].y * yv[1][w] + m[u].z * yv[2][w] + m[u].w * yv[3][w];
@@ -943,40 +1007,41 @@ __device__ __forceinline__ void block_update16(const float* __restrict__ Ms, int
   }
 }
 
-template <int W>
+template <int W, class VT>
 __global__ void __launch_bounds__(TS, 1)
 k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const float* __restrict__ Uinv,
-            float* __restrict__ Y, int N, int nrhs, int C, const RefineState* __restrict__ st, int only_active) {
+            VT* __restrict__ Y, int N, int nrhs, int C, const RefineState* __restrict__ st, int only_active) {
   namespace cg = cooperative_groups;
   cg::cluster_group cluster = cg::this_cluster();
-  extern __shared__ float tsm[];
+  extern __shared__ __align__(16) unsigned char tsm_raw[];
+  VT* tsm = reinterpret_cast<VT*>(tsm_raw);
   const int rank = (int)cluster.block_rank();
   const int s = blockIdx.x / C, c0 = blockIdx.y * W;
   if (only_active && st[s].status != kRefineActive) return;  // every CTA of the cluster: same system, same answer
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nb = N / kMxNB, nbl = (nb - rank + C - 1) / C;  // blocks this CTA owns
-  float* cl = tsm;                                  // [nbl][128][W] owned right-hand sides
-  float* yb = cl + (size_t)((nb + C - 1) / C) * kMxNB * W;  // [2][128][W] broadcast block solutions
-  float* tmp = yb + 2 * kMxNB * W;                  // [128][W]
+  VT* cl = tsm;                                  // [nbl][128][W] owned right-hand sides
+  VT* yb = cl + (size_t)((nb + C - 1) / C) * kMxNB * W;  // [2][128][W] broadcast block solutions
+  VT* tmp = yb + 2 * kMxNB * W;                  // [128][W]
   const float* Ms = M + (int64_t)s * N * N;
-  float* Ys = Y + (int64_t)s * N * nrhs;
+  VT* Ys = Y + (int64_t)s * N * nrhs;
   for (int idx = tid; idx < nbl * kMxNB * W; idx += TS) {
     const int lb = idx / (kMxNB * W), rem = idx % (kMxNB * W), i = (lb * C + rank) * kMxNB + rem / W, w = rem % W;
-    cl[idx] = c0 + w < nrhs ? Ys[(int64_t)i * nrhs + c0 + w] : 0.f;
+    cl[idx] = c0 + w < nrhs ? Ys[(int64_t)i * nrhs + c0 + w] : VT(0);
   }
   const float* Ls = Linv + (int64_t)s * N * kMxNB;
   const float* Us = Uinv + (int64_t)s * N * kMxNB;
   for (int pass = 0; pass < 2; ++pass) {  // L y = P c, then U x = y
     for (int t = 0; t < nb; ++t) {
       const int k = pass == 0 ? t : nb - 1 - t, K = k * kMxNB, buf = (pass * nb + t) & 1;
-      float* yk = yb + buf * kMxNB * W;
+      VT* yk = yb + buf * kMxNB * W;
       __syncthreads();  // this CTA's updates of the previous step are in
       if (k % C == rank) {
-        float* ck = cl + (k / C) * kMxNB * W;
-        block_apply16<W>((pass == 0 ? Ls : Us) + (int64_t)K * kMxNB, ck, tmp, warp, lane);
+        VT* ck = cl + (k / C) * kMxNB * W;
+        block_apply16<W, VT>((pass == 0 ? Ls : Us) + (int64_t)K * kMxNB, ck, tmp, warp, lane);
         __syncthreads();
         for (int q = 0; q < C; ++q) {
-          float* dst = cluster.map_shared_rank(yk, q);
+          VT* dst = cluster.map_shared_rank(yk, q);
           for (int idx = tid; idx < kMxNB * W; idx += TS) dst[idx] = tmp[idx];
         }
         for (int idx = tid; idx < kMxNB * W; idx += TS) ck[idx] = tmp[idx];
@@ -995,7 +1060,7 @@ k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const f
       for (int lb = 0; lb < nbl; ++lb) {
         const int j = lb * C + rank;
         if (pass == 0 ? j > k : j < k)
-          block_update16<W>(Ms, N, j * kMxNB, K, yk, cl + lb * kMxNB * W, warp, lane);
+          block_update16<W, VT>(Ms, N, j * kMxNB, K, yk, cl + lb * kMxNB * W, warp, lane);
       }
     }
   }
@@ -1008,8 +1073,9 @@ k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const f
 }
 
 // Y = U^T pad(R): thread per (row quad, right-hand side).
+template <class TR, class TY>
 __global__ void __launch_bounds__(256)
-k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, int nrhs,
+k_mx_rhs_in(const TR* __restrict__ R, TY* __restrict__ Y, int n, int N, int nrhs,
             const RefineState* __restrict__ st, int only_active, const double* __restrict__ tab) {
   const int s = blockIdx.y;
   if (only_active && st[s].status != kRefineActive) return;
@@ -1030,13 +1096,14 @@ k_mx_rhs_in(const float* __restrict__ R, float* __restrict__ Y, int n, int N, in
     double v = 0.0;
 #pragma unroll
     for (int b = 0; b < 4; ++b) v = fma(U[b][a], x[b], v);
-    Y[((int64_t)s * N + r + a * q) * nrhs + col] = (float)v;
+    Y[((int64_t)s * N + r + a * q) * nrhs + col] = (TY)v;
   }
 }
 
 // X (=|+=) cs * (V Y)[0:n] in FP64: thread per (column quad, right-hand side).
+template <class TY>
 __global__ void __launch_bounds__(256)
-k_mx_apply(const float* __restrict__ Y, double* __restrict__ X, const double* __restrict__ cs, int n, int N,
+k_mx_apply(const TY* __restrict__ Y, double* __restrict__ X, const double* __restrict__ cs, int n, int N,
            int nrhs, const RefineState* __restrict__ st, int init, const double* __restrict__ tab) {
   const int s = blockIdx.y;
   if (!init && st[s].status != kRefineActive) return;
@@ -1130,10 +1197,16 @@ cudaError_t mx_prepare() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
   const int csm = (int)(sizeof(float) * ((size_t)4096 * 8 + 3 * kMxNB * 8));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<8, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_trsv_c<1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_trsv_c<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_trsv_c<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
   const int tsm = (int)(sizeof(float) * ((size_t)4096 * 8 + kMxNB * 8));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
@@ -1300,8 +1373,8 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
 cudaError_t mx_rhs_in(const float* R, float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b,
                       cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
-  k_mx_rhs_in<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(R, Y, b.n, b.N, nrhs, st,
-                                                                                      only_active, b.rbt);
+  k_mx_rhs_in<float, float><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
+      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt);
   return cudaGetLastError();
 }
 
@@ -1318,11 +1391,11 @@ int trsv_cluster(int count, int chunks, int nb) {
   return c;
 }
 
-template <int W>
-cudaError_t launch_trsv_c(float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, int C,
+template <int W, class VT>
+cudaError_t launch_trsv_c(VT* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, int C,
                           cudaStream_t s) {
   const int nb = b.N / kMxNB;
-  const size_t sm = sizeof(float) * ((size_t)((nb + C - 1) / C) * kMxNB * W + 3 * kMxNB * W);
+  const size_t sm = sizeof(VT) * ((size_t)((nb + C - 1) / C) * kMxNB * W + 3 * kMxNB * W);
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)(b.count * C), (unsigned)((nrhs + W - 1) / W));
   cfg.blockDim = dim3(TS);
@@ -1335,26 +1408,60 @@ cudaError_t launch_trsv_c(float* Y, int nrhs, const RefineState* st, int only_ac
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_mx_trsv_c<W>, (const float*)b.M, (const float*)b.Linv, (const float*)b.Uinv, Y,
-                            b.N, nrhs, C, st, only_active);
+  return cudaLaunchKernelEx(&cfg, k_mx_trsv_c<W, VT>, (const float*)b.M, (const float*)b.Linv,
+                            (const float*)b.Uinv, Y, b.N, nrhs, C, st, only_active);
 }
 
 cudaError_t mx_solve(float* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b, cudaStream_t s) {
   const int W = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : nrhs <= 4 ? 4 : 8;
   const int C = trsv_cluster(b.count, (nrhs + W - 1) / W, b.N / kMxNB);
   switch (W) {
-    case 1: return launch_trsv_c<1>(Y, nrhs, st, only_active, b, C, s);
-    case 2: return launch_trsv_c<2>(Y, nrhs, st, only_active, b, C, s);
-    case 4: return launch_trsv_c<4>(Y, nrhs, st, only_active, b, C, s);
-    default: return launch_trsv_c<8>(Y, nrhs, st, only_active, b, C, s);
+    case 1: return launch_trsv_c<1, float>(Y, nrhs, st, only_active, b, C, s);
+    case 2: return launch_trsv_c<2, float>(Y, nrhs, st, only_active, b, C, s);
+    case 4: return launch_trsv_c<4, float>(Y, nrhs, st, only_active, b, C, s);
+    default: return launch_trsv_c<8, float>(Y, nrhs, st, only_active, b, C, s);
   }
+}
+
+// FP64 vectors: chunks of at most 4 right-hand sides (2 at order 4096 with a
+// one-CTA cluster), so that a CTA's share of the vectors fits shared memory.
+cudaError_t mx_solve64(double* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b,
+                       cudaStream_t s) {
+  const int nb = b.N / kMxNB;
+  int W = nrhs <= 1 ? 1 : nrhs <= 2 ? 2 : 4;
+  int C = trsv_cluster(b.count, (nrhs + W - 1) / W, nb);
+  while (W > 1 && sizeof(double) * ((size_t)((nb + C - 1) / C) * kMxNB * W + 3 * kMxNB * W) > kTrsv64Smem) {
+    W >>= 1;
+    C = trsv_cluster(b.count, (nrhs + W - 1) / W, nb);
+  }
+  switch (W) {
+    case 1: return launch_trsv_c<1, double>(Y, nrhs, st, only_active, b, C, s);
+    case 2: return launch_trsv_c<2, double>(Y, nrhs, st, only_active, b, C, s);
+    default: return launch_trsv_c<4, double>(Y, nrhs, st, only_active, b, C, s);
+  }
+}
+
+cudaError_t mx_rhs_in64(const double* R, double* Y, int nrhs, const RefineState* st, int only_active,
+                        const MxBufs& b, cudaStream_t s) {
+  const int work = b.N / 4 * nrhs;
+  k_mx_rhs_in<double, double><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
+      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt);
+  return cudaGetLastError();
+}
+
+cudaError_t mx_apply64(const double* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
+                       const MxBufs& b, cudaStream_t s) {
+  const int work = b.N / 4 * nrhs;
+  k_mx_apply<double><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
+      Y, X, cs, b.n, b.N, nrhs, st, init, b.rbt);
+  return cudaGetLastError();
 }
 
 cudaError_t mx_apply(const float* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
                      const MxBufs& b, cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
-  k_mx_apply<<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(Y, X, cs, b.n, b.N, nrhs, st,
-                                                                                     init, b.rbt);
+  k_mx_apply<float><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
+      Y, X, cs, b.n, b.N, nrhs, st, init, b.rbt);
   return cudaGetLastError();
 }
 

@@ -12,8 +12,10 @@
 //     products as error-compensated TF32, TF32, BF16 (mma.sync or tcgen05) or
 //     FP32 FMA;
 //  3. refine in FP64: R = B - A X, eta = normwise backward error; systems with
-//     eta <= tol stop, systems whose eta no longer halves are marked stalled;
-//     the others solve A d = R with the FP32 factors and add d in FP64;
+//     eta <= tol stop, systems whose contraction cannot reach tol are marked
+//     stalled; the others solve A d = R with the FP32 factors and add d in
+//     FP64 (with NPPB_MIXED_GMRES: d by GMRES on M^-1 A d = M^-1 R, M the FP32
+//     factorisation applied to FP64 vectors, Carson and Higham's GMRES-IR);
 //  4. every system that did not converge (stalled, FP32 zero pivot, or out of
 //     iterations) is refactored and solved in FP64;
 //  5. report per system: eta, forward error when X_true is given, corrections
@@ -26,6 +28,7 @@
 #include <vector>
 
 #include "../../include/numpp_b200.h"
+#include "gmres.hpp"
 #include "mixed.hpp"
 #include "mxlu.hpp"
 #include "runtime.hpp"
@@ -33,6 +36,10 @@
 using namespace nppb;
 
 namespace {
+
+// relative residual at which GMRES stops inside one correction (the outer
+// FP64 residual decides convergence)
+constexpr double kGmresTau = 1e-6;
 
 #define NPPB_CUDA(call, what)                            \
   do {                                                   \
@@ -54,7 +61,7 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   }
   const int arith = flags & (NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA);
   if ((flags & ~(NPPB_MIXED_NO_EQUILIBRATE | NPPB_MIXED_NO_FALLBACK | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 |
-                 NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05 | NPPB_MIXED_PIVOTED)) ||
+                 NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05 | NPPB_MIXED_PIVOTED | NPPB_MIXED_GMRES)) ||
       (arith & (arith - 1))) {
     set_error("unknown mixed flag bits, or more than one of TF32 / BF16 / FP32_FMA");
     return NPPB_E_ARG;
@@ -74,6 +81,11 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
   const bool pivoted =
       (flags & (NPPB_MIXED_PIVOTED | NPPB_MIXED_TF32 | NPPB_MIXED_BF16 | NPPB_MIXED_FP32_FMA | NPPB_MIXED_TCGEN05)) != 0;
   const bool blocked = n > 32 && !pivoted;
+  const bool gmres = blocked && (flags & NPPB_MIXED_GMRES);
+  if ((flags & NPPB_MIXED_GMRES) && pivoted) {
+    set_error("GMRES refinement runs on the default (blocked) factorisation only");
+    return NPPB_E_ARG;
+  }
   DevMem a32, piv, rpos, sc32, b32, y32, rsm, csm, cmx, stm, info32, act, mxw;
   if (!blocked) {
     NPPB_CUDA(a32.alloc(sizeof(float) * c * nn, st), "workspace");
@@ -126,18 +138,63 @@ int mixed(int64_t count64, int32_t n, int32_t nrhs, const double* dA, const doub
     NPPB_CUDA(mx_solve(Y, nrhs, S, 0, mb, st), "FP32 solve");
     NPPB_CUDA(mx_apply(Y, dX, csm.as<double>(), nrhs, S, 1, mb, st), "apply");
     int h_act = 0;
-    for (int it = 0;; ++it) {
-      NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
-      // the scaled residual lands in b32 (row order of A)
-      NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), nullptr, S, tol, it,
-                               max_iter, 1, act.as<int>(), st),
-                "residual");
-      NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
-      NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
-      if (h_act == 0 || it >= max_iter) break;
-      NPPB_CUDA(mx_rhs_in(b32.as<float>(), Y, nrhs, S, 1, mb, st), "transform residual");
-      NPPB_CUDA(mx_solve(Y, nrhs, S, 1, mb, st), "FP32 correction solve");
-      NPPB_CUDA(mx_apply(Y, dX, csm.as<double>(), nrhs, S, 0, mb, st), "apply");
+    if (!gmres) {
+      for (int it = 0;; ++it) {
+        NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
+        // the scaled residual lands in b32 (row order of A)
+        NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), b32.as<float>(), nullptr, S, tol,
+                                 it, max_iter, 1, act.as<int>(), st),
+                  "residual");
+        NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
+        NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+        if (h_act == 0 || it >= max_iter) break;
+        NPPB_CUDA(mx_rhs_in(b32.as<float>(), Y, nrhs, S, 1, mb, st), "transform residual");
+        NPPB_CUDA(mx_solve(Y, nrhs, S, 1, mb, st), "FP32 correction solve");
+        NPPB_CUDA(mx_apply(Y, dX, csm.as<double>(), nrhs, S, 0, mb, st), "apply");
+      }
+    } else {
+      // GMRES-IR: each correction by LU-preconditioned GMRES in FP64 (the
+      // preconditioner is the FP32 factorisation applied to FP64 vectors)
+      const size_t vec = c * nb;  // doubles of one vector plane (count x n x nrhs)
+      DevMem gV, gR, gY, gW, gS, gA;
+      NPPB_CUDA(gV.alloc(sizeof(double) * vec * (kGmM + 1), st), "workspace");
+      NPPB_CUDA(gR.alloc(sizeof(double) * vec, st), "workspace");
+      NPPB_CUDA(gY.alloc(sizeof(double) * c * (size_t)mb.N * nrhs, st), "workspace");
+      NPPB_CUDA(gW.alloc(sizeof(double) * vec, st), "workspace");
+      NPPB_CUDA(gS.alloc(sizeof(GmState) * c * nrhs, st), "workspace");
+      NPPB_CUDA(gA.alloc(sizeof(int), st), "workspace");
+      double* V = gV.as<double>();
+      auto precond = [&](const double* in, double* out) -> int {  // out = M^-1 in (in: already row-scaled)
+        NPPB_CUDA(mx_rhs_in64(in, gY.as<double>(), nrhs, S, 1, mb, st), "transform");
+        NPPB_CUDA(mx_solve64(gY.as<double>(), nrhs, S, 1, mb, st), "preconditioner solve");
+        NPPB_CUDA(mx_apply64(gY.as<double>(), out, csm.as<double>(), nrhs, S, 1, mb, st), "apply");
+        return NPPB_OK;
+      };
+      for (int it = 0;; ++it) {
+        NPPB_CUDA(cudaMemsetAsync(act.as<int>(), 0, sizeof(int), st), "memset");
+        NPPB_CUDA(mixed_residual(dA, dB, dX, count, n, nrhs, rsm.as<double>(), nullptr, nullptr, S, tol, it,
+                                 max_iter, 1, act.as<int>(), st, gR.as<double>()),
+                  "residual");
+        NPPB_CUDA(cudaMemcpyAsync(&h_act, act.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
+        NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+        if (h_act == 0 || it >= max_iter) break;
+        NPPB_RC(precond(gR.as<double>(), gW.as<double>()));
+        NPPB_CUDA(gm_start(gW.as<double>(), V, gS.as<GmState>(), S, count, n, nrhs, st), "GMRES start");
+        for (int k = 0; k < kGmM; ++k) {
+          NPPB_CUDA(mixed_matvec(dA, V + (size_t)k * vec, count, n, nrhs, rsm.as<double>(), gR.as<double>(), S, st),
+                    "GMRES product");
+          NPPB_RC(precond(gR.as<double>(), gW.as<double>()));
+          int h_in = 0;
+          NPPB_CUDA(cudaMemsetAsync(gA.as<int>(), 0, sizeof(int), st), "memset");
+          NPPB_CUDA(gm_arnoldi(gW.as<double>(), V, gS.as<GmState>(), S, count, n, nrhs, k, kGmresTau, gA.as<int>(),
+                               st),
+                    "GMRES step");
+          NPPB_CUDA(cudaMemcpyAsync(&h_in, gA.as<int>(), sizeof(int), cudaMemcpyDeviceToHost, st), "readback");
+          NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");
+          if (h_in == 0) break;
+        }
+        NPPB_CUDA(gm_update(V, dX, gS.as<GmState>(), S, count, n, nrhs, st), "GMRES update");
+      }
     }
     NPPB_CUDA(cudaMemcpyAsync(hs.data(), S, sizeof(RefineState) * c, cudaMemcpyDeviceToHost, st), "readback");
     NPPB_CUDA(cudaStreamSynchronize(st), "synchronize");

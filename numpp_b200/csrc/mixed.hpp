@@ -40,9 +40,14 @@ cudaError_t mixed_apply(double* X, const float* Y, const double* cs, int count, 
 // decide = 1: update status / iters and count the still-active systems into *active
 // (a system is stalled when its contraction cannot reach tol in max_iter - iter corrections).
 // R32 (optional): r * R in FP32, row i stored at row rpos[i] (the pivoted order) when rpos is given.
+// R64 (optional): r * R in FP64, natural row order.
 cudaError_t mixed_residual(const double* A, const double* B, const double* X, int count, int n, int nrhs,
                            const double* rs, float* R32, const int32_t* rpos, RefineState* st, double tol,
-                           int iter, int max_iter, int decide, int* active, cudaStream_t s);
+                           int iter, int max_iter, int decide, int* active, cudaStream_t s,
+                           double* R64 = nullptr);
+// R64 = -diag(rs) A X in FP64 for the systems still refining (no state update).
+cudaError_t mixed_matvec(const double* A, const double* X, int count, int n, int nrhs, const double* rs,
+                         double* R64, RefineState* st, cudaStream_t s);
 // rpos[s*n + i] = position of row i after the swaps of ipiv (s*n .. s*n+n-1).
 cudaError_t mixed_row_positions(const int32_t* ipiv, int count, int n, int32_t* rpos, cudaStream_t s);
 cudaError_t mixed_ferr(const double* X, const double* Xt, int count, int n, int nrhs, double* ferr,

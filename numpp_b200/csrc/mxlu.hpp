@@ -69,6 +69,15 @@ cudaError_t mx_solve(float* Y, int nrhs, const RefineState* st, int only_active,
 // X (count x n x nrhs, FP64) = cs * (V Y)[0:n] (init) or X += that (systems still refining).
 cudaError_t mx_apply(const float* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
                      const MxBufs& b, cudaStream_t s);
+// The same three steps on FP64 vectors (FP32 factors, FP64 accumulation): the
+// preconditioner of the GMRES refinement. R is already row-scaled; chunks of
+// up to 4 right-hand sides per substitution.
+cudaError_t mx_rhs_in64(const double* R, double* Y, int nrhs, const RefineState* st, int only_active,
+                        const MxBufs& b, cudaStream_t s);
+cudaError_t mx_solve64(double* Y, int nrhs, const RefineState* st, int only_active, const MxBufs& b,
+                       cudaStream_t s);
+cudaError_t mx_apply64(const double* Y, double* X, const double* cs, int nrhs, const RefineState* st, int init,
+                       const MxBufs& b, cudaStream_t s);
 // Bounded waits of the GEMM kernel that ran out since the last call (each
 // such CTA skipped its stores); the counter is reset. -1: unreadable.
 int mx_timeouts_take();

@@ -11,7 +11,8 @@ _FACTOR = {"3xtf32": 0, "fp32": _lib.MIXED_FP32_FMA, "tf32": _lib.MIXED_TF32, "b
 
 
 def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equilibrate: bool = True,
-                fallback: bool = True, factor: str = "3xtf32", tcgen05: bool = False, pivoted: bool = False):
+                fallback: bool = True, factor: str = "3xtf32", tcgen05: bool = False, pivoted: bool = False,
+                gmres: bool = False):
     """X for a (count, n, n) / (count, n, nrhs) float64 batch; returns
     (X, report) with report = dict(berr, ferr, iters, fallback, info) per system.
 
@@ -22,7 +23,10 @@ def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equil
     partial pivoting on the step-wise kernels, factor choosing the trailing
     products: "3xtf32" (error-compensated TF32, close to FP32), "tf32" or
     "bf16" (one tensor-core product), "fp32" (FMA); tcgen05: TF32 products on
-    the tcgen05 tensor cores with TMEM accumulators instead of mma.sync."""
+    the tcgen05 tensor cores with TMEM accumulators instead of mma.sync.
+    gmres=True (default factorisation only): each correction by GMRES
+    preconditioned with the FP32 factorisation on FP64 vectors (GMRES-IR), for
+    conditioning the plain refinement stalls on."""
     L = _lib.load()
     A = np.ascontiguousarray(A, np.float64)
     B = np.ascontiguousarray(B, np.float64)
@@ -35,7 +39,8 @@ def solve_mixed(A, B, X_true=None, tol: float = 1e-10, max_iter: int = 10, equil
     fb = np.zeros(cnt, np.int32)
     Xt = None if X_true is None else np.ascontiguousarray(X_true, np.float64)
     flags = ((0 if equilibrate else _lib.MIXED_NO_EQUILIBRATE) | (0 if fallback else _lib.MIXED_NO_FALLBACK)
-             | _FACTOR[factor] | (_lib.MIXED_TCGEN05 if tcgen05 else 0) | (_lib.MIXED_PIVOTED if pivoted else 0))
+             | _FACTOR[factor] | (_lib.MIXED_TCGEN05 if tcgen05 else 0) | (_lib.MIXED_PIVOTED if pivoted else 0)
+             | (_lib.MIXED_GMRES if gmres else 0))
     P = _lib.ptr
     _check(L.nppb_solve_mixed_batched(cnt, n, k, P(A), P(B), P(X), P(Xt), tol, max_iter, flags, P(info),
                                       P(berr), P(ferr), P(iters), P(fb)))

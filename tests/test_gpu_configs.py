@@ -9,7 +9,8 @@ size-independent ones, with oracle parity on a sample:
   normwise backward error computed on the device, and a 256-system sample
   against the oracle at the parity bar (1e-12 * cond(A), signs bit-exact);
 * mixed precision, FP32/TF32 factors + FP64 refinement: 8 x 4096 at
-  kappa 1e2 and 1e4, 64 x 1024 at kappa 1e8 (A = Q1 diag(sigma) Q2^T, sigma
+  kappa 1e2 and 1e4 (and with GMRES refinement at 1e4 and 1e6), 64 x 1024 at
+  kappa 1e8 (plain and GMRES refinement) (A = Q1 diag(sigma) Q2^T, sigma
   log-spaced 1..kappa, b = A x_true): reported and independently recomputed
   backward error <= 1e-10, forward error <= 10 * kappa * 1e-10, solutions
   against the FP64 LU (pivots bit-exact with the oracle up to 4096) and, for
@@ -93,14 +94,18 @@ def _fp64(lib, torch, A, B):
     return X
 
 
-@pytest.mark.parametrize("kappa", [1e2, 1e4])
-def test_mixed_8x4096(lib, kappa):
+@pytest.mark.parametrize("kappa,gmres", [(1e2, False), (1e4, False), (1e4, True), (1e6, True)])
+def test_mixed_8x4096(lib, kappa, gmres):
+    """Plain refinement at kappa 1e2 must not fall back; at 1e4 a system whose
+    block-pivoted factors grew too much may stall and is then refactored in
+    FP64 (flagged); with GMRES refinement no system may fall back at 1e4 or 1e6."""
     torch = _torch()
     A, B, Xt = _conditioned(torch, 8, 4096, kappa, 1, seed=4096 + int(np.log10(kappa)))
-    X, rep = _mixed(lib, torch, A, B, Xt)
+    X, rep = _mixed(lib, torch, A, B, Xt, flags=_lib.MIXED_GMRES if gmres else 0)
     assert not rep["info"].any()
     assert np.all(rep["berr"] <= TOL), rep["berr"]
-    assert np.all(rep["fallback"] == 0), rep
+    if gmres or kappa <= 1e2:
+        assert np.all(rep["fallback"] == 0), rep
     eta = _backward_error(A, B, X).cpu().numpy()
     assert np.all(eta <= TOL), eta  # the reported figure, recomputed independently
     # (a residual of 1e-12 relative is mostly cancellation: the two sums agree to a few digits)
@@ -111,15 +116,19 @@ def test_mixed_8x4096(lib, kappa):
     assert np.all(rel <= 10 * kappa * TOL), rel
 
 
-def test_mixed_64x1024_kappa1e8(lib, oracle):
-    """kappa * u_fp32 > 1: refinement cannot be relied on; every system must
-    still end at the bar, by refinement or by the flagged FP64 refactorisation."""
+@pytest.mark.parametrize("gmres", [False, True])
+def test_mixed_64x1024_kappa1e8(lib, oracle, gmres):
+    """kappa * u_fp32 > 1: plain refinement cannot be relied on; every system
+    must still end at the bar, by refinement or by the flagged FP64
+    refactorisation. GMRES refinement must get there without the fallback."""
     torch = _torch()
     kappa = 1e8
     A, B, Xt = _conditioned(torch, 64, 1024, kappa, 1, seed=1024 + 8)
-    X, rep = _mixed(lib, torch, A, B, Xt)
+    X, rep = _mixed(lib, torch, A, B, Xt, flags=_lib.MIXED_GMRES if gmres else 0)
     assert not rep["info"].any()
     assert np.all(rep["berr"] <= TOL), rep["berr"]
+    if gmres:
+        assert np.all(rep["fallback"] == 0), rep
     eta = _backward_error(A, B, X).cpu().numpy()
     assert np.all(eta <= TOL), eta
     assert np.all(rep["ferr"] <= 10 * kappa * TOL), rep["ferr"]

@@ -100,3 +100,43 @@ def test_pivoted_flag_keeps_the_step_kernels(lib, oracle):
     A, B, Xt = workloads.conditioned_batch(seed=67, count=3, n=200, kappa=1e4, nrhs=2)
     Xp, rp = solve_mixed(A, B, X_true=Xt, pivoted=True)
     _check(oracle, A, B, Xt, Xp, rp, 1e4)
+
+
+# GMRES refinement (Carson and Higham's GMRES-IR on the same FP32 factors)
+
+@pytest.mark.parametrize("n", [256, 640])
+@pytest.mark.parametrize("kappa", [1e6, 1e8])
+def test_gmres_high_kappa(lib, oracle, n, kappa):
+    A, B, Xt = workloads.conditioned_batch(seed=90 + n + int(np.log10(kappa)), count=4, n=n, kappa=kappa, nrhs=1)
+    X, rep = solve_mixed(A, B, X_true=Xt, gmres=True, max_iter=10)
+    _check(oracle, A, B, Xt, X, rep, kappa)
+
+
+def test_gmres_easy_and_multi_rhs(lib, oracle):
+    A, B, Xt = workloads.conditioned_batch(seed=93, count=3, n=300, kappa=1e2, nrhs=1)
+    X, rep = solve_mixed(A, B, X_true=Xt, gmres=True)
+    _check(oracle, A, B, Xt, X, rep, 1e2)
+    A, B, Xt = workloads.conditioned_batch(seed=94, count=3, n=384, kappa=1e6, nrhs=5)
+    X, rep = solve_mixed(A, B, X_true=Xt, gmres=True)
+    _check(oracle, A, B, Xt, X, rep, 1e6)
+
+
+def test_gmres_row_scaled(lib, oracle):
+    A, B, Xt = workloads.conditioned_batch(seed=95, count=4, n=256, kappa=1e4, nrhs=4, row_scale_decades=6)
+    X, rep = solve_mixed(A, B, X_true=Xt, gmres=True)
+    _check(oracle, A, B, Xt, X, rep, 1e4)
+
+
+def test_gmres_alone_and_in_a_batch_agree_bitwise(lib):
+    A, B, Xt = workloads.conditioned_batch(seed=96, count=4, n=300, kappa=1e6, nrhs=2)
+    Xb, rb = solve_mixed(A, B, gmres=True)
+    for s in (0, 2):
+        Xs, rs = solve_mixed(A[s:s + 1], B[s:s + 1], gmres=True)
+        assert np.array_equal(Xs[0], Xb[s]), s
+        assert rs["iters"][0] == rb["iters"][s]
+
+
+def test_gmres_rejects_pivoted(lib):
+    A, B, _ = workloads.conditioned_batch(seed=97, count=1, n=64, kappa=1e2, nrhs=1)
+    with pytest.raises(Exception):
+        solve_mixed(A, B, gmres=True, pivoted=True)
