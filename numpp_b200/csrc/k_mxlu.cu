@@ -6,11 +6,14 @@
 //                  butterfly restricted to the rows {r, r+N/4, r+N/2, r+3N/4}
 //                  is a 4x4 matrix, so each thread maps one 4x4 quad of A to
 //                  one quad of M.
-//  k_mx_transpose  the first block's panel row, transposed (A12^T).
-//  k_mx_diag       LU of the 128 x 128 diagonal block with partial pivoting
-//                  among its own rows (one CTA, the block in shared memory,
-//                  32-column panels factored by one warp in registers), then
-//                  L^-1 P, U^-1 and U^-T by blocked inversion in shared memory.
+//  k_mx_diag       LU of the 256 x 128 window panel (the diagonal block's
+//                  rows and the next block's) with partial pivoting (one CTA,
+//                  the window in shared memory, 32-column panels with the
+//                  rows in registers), then L^-1, U^-1 and U^-T of the block by
+//                  blocked inversion in shared memory, and the window's order.
+//  k_mx_permute    that order applied to the rest of the window's rows; the
+//                  new panel row transposed (A12^T).
+//  k_mx_rowpos     the windows' orders composed: the final position of each row.
 //  k_mx_gemm       C (=|-=) A B^T for 128 x 128 tiles with K = 128: operands
 //                  by TMA in 128-byte-swizzled boxes (two stages of 32-column
 //                  chunks), split into TF32 hi / lo in shared memory, one
@@ -155,21 +158,9 @@ k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const do
     }
 }
 
-// T[buf][s][j][r] = M[s][K + r][j] for r < 128, K + 128 <= j < N.
-__global__ void __launch_bounds__(256)
-k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K, int count, int buf) {
-  __shared__ float t[32][33];
-  const int s = blockIdx.z, j0 = K + kMxNB + blockIdx.x * 32, r0 = blockIdx.y * 32;
-  const float* Ms = M + (int64_t)s * N * N;
-  for (int y = threadIdx.y; y < 32; y += 8) t[y][threadIdx.x] = Ms[(int64_t)(K + r0 + y) * N + j0 + threadIdx.x];
-  __syncthreads();
-  float* Tz = T + ((int64_t)buf * count + s) * N * kMxNB;
-  for (int y = threadIdx.y; y < 32; y += 8) Tz[(int64_t)(j0 + y) * kMxNB + r0 + threadIdx.x] = t[threadIdx.x][y];
-}
-
 // ---------------------------------------------------------------------------
-// Diagonal block: LU with partial pivoting restricted to the block's 128 rows,
-// then (L^-1 P), U^-1 and U^-T.
+// Diagonal block: LU of the 256-row window panel with partial pivoting over
+// the window, then L^-1, U^-1 and U^-T of the 128 rows chosen.
 //
 // LU, in shared memory, blocked by 32-column panels. Rows never move: each
 // physical row of the block gets its position when it is chosen as a pivot
@@ -187,22 +178,24 @@ k_mx_transpose(const float* __restrict__ M, float* __restrict__ T, int N, int K,
 // [U00^-1 -U00^-1 U01 U11^-1; 0 U11^-1], as 32^3 and 64^3 shared-memory GEMMs
 // (temporaries in the quadrants the results leave zero, and at the last level
 // in the factors' diagonal quadrants).
-// Out: the packed LU of P A11 in M, L^-1 P (the permutation folded into the
-// stored inverse, so that U12 = (L^-1 P) A12 and the forward substitution
-// need no row exchanges), U^-1 and U^-T.
+// Out: in M's window rows (position order), the packed LU of the 128 rows
+// chosen and the other rows' multipliers; L^-1, U^-1 and U^-T; the window
+// order (the physical window row of each position). The window rows outside
+// the panel columns are reordered by k_mx_permute.
 constexpr int DT = 256;
 constexpr int DLD = 132;  // leading dimension of the shared 128 x 128 arrays (16-byte rows, 4-bank row offset)
-// shared state of the LU besides the three 128 x DLD arrays
+// shared state of the LU besides the window (256 x DLD) and U^-1 (128 x DLD)
+constexpr int kMxWin = 2 * kMxNB;  // pivot window: the block's rows and the next block's
 struct DiagAux {
-  int pos_of[kMxNB];   // position of each physical row, -1 until chosen as a pivot
-  int phys_of[kMxNB];  // physical row of each position
-  int act[kMxNB];      // rows not yet chosen, after a panel
-  uint32_t keys[2][4];   // per warp: the key of its winner; two buffers (alternating steps)
-  float crow[2][4][32];  // per warp: its winner's panel values
+  int pos_of[kMxWin];    // position of each physical row, -1 until chosen as a pivot
+  int phys_of[kMxWin];   // physical row of each position
+  int act[kMxWin];       // rows not yet chosen, after a panel
+  uint32_t keys[2][8];   // per warp: the key of its winner; two buffers (alternating steps)
+  float crow[2][8][32];  // per warp: its winner's panel values
   float lcol[32][32];    // the panel's L11 columns below the diagonal (shifted to index 0)
   int fail;  // 1 + first position whose pivot failed, INT_MAX if none
 };
-constexpr size_t kDiagSmem = sizeof(float) * (3 * kMxNB * DLD) + sizeof(DiagAux);
+constexpr size_t kDiagSmem = sizeof(float) * ((kMxWin + kMxNB) * DLD) + sizeof(DiagAux);
 
 // Inverse of one 32 x 32 diagonal block of the packed factors at (o, o), one
 // warp, lane = column: unit lower (L) by substitution down, upper (U) up.
@@ -294,22 +287,22 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
-// Panel of the LU (columns c0 .. c0+31) on warps 0-3, thread t = physical row
-// t, in a rolled loop over the steps (the code stays small: this kernel is
-// otherwise bound by instruction fetch). At step j a row's 32 registers hold
-// its values in columns c0 + j .. c0 + j + 31 (shifted left by one every step
-// while the row is not chosen, so register indices are static). Step j: each
-// warp's largest key (magnitude with its 7 low mantissa bits dropped, plus
-// one) << 7 | (127 - row) over the rows not yet chosen by one warp reduction;
-// lane 0 publishes it and the warp's winner its values; one named barrier over
-// the four warps; the overall winner (the largest |a[j]| up to a relative
-// 2^-16, the lowest row among those) takes position c0 + j, and every row not
-// yet chosen stores l = a[j] / pivot and updates its values right of j. Keys
-// and rows sit in two alternating buffers, so one barrier per step suffices.
-__device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t) {
+// Panel of the LU (columns c0 .. c0+31) on the eight warps, thread t =
+// physical row t of the window (R rows), in a rolled loop over the steps (the
+// code stays small). At step j a row's 32 registers hold its values in
+// columns c0 + j .. c0 + j + 31 (shifted left by one every step while the row
+// is not chosen, so register indices are static). Step j: each warp's largest
+// key (magnitude with its 8 low mantissa bits dropped, plus one) << 8 |
+// (255 - row) over the rows not yet chosen by one warp reduction; lane 0
+// publishes it and the warp's winner its values (predicated stores); one
+// barrier; the overall winner (the largest |a[j]| up to a relative 2^-15, the
+// lowest row among those) takes position c0 + j, and every row not yet chosen
+// stores l = a[j] / pivot and updates its values right of j. Keys and rows sit
+// in two alternating buffers, so one barrier per step suffices.
+__device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t, int R) {
   constexpr unsigned FULL = 0xffffffffu;
   const int w = t >> 5, lane = t & 31;
-  const bool was = ax.pos_of[t] >= 0;
+  const bool was = t >= R || ax.pos_of[t] >= 0;  // rows past the window never compete
   bool done = was;
   int jd = 0;         // step at which this row was chosen
   int bad = INT_MAX;  // 1 + position of this row if its pivot failed
@@ -329,16 +322,17 @@ __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t
   for (int j = 0; j < 32; ++j) {
     const int b = j & 1;
     const uint32_t key =
-        done ? 0u : ((((__float_as_uint(fabsf(v[0])) >> 7) + 1u) << 7) | (uint32_t)(127 - t));
+        done ? 0u : ((((__float_as_uint(fabsf(v[0])) >> 8) + 1u) << 8) | (uint32_t)(255 - t));
     const uint32_t wkey = __reduce_max_sync(FULL, key);
     // predicated stores, not a divergent branch (a one-lane branch around
     // these stores costs several times their latency)
     st_shared_u32_if(lane == 0, smem_addr(&ax.keys[b][w]), wkey);
-    st_shared_row_if(wkey != 0u && t == 127 - (int)(wkey & 127u), smem_addr(ax.crow[b][w]), v);
-    asm volatile("bar.sync 1, 128;\n" ::: "memory");
-    const uint4 kk = *reinterpret_cast<const uint4*>(ax.keys[b]);
-    const uint32_t best = max(max(kk.x, kk.y), max(kk.z, kk.w));
-    const int prow = 127 - (int)(best & 127u);
+    st_shared_row_if(wkey != 0u && t == 255 - (int)(wkey & 255u), smem_addr(ax.crow[b][w]), v);
+    asm volatile("bar.sync 1, 256;\n" ::: "memory");
+    const uint4 k0 = *reinterpret_cast<const uint4*>(ax.keys[b]);
+    const uint4 k1 = *reinterpret_cast<const uint4*>(ax.keys[b] + 4);
+    const uint32_t best = max(max(max(k0.x, k0.y), max(k0.z, k0.w)), max(max(k1.x, k1.y), max(k1.z, k1.w)));
+    const int prow = 255 - (int)(best & 255u);
     const float* pr = ax.crow[b][prow >> 5];
     // the winner's bookkeeping without a branch
     const bool win = t == prow;
@@ -375,29 +369,29 @@ __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t
 
 __global__ void __launch_bounds__(DT, 1)
 k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
-          int32_t* __restrict__ info, int N, int k) {
+          int32_t* __restrict__ perm, int32_t* __restrict__ info, int N, int k) {
   extern __shared__ __align__(16) float dsm[];
-  float* W0 = dsm;                   // [128][DLD] the block by physical row; later L^-1
-  float* W1 = W0 + kMxNB * DLD;      // [128][DLD] the packed factors in position order
-  float* Ui = W1 + kMxNB * DLD;      // [128][DLD] U^-1
+  float* W0 = dsm;                    // [256][DLD] the window by physical row; later L^-1 and the factors
+  float* Ui = W0 + kMxWin * DLD;      // [128][DLD] U^-1 (first the factors in position order)
   DiagAux& ax = *reinterpret_cast<DiagAux*>(Ui + kMxNB * DLD);
   const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int R = min(kMxWin, N - K);  // window rows: this block's and the next block's
   constexpr unsigned FULL = 0xffffffffu;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
-  for (int idx = tid; idx < kMxNB * 32; idx += DT) {
+  for (int idx = tid; idx < R * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
     *reinterpret_cast<float4*>(W0 + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
   }
-  if (tid < kMxNB) ax.pos_of[tid] = -1;
+  ax.pos_of[tid] = -1;  // DT == kMxWin: one entry per thread
   if (tid == 0) ax.fail = INT_MAX;
   __syncthreads();
 #pragma unroll 1
   for (int p = 0; p < 4; ++p) {
     const int c0 = 32 * p;
-    if (warp < 4) diag_panel(W0, ax, c0, tid);
+    diag_panel(W0, ax, c0, tid, R);
     __syncthreads();
-    if (p == 3) break;
-    const int W = kMxNB - c0 - 32;  // trailing columns (and rows not yet chosen)
+    const int W = kMxNB - c0 - 32;  // trailing columns of the block
+    const int Rn = R - c0 - 32;     // rows not yet chosen
     if (tid < W) {
       // U12 = L11^-1 A12 on the panel's pivot rows, thread = column, in a
       // rolled loop: v[i] holds position c0 + j + i at step j (shifted like
@@ -430,23 +424,25 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
       }
       W0[ax.phys_of[c0 + 31] * DLD + c] = v[0];
     } else if (warp == 4) {
-      // the rows not yet chosen, in physical order
+      // the rows not yet chosen, in physical order (also after the last panel:
+      // the window's rows that stay below the block)
       int base = 0;
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < kMxWin / 32; ++q) {
         const int r = 32 * q + lane;
-        const bool nd = ax.pos_of[r] < 0;
+        const bool nd = r < R && ax.pos_of[r] < 0;
         const unsigned m = __ballot_sync(FULL, nd);
         if (nd) ax.act[base + __popc(m & ((1u << lane) - 1u))] = r;
         base += __popc(m);
       }
     }
     __syncthreads();
+    if (p == 3) break;
     // A22 -= L21 U12: 4 rows (of act) x 4 columns per task
     {
-      const int ng = W >> 2, ntask = ng * ng;
+      const int ngc = W >> 2, ntask = (Rn >> 2) * ngc;
       for (int task = tid; task < ntask; task += DT) {
-        const int rg = task / ng, cc = c0 + 32 + 4 * (task - rg * ng);
+        const int rg = task / ngc, cc = c0 + 32 + 4 * (task - rg * ngc);
         float* rp[4];
         float4 acc[4];
 #pragma unroll
@@ -472,17 +468,25 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
     }
     __syncthreads();
   }
-  // the packed factors in position order: to W1 and M
-  for (int idx = tid; idx < kMxNB * 32; idx += DT) {
+  // the window's order: positions 0..127 the pivots, 128..R-1 the other rows
+  // (their panel values are now their multipliers, L21 = A21 U11^-1)
+  int32_t* pw = perm + ((int64_t)s * (N / kMxNB) + k) * kMxWin;
+  if (tid < R) pw[tid] = tid < kMxNB ? ax.phys_of[tid] : ax.act[tid - kMxNB];
+  for (int idx = tid; idx < R * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
-    const float4 v = *reinterpret_cast<const float4*>(W0 + ax.phys_of[r] * DLD + c);
-    *reinterpret_cast<float4*>(W1 + r * DLD + c) = v;
+    const int ph = r < kMxNB ? ax.phys_of[r] : ax.act[r - kMxNB];
+    const float4 v = *reinterpret_cast<const float4*>(W0 + ph * DLD + c);
     *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = v;
+    if (r < kMxNB) *reinterpret_cast<float4*>(Ui + r * DLD + c) = v;  // the factors, position order
   }
   __syncthreads();
-  float* LU = W1;
+  float* LU = W0 + kMxNB * DLD;
   float* Li = W0;
-  const int* posOf = ax.pos_of;
+  for (int idx = tid; idx < kMxNB * 32; idx += DT) {
+    const int r = idx >> 5, c = (idx & 31) * 4;
+    *reinterpret_cast<float4*>(LU + r * DLD + c) = *reinterpret_cast<const float4*>(Ui + r * DLD + c);
+  }
+  __syncthreads();
   for (int idx = tid; idx < kMxNB * DLD; idx += DT) {
     Li[idx] = 0.f;
     Ui[idx] = 0.f;
@@ -527,8 +531,8 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   float* Ub = Uinv + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   float* UTb = UinvT + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   for (int idx = tid; idx < kMxNB * kMxNB; idx += DT) {
-    const int r = idx >> 7, c = idx & 127, pc = posOf[c];
-    Lb[idx] = pc <= r ? Li[r * DLD + pc] : 0.f;      // (L^-1 P)[r][c]
+    const int r = idx >> 7, c = idx & 127;
+    Lb[idx] = c <= r ? Li[r * DLD + c] : 0.f;        // L^-1[r][c] (rows already in position order)
     Ub[idx] = c >= r ? Ui[r * DLD + c] : 0.f;        // U^-1[r][c]
     UTb[idx] = r >= c ? Ui[c * DLD + r] : 0.f;       // U^-T[r][c]
   }
@@ -547,10 +551,10 @@ struct MxGemmArgs {
   int bx, by, bz;  // B (stored as B^T: row = output column) of tile (nt = 0)
   int cx, cy, cz;  // C tile (0, 0)
   int split3;
-  // tile of this CTA: cross = 1: blockIdx.x < tiles -> (0, blockIdx.x), else
-  // (blockIdx.x - tiles + 1, 0) (the next block's panel row and column);
-  // cross = 0: (blockIdx.y + toff, blockIdx.x + toff)
-  int cross, tiles, toff;
+  // tile (mt, nt) of this CTA: cross = 1: the first two tile rows and the
+  // first tile column (x < tiles: (0, x); x < 2 tiles: (1, x - tiles); else
+  // (x - 2 tiles + 2, 0)); cross = 0: (blockIdx.y + moff, blockIdx.x + noff)
+  int cross, tiles, moff, noff;
   // optional transposed copy of each result element (r, c) of tile (mt, nt):
   // tr + s * tr_sys + (tr_r0 + 128 mt + r) * tr_row + (tr_c0 + 128 nt + c) * tr_col
   float* tr;
@@ -671,9 +675,9 @@ k_mx_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
   int* abort_flag = reinterpret_cast<int*>(bars + 7);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int s = blockIdx.z;
-  const bool in_row = !g.cross || (int)blockIdx.x < g.tiles;
-  const int nt = g.cross ? (in_row ? (int)blockIdx.x : 0) : (int)blockIdx.x + g.toff;
-  const int mt = g.cross ? (in_row ? 0 : (int)blockIdx.x - g.tiles + 1) : (int)blockIdx.y + g.toff;
+  const int bx = (int)blockIdx.x;
+  const int mt = !g.cross ? (int)blockIdx.y + g.moff : bx < g.tiles ? 0 : bx < 2 * g.tiles ? 1 : bx - 2 * g.tiles + 2;
+  const int nt = !g.cross ? bx + g.noff : bx < g.tiles ? bx : bx < 2 * g.tiles ? bx - g.tiles : 0;
   const uint32_t bar0 = smem_u32(bars);
   auto full = [&](int st) { return bar0 + 8u * st; };
   auto freed = [&](int st) { return bar0 + 16u + 8u * st; };
@@ -1072,11 +1076,73 @@ k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const f
   cluster.sync();  // no CTA leaves while a peer may still write into its shared memory
 }
 
-// Y = U^T pad(R): thread per (row quad, right-hand side).
+// Window k's row order applied to the rest of its rows (the row interchanges
+// of LAPACK's getrf, left of the block as well as right of it, so that the
+// factors end in one global row order), and the block's new panel row,
+// transposed, into T[buf]: CTA per (64-column chunk, system); the panel
+// columns themselves were written in order by the diagonal kernel.
+constexpr int PC = 64, PLD = PC + 1;  // columns per CTA; odd row stride: conflict-free columns
+constexpr size_t kPermSmem = sizeof(float) * kMxWin * PLD;
+__global__ void __launch_bounds__(256)
+k_mx_permute(float* __restrict__ M, float* __restrict__ T, const int32_t* __restrict__ perm, int N, int k,
+             int count, int buf) {
+  __shared__ int pw[kMxWin];
+  extern __shared__ float psm[];  // [R][PLD]
+  const int s = blockIdx.y, c0 = blockIdx.x * PC, K = k * kMxNB, R = min(kMxWin, N - K);
+  if (c0 >= K && c0 < K + kMxNB) return;
+  const int32_t* pp = perm + ((int64_t)s * (N / kMxNB) + k) * kMxWin;
+  for (int i = threadIdx.x; i < R; i += 256) pw[i] = pp[i];
+  float* Ms = M + (int64_t)s * N * N + (int64_t)K * N + c0;
+  for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
+    const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
+    const float4 v = *reinterpret_cast<const float4*>(Ms + (int64_t)r * N + c);
+    float* d = psm + r * PLD + c;
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
+    const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
+    const float* q = psm + pw[r] * PLD + c;
+    *reinterpret_cast<float4*>(Ms + (int64_t)r * N + c) = make_float4(q[0], q[1], q[2], q[3]);
+  }
+  if (c0 >= K + kMxNB) {  // T[col][row] for the block's 128 rows
+    float* Tz = T + ((int64_t)buf * count + s) * N * kMxNB + (int64_t)c0 * kMxNB;
+    for (int idx = threadIdx.x; idx < PC * kMxNB; idx += 256) {
+      const int c = idx / kMxNB, r = idx % kMxNB;
+      Tz[(int64_t)c * kMxNB + r] = psm[pw[r] * PLD + c];
+    }
+  }
+}
+
+// Position of every row of M in the final order: the windows' orders
+// composed in sequence (one CTA per system).
+__global__ void __launch_bounds__(256)
+k_mx_rowpos(const int32_t* __restrict__ perm, int32_t* __restrict__ rowpos, int N) {
+  extern __shared__ int at[];  // [N] the original row now at each position, then [kMxWin] scratch
+  int* tmp = at + N;
+  const int s = blockIdx.x, nb = N / kMxNB;
+  for (int i = threadIdx.x; i < N; i += 256) at[i] = i;
+  __syncthreads();
+  for (int k = 0; k < nb; ++k) {
+    const int K = k * kMxNB, R = min(kMxWin, N - K);
+    const int32_t* pw = perm + ((int64_t)s * nb + k) * kMxWin;
+    for (int j = threadIdx.x; j < R; j += 256) tmp[j] = at[K + pw[j]];
+    __syncthreads();
+    for (int j = threadIdx.x; j < R; j += 256) at[K + j] = tmp[j];
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < N; i += 256) rowpos[(int64_t)s * N + at[i]] = i;
+}
+
+// Y = P U^T pad(R) (P: the factorisation's row order): thread per (row quad, right-hand side).
 template <class TR, class TY>
 __global__ void __launch_bounds__(256)
 k_mx_rhs_in(const TR* __restrict__ R, TY* __restrict__ Y, int n, int N, int nrhs,
-            const RefineState* __restrict__ st, int only_active, const double* __restrict__ tab) {
+            const RefineState* __restrict__ st, int only_active, const double* __restrict__ tab,
+            const int32_t* __restrict__ rowpos) {
   const int s = blockIdx.y;
   if (only_active && st[s].status != kRefineActive) return;
   const int q = N / 4;
@@ -1096,7 +1162,7 @@ k_mx_rhs_in(const TR* __restrict__ R, TY* __restrict__ Y, int n, int N, int nrhs
     double v = 0.0;
 #pragma unroll
     for (int b = 0; b < 4; ++b) v = fma(U[b][a], x[b], v);
-    Y[((int64_t)s * N + r + a * q) * nrhs + col] = (TY)v;
+    Y[((int64_t)s * N + rowpos[(int64_t)s * N + r + a * q]) * nrhs + col] = (TY)v;
   }
 }
 
@@ -1166,7 +1232,8 @@ size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 size_t mx_workspace_bytes(int count, int n) {
   const size_t N = (size_t)mx_padded(n), c = (size_t)count;
   return align256(4 * c * N * N) + align256(4 * 2 * c * N * kMxNB) + 3 * align256(4 * c * N * kMxNB) +
-         align256(4 * c) + align256(sizeof(double) * 12 * (N / 2));
+         align256(4 * c) + align256(sizeof(double) * 12 * (N / 2)) + align256(4 * c * (N / kMxNB) * kMxWin) +
+         align256(4 * c * N);
 }
 
 void mx_carve(MxBufs& b, void* base, int count, int n) {
@@ -1188,6 +1255,10 @@ void mx_carve(MxBufs& b, void* base, int count, int n) {
   b.info = reinterpret_cast<int32_t*>(p);
   p += align256(4 * c);
   b.rbt = reinterpret_cast<double*>(p);
+  p += align256(sizeof(double) * 12 * (N / 2));
+  b.perm = reinterpret_cast<int32_t*>(p);
+  p += align256(4 * c * (N / kMxNB) * kMxWin);
+  b.rowpos = reinterpret_cast<int32_t*>(p);
 }
 
 cudaError_t mx_prepare() {
@@ -1196,6 +1267,8 @@ cudaError_t mx_prepare() {
     e = cudaFuncSetAttribute(k_mx_gemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPermSmem);
   const int csm = (int)(sizeof(float) * ((size_t)4096 * 8 + 3 * kMxNB * 8));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
@@ -1276,13 +1349,15 @@ MxStreams* mx_streams() {
 
 }  // namespace
 
-// Blocked factorisation with look-ahead. On the panel stream: block k's
-// diagonal factor and triangular solves, then the cross of its trailing
-// update that block k+1 needs (the first row and column of 128 x 128 tiles);
-// on the side stream, once block k's triangular solves are done, the rest of
-// its trailing update. Block k+1's diagonal factor and solves therefore run
-// beside the bulk of block k's update; block k+1's trailing update waits for
-// it. Every element sees the same operations in the same order either way.
+// Blocked factorisation with look-ahead. Per block k, on the panel stream:
+// the diagonal kernel (pivots from the 256-row window), the window's row
+// order applied to the rest of its rows (and the new panel row transposed),
+// L21 for the rows below the window, U12, and the part of the trailing update
+// the next window needs (its two 128-row tile rows and the next panel column);
+// on the side stream, once U12 is in, the rest of the trailing update. Block
+// k+1's diagonal factor, row order and solves therefore run beside the bulk of
+// block k's update; block k+1's trailing update waits for it. Every element
+// sees the same operations in the same order either way.
 cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
   const int N = b.N, count = b.count, nb = N / kMxNB;
   CUtensorMap mM, mT, mL, mUT;
@@ -1293,11 +1368,6 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
   cudaStream_t ps = ms ? ms->panel : s, ss = ms ? ms->side : s;
   cudaError_t e = cudaMemsetAsync(b.info, 0, sizeof(int32_t) * count, s);
   if (e != cudaSuccess) return e;
-  if (nb > 1) {
-    k_mx_transpose<<<dim3((unsigned)((N - kMxNB) / 32), kMxNB / 32, (unsigned)count), dim3(32, 8), 0, s>>>(
-        b.M, b.T, N, 0, count, 0);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
   if (ms) {  // the panel stream starts behind everything queued on s
     if ((e = cudaEventRecord(ms->ev[0], s)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(ps, ms->ev[0], 0)) != cudaSuccess) return e;
@@ -1306,19 +1376,25 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
   int buf = 0;
   for (int k = 0; k < nb; ++k) {
     const int K = k * kMxNB, tiles = nb - k - 1;
-    // block k's panel was last written by block k-1's cross, earlier on ps
-    k_mx_diag<<<count, DT, kDiagSmem, ps>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.info, N, k);
+    // block k's window was last written by block k-1's cross update, earlier on ps
+    k_mx_diag<<<count, DT, kDiagSmem, ps>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.perm, b.info, N, k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_mx_permute<<<dim3((unsigned)(N / PC), (unsigned)count), 256, kPermSmem, ps>>>(b.M, b.T, b.perm, N, k, count,
+                                                                                   buf);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (tiles == 0) break;
     MxGemmArgs g{};
     g.split3 = b.split3;
-    // L21 = A21 U11^-1: B^T = U11^-T (block k of UinvT)
-    g.ax = K; g.ay = K + kMxNB; g.az = 0;
-    g.bx = 0; g.by = K; g.bz = 0;
-    g.cx = K; g.cy = K + kMxNB; g.cz = 0;
-    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mUT, mM, g);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // U12^T = A12^T (L11^-1 P)^T: B^T = L11^-1 P (block k of Linv); U12 also written back into M's panel row
+    if (tiles > 1) {
+      // L21 = A21 U11^-1 below the window (the window's rows got theirs from the
+      // diagonal kernel): B^T = U11^-T (block k of UinvT)
+      g.ax = K; g.ay = K + 2 * kMxNB; g.az = 0;
+      g.bx = 0; g.by = K; g.bz = 0;
+      g.cx = K; g.cy = K + 2 * kMxNB; g.cz = 0;
+      k_mx_gemm<0><<<dim3(1, (unsigned)(tiles - 1), (unsigned)count), GT, kGemmSmem, ps>>>(mM, mUT, mM, g);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    // U12^T = A12^T L11^-T: B^T = L11^-1 (block k of Linv); U12 also written back into M's panel row
     g.ax = 0; g.ay = K + kMxNB; g.az = buf * count;
     g.bx = 0; g.by = K; g.bz = 0;
     g.cx = 0; g.cy = K + kMxNB; g.cz = buf * count;
@@ -1326,29 +1402,28 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
     g.tr_mt0_only = 0;
     k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mT, mL, mT, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    // A22 -= L21 U12 over the trailing tiles; tile row 0 also writes the next panel row, transposed
+    // A22 -= L21 U12 over the trailing tiles
     g.ax = K; g.ay = K + kMxNB; g.az = 0;
     g.bx = 0; g.by = K + kMxNB; g.bz = buf * count;
     g.cx = K + kMxNB; g.cy = K + kMxNB; g.cz = 0;
-    g.tr = b.T + (int64_t)(buf ^ 1) * count * N * kMxNB;
-    g.tr_sys = (int64_t)N * kMxNB; g.tr_col = kMxNB; g.tr_row = 1; g.tr_c0 = K + kMxNB; g.tr_r0 = 0;
-    g.tr_mt0_only = 1;
+    g.tr = nullptr;
     g.tiles = tiles;
-    if (ms && tiles > 1) {
-      // the bulk (tiles >= 1 in both directions) on the side stream once the solves are in;
-      // the previous bulk is ahead of it on the same stream
+    if (ms && tiles > 2) {
+      // the bulk (tile rows >= 2, tile columns >= 1) on the side stream once
+      // the solves are in; the previous bulk is ahead of it on the same stream
       if ((e = cudaEventRecord(ms->ev[1], ps)) != cudaSuccess) return e;
       if ((e = cudaStreamWaitEvent(ss, ms->ev[1], 0)) != cudaSuccess) return e;
       MxGemmArgs gr = g;
       gr.cross = 0;
-      gr.toff = 1;
-      k_mx_gemm<1><<<dim3((unsigned)(tiles - 1), (unsigned)(tiles - 1), (unsigned)count), GT, kGemmSmem, ss>>>(
+      gr.moff = 2;
+      gr.noff = 1;
+      k_mx_gemm<1><<<dim3((unsigned)(tiles - 1), (unsigned)(tiles - 2), (unsigned)count), GT, kGemmSmem, ss>>>(
           mM, mT, mM, gr);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       // the cross on the panel stream; it touches tiles the previous bulk updated
       if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
       g.cross = 1;
-      k_mx_gemm<1><<<dim3((unsigned)(2 * tiles - 1), 1, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
+      k_mx_gemm<1><<<dim3((unsigned)(3 * tiles - 2), 1, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if ((e = cudaEventRecord(ms->ev[2], ss)) != cudaSuccess) return e;
       rest_pending = true;
@@ -1356,12 +1431,15 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
       if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
       rest_pending = false;
       g.cross = 0;
-      g.toff = 0;
+      g.moff = g.noff = 0;
       k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     buf ^= 1;
   }
+  // the global row order of the factors, for the substitutions' right-hand sides
+  k_mx_rowpos<<<count, 256, sizeof(int) * (N + kMxWin), ps>>>(b.perm, b.rowpos, N);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (ms) {  // s resumes behind both streams
     if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
     if ((e = cudaEventRecord(ms->ev[3], ps)) != cudaSuccess) return e;
@@ -1374,7 +1452,7 @@ cudaError_t mx_rhs_in(const float* R, float* Y, int nrhs, const RefineState* st,
                       cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
   k_mx_rhs_in<float, float><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
-      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt);
+      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt, b.rowpos);
   return cudaGetLastError();
 }
 
@@ -1445,7 +1523,7 @@ cudaError_t mx_rhs_in64(const double* R, double* Y, int nrhs, const RefineState*
                         const MxBufs& b, cudaStream_t s) {
   const int work = b.N / 4 * nrhs;
   k_mx_rhs_in<double, double><<<dim3((unsigned)((work + 255) / 256), (unsigned)b.count), 256, 0, s>>>(
-      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt);
+      R, Y, b.n, b.N, nrhs, st, only_active, b.rbt, b.rowpos);
   return cudaGetLastError();
 }
 

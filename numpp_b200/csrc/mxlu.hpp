@@ -8,14 +8,21 @@
 // differ: the equilibrated matrix is mixed by a depth-2 recursive butterfly
 // transform on both sides (Parker; Baboulin, Dongarra, Herrmann and Tomov,
 // ACM TOMS 39(2), 2013), M = U^T (Dr A Dc) V, and M is factored in 128-column
-// blocks with partial pivoting restricted to each diagonal block's own rows.
+// blocks with partial pivoting over a window of 256 rows: the diagonal
+// block's and the next block's (the multipliers stay below 2 in practice where
+// pivoting within the block alone let them reach 1e2 and more).
 // Per block k (K = 128 k):
-//   diag   P11 M11 = L11 U11 in one CTA, with (L11^-1 P11) and U11^-1 (Gauss
-//          elimination on the same row operations), one CTA per system;
-//   trsmL  L21 = A21 U11^-1               (tcgen05 GEMM, K = 128)
-//   trsmU  U12^T = A12^T (L11^-1 P11)^T   (tcgen05 GEMM on the transposed panel row)
-//   trail  A22 -= L21 U12                 (tcgen05 GEMM, K = 128); the first
-//          128-row tile also writes the next block's transposed panel row.
+//   diag   the 256 x 128 window panel factored with partial pivoting in one
+//          CTA per system: the packed L11 U11 of the 128 rows chosen, the other
+//          rows' multipliers (their L21), L11^-1 and U11^-1 (blocked
+//          inversion), and the window's row order;
+//   perm   that order applied to the rest of the window's rows, left and right
+//          of the block (as LAPACK's row interchanges), and the new panel row
+//          transposed;
+//   trsmL  L21 = A21 U11^-1 below the window  (tcgen05 GEMM, K = 128)
+//   trsmU  U12^T = A12^T L11^-T               (tcgen05 GEMM on the transposed panel row)
+//   trail  A22 -= L21 U12                     (tcgen05 GEMM, K = 128).
+// The composed row order P goes to the right-hand sides: M = P^T L U.
 // The GEMM operands come in by TMA (non-multicast, this GPU's own memory)
 // in 128-byte-swizzled tiles; products are error-compensated TF32
 // (hi*hi + hi*lo + lo*hi) with FP32 accumulators in TMEM.
@@ -45,10 +52,12 @@ struct MxBufs {
   float* UinvT = nullptr;  // count x N x 128: U_kk^-T
   int32_t* info = nullptr; // count: 0, or 1 + first column whose pivot was zero / not finite
   double* rbt = nullptr;   // 12 x N/2: the butterflies' random diagonals (computed by mx_build)
+  int32_t* perm = nullptr;   // count x N/128 x 256: each block's window order (window row of each position)
+  int32_t* rowpos = nullptr; // count x N: final position of every row of M
   int split3 = 1;          // error-compensated TF32 (1) or plain TF32 (0) products
 };
 
-// Device bytes of the factorisation's buffers for a batch (M, T, Linv, Uinv, UinvT, info, rbt).
+// Device bytes of the factorisation's buffers for a batch (M, T, Linv, Uinv, UinvT, info, rbt, perm, rowpos).
 size_t mx_workspace_bytes(int count, int n);
 // Carve the buffers out of one allocation of mx_workspace_bytes (256-byte aligned).
 void mx_carve(MxBufs& b, void* base, int count, int n);

@@ -107,9 +107,12 @@ def test_pivoted_flag_keeps_the_step_kernels(lib, oracle):
 @pytest.mark.parametrize("n", [256, 640])
 @pytest.mark.parametrize("kappa", [1e6, 1e8])
 def test_gmres_high_kappa(lib, oracle, n, kappa):
+    """kappa 1e6 (where plain refinement stalls): no fallback. kappa 1e8
+    (kappa * u_fp32 > 1): every system at the bar, the FP64 fallback allowed
+    for the systems whose first corrections do not contract."""
     A, B, Xt = workloads.conditioned_batch(seed=90 + n + int(np.log10(kappa)), count=4, n=n, kappa=kappa, nrhs=1)
     X, rep = solve_mixed(A, B, X_true=Xt, gmres=True, max_iter=10)
-    _check(oracle, A, B, Xt, X, rep, kappa)
+    _check(oracle, A, B, Xt, X, rep, kappa, fallback_ok=kappa > 1e6)
 
 
 def test_gmres_easy_and_multi_rhs(lib, oracle):
