@@ -97,7 +97,7 @@ __device__ __forceinline__ double pow2_scale(double m) {
 
 constexpr int BQX = 128, BQY = 2;  // a block reads 1 KB runs of each of its rows; quads in registers
 
-__global__ void __launch_bounds__(BQX * BQY)
+__global__ void __launch_bounds__(BQX * BQY, 3)
 k_mx_build(const double* __restrict__ A, const double* __restrict__ rs, const double* __restrict__ cmax, int equil,
            double* __restrict__ cs, RefineState* __restrict__ st, float* __restrict__ M, int n, int N,
            const double* __restrict__ tab) {
@@ -663,8 +663,18 @@ __device__ __forceinline__ void split_box(float* raw, float* lo, int tid) {
 
 template <int SUB>
 __global__ void __launch_bounds__(GT, 1)
-k_mx_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mB,
-          const __grid_constant__ CUtensorMap mC, const MxGemmArgs g) {
+k_mx_gemm(const __grid_constant__ CUtensorMap mA1, const __grid_constant__ CUtensorMap mB1,
+          const __grid_constant__ CUtensorMap mC1, const MxGemmArgs g1,
+          const __grid_constant__ CUtensorMap mA2, const __grid_constant__ CUtensorMap mB2,
+          const __grid_constant__ CUtensorMap mC2, const MxGemmArgs g2, int rows1) {
+  // two independent products in one launch: grid rows y < rows1 run the first
+  // (maps 1, args 1), the others the second (tile row y - rows1)
+  const bool second = (int)blockIdx.y >= rows1;
+  const CUtensorMap& mA = second ? mA2 : mA1;
+  const CUtensorMap& mB = second ? mB2 : mB1;
+  const CUtensorMap& mC = second ? mC2 : mC1;
+  const MxGemmArgs& g = second ? g2 : g1;
+  const int by_ = (int)blockIdx.y - (second ? rows1 : 0);
   extern __shared__ __align__(1024) unsigned char gsm_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(gsm_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -676,7 +686,7 @@ k_mx_gemm(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtens
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int s = blockIdx.z;
   const int bx = (int)blockIdx.x;
-  const int mt = !g.cross ? (int)blockIdx.y + g.moff : bx < g.tiles ? 0 : bx < 2 * g.tiles ? 1 : bx - 2 * g.tiles + 2;
+  const int mt = !g.cross ? by_ + g.moff : bx < g.tiles ? 0 : bx < 2 * g.tiles ? 1 : bx - 2 * g.tiles + 2;
   const int nt = !g.cross ? bx + g.noff : bx < g.tiles ? bx : bx < 2 * g.tiles ? bx - g.tiles : 0;
   const uint32_t bar0 = smem_u32(bars);
   auto full = [&](int st) { return bar0 + 8u * st; };
@@ -1383,26 +1393,26 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
                                                                                    buf);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (tiles == 0) break;
-    MxGemmArgs g{};
-    g.split3 = b.split3;
-    if (tiles > 1) {
-      // L21 = A21 U11^-1 below the window (the window's rows got theirs from the
-      // diagonal kernel): B^T = U11^-T (block k of UinvT)
-      g.ax = K; g.ay = K + 2 * kMxNB; g.az = 0;
-      g.bx = 0; g.by = K; g.bz = 0;
-      g.cx = K; g.cy = K + 2 * kMxNB; g.cz = 0;
-      k_mx_gemm<0><<<dim3(1, (unsigned)(tiles - 1), (unsigned)count), GT, kGemmSmem, ps>>>(mM, mUT, mM, g);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    }
-    // U12^T = A12^T L11^-T: B^T = L11^-1 (block k of Linv); U12 also written back into M's panel row
-    g.ax = 0; g.ay = K + kMxNB; g.az = buf * count;
-    g.bx = 0; g.by = K; g.bz = 0;
-    g.cx = 0; g.cy = K + kMxNB; g.cz = buf * count;
-    g.tr = b.M; g.tr_sys = (int64_t)N * N; g.tr_col = N; g.tr_row = 1; g.tr_c0 = K; g.tr_r0 = K + kMxNB;
-    g.tr_mt0_only = 0;
-    k_mx_gemm<0><<<dim3(1, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mT, mL, mT, g);
+    // one launch for the two triangular solves (independent of each other):
+    // L21 = A21 U11^-1 below the window (the window's rows got theirs from the
+    // diagonal kernel): B^T = U11^-T (block k of UinvT); and
+    // U12^T = A12^T L11^-T: B^T = L11^-1 (block k of Linv), U12 also written back into M's panel row
+    MxGemmArgs gl{}, gu{};
+    gl.split3 = gu.split3 = b.split3;
+    gl.ax = K; gl.ay = K + 2 * kMxNB; gl.az = 0;
+    gl.bx = 0; gl.by = K; gl.bz = 0;
+    gl.cx = K; gl.cy = K + 2 * kMxNB; gl.cz = 0;
+    gu.ax = 0; gu.ay = K + kMxNB; gu.az = buf * count;
+    gu.bx = 0; gu.by = K; gu.bz = 0;
+    gu.cx = 0; gu.cy = K + kMxNB; gu.cz = buf * count;
+    gu.tr = b.M; gu.tr_sys = (int64_t)N * N; gu.tr_col = N; gu.tr_row = 1; gu.tr_c0 = K; gu.tr_r0 = K + kMxNB;
+    const int lrows = tiles - 1;
+    k_mx_gemm<0><<<dim3(1, (unsigned)(lrows + tiles), (unsigned)count), GT, kGemmSmem, ps>>>(mM, mUT, mM, gl, mT, mL,
+                                                                                           mT, gu, lrows);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // A22 -= L21 U12 over the trailing tiles
+    MxGemmArgs g{};
+    g.split3 = b.split3;
     g.ax = K; g.ay = K + kMxNB; g.az = 0;
     g.bx = 0; g.by = K + kMxNB; g.bz = buf * count;
     g.cx = K + kMxNB; g.cy = K + kMxNB; g.cz = 0;
@@ -1418,12 +1428,13 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
       gr.moff = 2;
       gr.noff = 1;
       k_mx_gemm<1><<<dim3((unsigned)(tiles - 1), (unsigned)(tiles - 2), (unsigned)count), GT, kGemmSmem, ss>>>(
-          mM, mT, mM, gr);
+          mM, mT, mM, gr, mM, mT, mM, gr, 1 << 30);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       // the cross on the panel stream; it touches tiles the previous bulk updated
       if (rest_pending && (e = cudaStreamWaitEvent(ps, ms->ev[2], 0)) != cudaSuccess) return e;
       g.cross = 1;
-      k_mx_gemm<1><<<dim3((unsigned)(3 * tiles - 2), 1, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
+      k_mx_gemm<1><<<dim3((unsigned)(3 * tiles - 2), 1, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g, mM, mT,
+                                                                                              mM, g, 1 << 30);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if ((e = cudaEventRecord(ms->ev[2], ss)) != cudaSuccess) return e;
       rest_pending = true;
@@ -1432,7 +1443,8 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
       rest_pending = false;
       g.cross = 0;
       g.moff = g.noff = 0;
-      k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g);
+      k_mx_gemm<1><<<dim3((unsigned)tiles, (unsigned)tiles, (unsigned)count), GT, kGemmSmem, ps>>>(mM, mT, mM, g, mM,
+                                                                                               mT, mM, g, 1 << 30);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
     buf ^= 1;
