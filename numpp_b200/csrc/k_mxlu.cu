@@ -1089,15 +1089,16 @@ k_mx_trsv_c(const float* __restrict__ M, const float* __restrict__ Linv, const f
 // Window k's row order applied to the rest of its rows (the row interchanges
 // of LAPACK's getrf, left of the block as well as right of it, so that the
 // factors end in one global row order), and the block's new panel row,
-// transposed, into T[buf]: CTA per (64-column chunk, system); the panel
-// columns themselves were written in order by the diagonal kernel.
-constexpr int PC = 64, PLD = PC + 1;  // columns per CTA; odd row stride: conflict-free columns
+// transposed, into T[buf]: CTA per (64-column chunk, system), the chunk's
+// window rows staged in shared memory; the panel columns themselves were
+// written in order by the diagonal kernel.
+constexpr int PC = 64, PLD = PC + 4;  // columns per CTA; row stride of 16-byte pieces, padded by one piece
 constexpr size_t kPermSmem = sizeof(float) * kMxWin * PLD;
 __global__ void __launch_bounds__(256)
 k_mx_permute(float* __restrict__ M, float* __restrict__ T, const int32_t* __restrict__ perm, int N, int k,
              int count, int buf) {
   __shared__ int pw[kMxWin];
-  extern __shared__ float psm[];  // [R][PLD]
+  extern __shared__ __align__(16) float psm[];  // [R][PLD]
   const int s = blockIdx.y, c0 = blockIdx.x * PC, K = k * kMxNB, R = min(kMxWin, N - K);
   if (c0 >= K && c0 < K + kMxNB) return;
   const int32_t* pp = perm + ((int64_t)s * (N / kMxNB) + k) * kMxWin;
@@ -1105,24 +1106,22 @@ k_mx_permute(float* __restrict__ M, float* __restrict__ T, const int32_t* __rest
   float* Ms = M + (int64_t)s * N * N + (int64_t)K * N + c0;
   for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
     const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
-    const float4 v = *reinterpret_cast<const float4*>(Ms + (int64_t)r * N + c);
-    float* d = psm + r * PLD + c;
-    d[0] = v.x;
-    d[1] = v.y;
-    d[2] = v.z;
-    d[3] = v.w;
+    *reinterpret_cast<float4*>(psm + r * PLD + c) = *reinterpret_cast<const float4*>(Ms + (int64_t)r * N + c);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
     const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
-    const float* q = psm + pw[r] * PLD + c;
-    *reinterpret_cast<float4*>(Ms + (int64_t)r * N + c) = make_float4(q[0], q[1], q[2], q[3]);
+    *reinterpret_cast<float4*>(Ms + (int64_t)r * N + c) = *reinterpret_cast<const float4*>(psm + pw[r] * PLD + c);
   }
-  if (c0 >= K + kMxNB) {  // T[col][row] for the block's 128 rows
+  if (c0 >= K + kMxNB) {  // T[col][row] for the block's 128 rows: thread = (row, 4 columns), rows fastest
     float* Tz = T + ((int64_t)buf * count + s) * N * kMxNB + (int64_t)c0 * kMxNB;
-    for (int idx = threadIdx.x; idx < PC * kMxNB; idx += 256) {
-      const int c = idx / kMxNB, r = idx % kMxNB;
-      Tz[(int64_t)c * kMxNB + r] = psm[pw[r] * PLD + c];
+    for (int idx = threadIdx.x; idx < kMxNB * (PC / 4); idx += 256) {
+      const int r = idx % kMxNB, c = (idx / kMxNB) * 4;
+      const float4 v = *reinterpret_cast<const float4*>(psm + pw[r] * PLD + c);
+      Tz[(int64_t)c * kMxNB + r] = v.x;
+      Tz[(int64_t)(c + 1) * kMxNB + r] = v.y;
+      Tz[(int64_t)(c + 2) * kMxNB + r] = v.z;
+      Tz[(int64_t)(c + 3) * kMxNB + r] = v.w;
     }
   }
 }
