@@ -58,49 +58,69 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* bits, doub
 }
 
 // Row pass, one CTA per (system, kMixedRows rows): row scales, ||A||_inf, and
-// the column maxima of diag(r) |A| over this CTA's rows. A warp takes a row:
-// its maximum and sum, then (with equilibration) the same row again while it
-// is still in L1 / L2, each r |a_ij| into the CTA's column maxima in shared
-// memory (64-bit atomics on the bit patterns of non-negative doubles), which
-// go to the system's maxima once at the end.
+// the column maxima of diag(r) |A| over this CTA's rows. The rows go in groups
+// of eight: a warp takes a row (its maximum and sum), then after a barrier
+// every thread takes its columns of the group's rows again while they are
+// still in cache, keeping its columns' maxima in registers; they go to the
+// system's maxima once at the end.
+constexpr int kEqGroup = MT / 32;                 // rows per group: one per warp
+constexpr int kEqCols = kMixedMaxN / MT;          // columns per thread
 __global__ void __launch_bounds__(MT)
 k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict__ rs,
              double* __restrict__ cmax, RefineState* __restrict__ st) {
-  extern __shared__ unsigned long long cm[];  // [n] column maxima (bit patterns)
+  __shared__ double rsc[kMixedRows];
   __shared__ double red[MT / 32];
   const int s = blockIdx.x, r0 = blockIdx.y * kMixedRows;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int rows = min(kMixedRows, n - r0);
   const double* a = A + (int64_t)s * n * n + (int64_t)r0 * n;
-  if (equil)
-    for (int j = tid; j < n; j += MT) cm[j] = 0ull;
-  __syncthreads();
   double arow = 0.0;
-  for (int i = warp; i < rows; i += MT / 32) {
-    const double* ai = a + (int64_t)i * n;
-    double m = 0.0, sum = 0.0;
+  double cm[kEqCols];
+#pragma unroll
+  for (int t = 0; t < kEqCols; ++t) cm[t] = 0.0;
+  for (int g0 = 0; g0 < rows; g0 += kEqGroup) {
+    const int i = g0 + warp;
+    if (i < rows) {
+      const double* ai = a + (int64_t)i * n;
+      double m = 0.0, sum = 0.0;
 #pragma unroll 8
-    for (int j = lane; j < n; j += 32) {
-      const double v = fabs(ai[j]);
-      m = fmax(m, v);
-      sum += v;
+      for (int j = lane; j < n; j += 32) {
+        const double v = fabs(ai[j]);
+        m = fmax(m, v);
+        sum += v;
+      }
+      m = warp_max(m);
+      sum = warp_sum(sum);
+      const double r = equil ? pow2_scale(m) : 1.0;
+      if (lane == 0) {
+        rsc[i] = r;
+        rs[(int64_t)s * n + r0 + i] = r;
+      }
+      arow = fmax(arow, sum);
     }
-    m = warp_max(m);
-    sum = warp_sum(sum);
-    const double r = equil ? pow2_scale(m) : 1.0;
-    if (lane == 0) rs[(int64_t)s * n + r0 + i] = r;
-    arow = fmax(arow, sum);
-    if (equil) {
-#pragma unroll 8
-      for (int j = lane; j < n; j += 32)
-        atomicMax(&cm[j], (unsigned long long)__double_as_longlong(r * fabs(ai[j])));
+    if (!equil) continue;
+    __syncthreads();  // the group's row scales
+    const int gr = min(kEqGroup, rows - g0);
+#pragma unroll
+    for (int t = 0; t < kEqCols; ++t) {
+      const int j = tid + MT * t;
+      if (j < n) {
+        double m = cm[t];
+#pragma unroll
+        for (int q = 0; q < kEqGroup; ++q)
+          if (q < gr) m = fmax(m, rsc[g0 + q] * fabs(a[(int64_t)(g0 + q) * n + j]));
+        cm[t] = m;
+      }
     }
   }
-  const double anorm = block_max(arow, red);  // includes the barrier after the column maxima
+  const double anorm = block_max(arow, red);
   if (tid == 0) atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&st[s].anorm), anorm);
   if (!equil) return;
-  for (int j = tid; j < n; j += MT)
-    atomicMax(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), cm[j]);
+#pragma unroll
+  for (int t = 0; t < kEqCols; ++t) {
+    const int j = tid + MT * t;
+    if (j < n) atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), cm[t]);
+  }
 }
 
 // Column scales from the maxima, the scaled matrix in FP32, and the state of
@@ -342,7 +362,7 @@ __global__ void k_mark_fp32_failures(const int32_t* __restrict__ info32, RefineS
 cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, float* A32, double* rs, double* cs,
                               double* cmax, RefineState* st, cudaStream_t s) {
   const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
-  k_equil_rows<<<grid, MT, sizeof(unsigned long long) * n, s>>>(A, n, equil, rs, cmax, st);
+  k_equil_rows<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   k_equil_apply<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, cs, A32, st);
@@ -351,7 +371,7 @@ cudaError_t mixed_equilibrate(const double* A, int count, int n, int equil, floa
 cudaError_t mixed_equil_scan(const double* A, int count, int n, int equil, double* rs, double* cmax,
                              RefineState* st, cudaStream_t s) {
   const dim3 grid((unsigned)count, (unsigned)((n + kMixedRows - 1) / kMixedRows));
-  k_equil_rows<<<grid, MT, sizeof(unsigned long long) * n, s>>>(A, n, equil, rs, cmax, st);
+  k_equil_rows<<<grid, MT, 0, s>>>(A, n, equil, rs, cmax, st);
   return cudaGetLastError();
 }
 cudaError_t mixed_scale_rhs(const double* B, int count, int n, int nrhs, const double* rs, float* B32,

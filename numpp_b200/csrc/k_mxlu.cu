@@ -378,6 +378,7 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   const int R = min(kMxWin, N - K);  // window rows: this block's and the next block's
   constexpr unsigned FULL = 0xffffffffu;
   float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
+#pragma unroll 8  // several rows' loads in flight
   for (int idx = tid; idx < R * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
     *reinterpret_cast<float4*>(W0 + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
@@ -1104,11 +1105,13 @@ k_mx_permute(float* __restrict__ M, float* __restrict__ T, const int32_t* __rest
   const int32_t* pp = perm + ((int64_t)s * (N / kMxNB) + k) * kMxWin;
   for (int i = threadIdx.x; i < R; i += 256) pw[i] = pp[i];
   float* Ms = M + (int64_t)s * N * N + (int64_t)K * N + c0;
+#pragma unroll 8  // several rows' loads in flight
   for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
     const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
     *reinterpret_cast<float4*>(psm + r * PLD + c) = *reinterpret_cast<const float4*>(Ms + (int64_t)r * N + c);
   }
   __syncthreads();
+#pragma unroll 8
   for (int idx = threadIdx.x; idx < R * (PC / 4); idx += 256) {
     const int r = idx / (PC / 4), c = (idx % (PC / 4)) * 4;
     *reinterpret_cast<float4*>(Ms + (int64_t)r * N + c) = *reinterpret_cast<const float4*>(psm + pw[r] * PLD + c);
