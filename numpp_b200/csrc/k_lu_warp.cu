@@ -1,19 +1,24 @@
 // Batched LU with partial pivoting for orders n <= 32: one warp per system.
 //
-// Lane r holds row r of A in registers for the whole factorisation. Rows never
-// move: a row exchange only swaps the two lanes' `pos` labels (the row's
-// position in the pivoted order), so a pivot step costs one warp argmax plus
-// one shuffle per trailing column. The algorithm is the reference's unblocked
-// right-looking elimination (src/linalg/linalg.cpp:48-71): at step k the pivot
-// is the first position p >= k with the largest |a[p,k]| (ties go to the lower
-// position, as the reference's strict '>' scan does), multipliers are
-// a[i,k]/a[k,k] and the trailing update is a[i,j] -= f*a[k,j] (one FMA here).
+// Lane r owns row r of A, kept in shared memory (one 32 x 33 tile per warp,
+// loaded coalesced) so that every loop is a rolled loop over a runtime index:
+// fully unrolled code for 32 steps plus the substitutions was bound by
+// instruction fetch. Rows never move: a row exchange only swaps the two lanes'
+// `pos` labels (the row's position in the pivoted order). The algorithm is the
+// reference's unblocked right-looking elimination (src/linalg/linalg.cpp:48-71):
+// at step k the pivot is the first position p >= k with the largest |a[p,k]|
+// (ties go to the lower position, as the reference's strict '>' scan does),
+// found exactly by warp reductions on the bit patterns of |a| (non-negative
+// doubles order like their patterns: high word, then low word, then the lowest
+// position among the lanes holding both); multipliers are a[i,k]/a[k,k] and
+// the trailing update is a[i,j] -= f*a[k,j] (one FMA here). NaN entries are
+// never pivot candidates.
 //
-// The same launch finishes the requested outputs from the registers:
+// The same launch finishes the requested outputs:
 //  * det  = permsign * prod U[i,i] in order i = 0..n-1   (linalg.cpp:393-407)
 //  * slogdet sign / sum log|U[i,i]| in order               (linalg.cpp:408-439)
 //  * X = A^-1 B: X[pos(r)] starts as B[r]; forward (unit L) and back (U)
-//    substitution run across lanes, RC columns at a time  (linalg.cpp:73-90)
+//    substitution run across lanes, up to RC columns at a time (linalg.cpp:73-90)
 //  * inverse = the same solve against I                    (linalg.cpp:105-115)
 //  * LU + ipiv (LAPACK-style swap list, 0-based) for getrf.
 #include <cfloat>
@@ -26,12 +31,14 @@ namespace nppb {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kWarpsPerCta = 4;
+constexpr int kWarpsPerCta = 2;  // small batches spread over more SMs
+constexpr int kLd = 33;          // row stride of a warp's tile (doubles): conflict-free columns
 
 template <int NP, int RC>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   __shared__ int s_lane_of_pos[kWarpsPerCta][32];
+  __shared__ double s_rows[kWarpsPerCta][32 * kLd];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = blockIdx.x * kWarpsPerCta + wib;
@@ -41,17 +48,17 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   const int n = v.n;
   const int flags = bt.flags;
   const bool live = lane < n;
+  double* R = s_rows[wib];
+  double* row = R + lane * kLd;  // this lane's row
 
-  double a[NP];
-  if (flags & kSolveOnly) {
-    // getrs from a stored factorisation: LU rows are already in pivoted order,
-    // so lane r holds position r; the right-hand side is gathered through ipiv.
-#pragma unroll 64
-    for (int j = 0; j < NP; ++j) a[j] = (live && j < n) ? v.LU[(int64_t)lane * n + j] : 0.0;
-  } else {
-#pragma unroll 64
-    for (int j = 0; j < NP; ++j) a[j] = (live && j < n) ? v.A[(int64_t)lane * n + j] : 0.0;
+  {
+    // coalesced: lane c reads column c of each row in turn
+    const double* src = (flags & kSolveOnly) ? v.LU : v.A;
+#pragma unroll 4
+    for (int r = 0; r < n; ++r)
+      if (live) R[r * kLd + lane] = src[(int64_t)r * n + lane];
   }
+  __syncwarp();
 
   int pos = lane;
   int info = 0;
@@ -61,21 +68,23 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   int orig = lane;
 
   if (!(flags & kSolveOnly)) {
-#pragma unroll 64
-    for (int k = 0; k < NP; ++k) {
-      if (k >= n || info) continue;
-      const bool nopiv = flags & kNoPivot;
+    const bool nopiv = flags & kNoPivot;
+#pragma unroll 1
+    for (int k = 0; k < n; ++k) {
       const bool cand = live && (nopiv ? pos == k : pos >= k);
+      const double akk = live ? row[k] : 0.0;
       // without pivoting the diagonal is the only candidate; <= 0 counts as a zero pivot
-      double best = cand ? (nopiv ? (a[k] > 0.0 ? a[k] : 0.0) : fabs(a[k])) : -1.0;
-      int key = cand ? pos : INT_MAX;
-#pragma unroll 64
-      for (int off = 16; off; off >>= 1) {
-        const double ob = __shfl_xor_sync(kFull, best, off);
-        const int ok = __shfl_xor_sync(kFull, key, off);
-        if (ob > best || (ob == best && ok < key)) { best = ob; key = ok; }
+      const double mag = cand ? (nopiv ? (akk > 0.0 ? akk : 0.0) : fabs(akk)) : 0.0;
+      const unsigned long long bits = (mag == mag) ? (unsigned long long)__double_as_longlong(mag) : 0ull;
+      const uint32_t hi = (uint32_t)(bits >> 32), lo = (uint32_t)bits;
+      const uint32_t mhi = __reduce_max_sync(kFull, hi);
+      const uint32_t mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+      if ((mhi | mlo) == 0u) {  // no nonzero candidate: singular
+        info = k + 1;
+        break;
       }
-      if (best == 0.0) { info = k + 1; continue; }  // exact zero pivot: singular
+      const bool top = cand && hi == mhi && lo == mlo;
+      const int key = (int)__reduce_min_sync(kFull, top ? (uint32_t)pos : 0xffffffffu);
       const int pl = __ffs(__ballot_sync(kFull, live && pos == key)) - 1;
       const int kl = __ffs(__ballot_sync(kFull, live && pos == k)) - 1;
       if (key != k) {
@@ -84,17 +93,16 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
         ++nswap;
       }
       if ((flags & kWantLU) && lane == 0) v.ipiv[k] = key;
-      const double pk = __shfl_sync(kFull, a[k], pl);
+      const double* prow = R + pl * kLd;
+      const double pk = prow[k];
       if (lane == pl) dg = pk;
-      const bool below = live && pos > k;
-      double f = 0.0;
-      if (below) { f = a[k] / pk; a[k] = f; }
-#pragma unroll 64
-      for (int j = k + 1; j < NP; ++j) {
-        // columns j >= n are zero in every row, so the update leaves them zero
-        const double pj = __shfl_sync(kFull, a[j], pl);
-        if (below) a[j] = fma(-f, pj, a[j]);
+      if (live && pos > k) {
+        const double f = row[k] / pk;
+        row[k] = f;
+#pragma unroll 4
+        for (int j = k + 1; j < n; ++j) row[j] = fma(-f, prow[j], row[j]);
       }
+      __syncwarp();
     }
   } else {
     // Replay the stored swap list to find which original row each position holds.
@@ -118,10 +126,11 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   __syncwarp();
   const int* lop = s_lane_of_pos[wib];
 
-  if ((flags & kWantLU) && !(flags & kSolveOnly) && live) {
-#pragma unroll 64
-    for (int j = 0; j < NP; ++j)
-      if (j < n) v.LU[(int64_t)pos * n + j] = a[j];
+  if ((flags & kWantLU) && !(flags & kSolveOnly)) {
+    // row-major by position (the partial factors too when a pivot was zero), coalesced
+#pragma unroll 4
+    for (int p = 0; p < n; ++p)
+      if (live) v.LU[(int64_t)p * n + lane] = R[lop[p] * kLd + lane];
   }
 
   if ((flags & (kWantDet | kWantSlogdet)) && !(flags & kSolveOnly)) {
@@ -150,19 +159,20 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   if (lane == 0 && bt.info && !(flags & kSolveOnly)) bt.info[v.idx] = info;
   if (info) return;
 
-  // ---- substitution: X = U^-1 L^-1 P B, RC right-hand-side columns at a time ----
+  // ---- substitution: X = U^-1 L^-1 P B, up to RC right-hand-side columns at a time ----
   for (int pass = 0; pass < 2; ++pass) {
     const bool is_inv = pass == 1;
     if (!is_inv && !(flags & kWantSolve)) continue;
     if (is_inv && (!(flags & kWantInv) || v.inv == nullptr)) continue;
     const int ncols = is_inv ? n : v.nrhs;
     for (int c0 = 0; c0 < ncols; c0 += RC) {
+      const int nc = min(RC, ncols - c0);  // columns of this chunk (warp-uniform)
       double x[RC];
-#pragma unroll 64
+#pragma unroll
       for (int c = 0; c < RC; ++c) {
         const int col = c0 + c;
         double b = 0.0;
-        if (live && col < ncols) {
+        if (live && c < nc) {
           if (is_inv) b = (orig == col) ? 1.0 : 0.0;
           else b = v.B[(int64_t)orig * ncols + col];
         }
@@ -170,40 +180,43 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
       }
       __syncwarp();  // every lane has read its right-hand side before any lane writes X (getrs in place)
       // forward: unit lower, position order
-#pragma unroll 64
-      for (int k = 0; k < NP; ++k) {
-        if (k >= n) continue;
+#pragma unroll 1
+      for (int k = 0; k < n; ++k) {
         const int l = lop[k];
         const bool below = live && pos > k;
-#pragma unroll 64
+        const double lk = below ? row[k] : 0.0;
+#pragma unroll
         for (int c = 0; c < RC; ++c) {
-          const double xk = __shfl_sync(kFull, x[c], l);
-          if (below) x[c] = fma(-a[k], xk, x[c]);
+          if (c < nc) {
+            const double xk = __shfl_sync(kFull, x[c], l);
+            if (below) x[c] = fma(-lk, xk, x[c]);
+          }
         }
       }
       // back: upper, divide by the diagonal when the row is final
-#pragma unroll 64
-      for (int k = NP - 1; k >= 0; --k) {
-        if (k < n) {
-          const int l = lop[k];
-          if (lane == l) {
-            const double rd = 1.0 / a[k];
-#pragma unroll 64
-            for (int c = 0; c < RC; ++c) x[c] *= rd;
-          }
-          const bool above = live && pos < k;
-#pragma unroll 64
-          for (int c = 0; c < RC; ++c) {
+#pragma unroll 1
+      for (int k = n - 1; k >= 0; --k) {
+        const int l = lop[k];
+        if (lane == l) {
+          const double rd = 1.0 / row[k];
+#pragma unroll
+          for (int c = 0; c < RC; ++c) x[c] *= rd;
+        }
+        const bool above = live && pos < k;
+        const double uk = above ? row[k] : 0.0;
+#pragma unroll
+        for (int c = 0; c < RC; ++c) {
+          if (c < nc) {
             const double xk = __shfl_sync(kFull, x[c], l);
-            if (above) x[c] = fma(-a[k], xk, x[c]);
+            if (above) x[c] = fma(-uk, xk, x[c]);
           }
         }
       }
       if (live) {
         double* out = is_inv ? v.inv : v.X;
-#pragma unroll 64
+#pragma unroll
         for (int c = 0; c < RC; ++c)
-          if (c0 + c < ncols) out[(int64_t)pos * ncols + c0 + c] = x[c];
+          if (c < nc) out[(int64_t)pos * ncols + c0 + c] = x[c];
       }
     }
   }
@@ -221,8 +234,7 @@ cudaError_t launch_np(const Batch& bt, const int32_t* order, int nsys, cudaStrea
 cudaError_t launch_lu_warp(const Batch& bt, const int32_t* order, int nsys, int np,
                            cudaStream_t st) {
   if (nsys <= 0) return cudaSuccess;
-  if (np <= 8) return launch_np<8>(bt, order, nsys, st);
-  if (np <= 16) return launch_np<16>(bt, order, nsys, st);
+  (void)np;  // one kernel for every order <= 32: its loops run over the order at run time
   return launch_np<32>(bt, order, nsys, st);
 }
 
