@@ -145,16 +145,20 @@ int d_linalg(int64_t count, int32_t n, int32_t nrhs, int flags, const double* dA
     p.ipiv = dipiv ? dipiv : pl->d_piv;
     return pl->execute(p, st);
   }
+  // the warp kernel writes factors and pivots only when they are kept: no
+  // workspace otherwise (a small batch is then one launch and nothing else)
   DevMem lu_m, piv_m;
   double* LU = dLU;
   int32_t* piv = dipiv;
-  if (!LU) {
-    NPPB_RC(scratch<double>(lu_m, (size_t)count * nn, st));
-    LU = lu_m.as<double>();
-  }
-  if (!piv) {
-    NPPB_RC(scratch<int32_t>(piv_m, (size_t)count * n, st));
-    piv = piv_m.as<int32_t>();
+  if (flags & NPPB_WANT_LU) {
+    if (!LU) {
+      NPPB_RC(scratch<double>(lu_m, (size_t)count * nn, st));
+      LU = lu_m.as<double>();
+    }
+    if (!piv) {
+      NPPB_RC(scratch<int32_t>(piv_m, (size_t)count * n, st));
+      piv = piv_m.as<int32_t>();
+    }
   }
   Batch bt{};
   bt.A = dA; bt.LU = LU; bt.ipiv = piv; bt.B = dB; bt.X = dX;

@@ -81,8 +81,8 @@ __device__ __forceinline__ SysView sys_view(const Batch& bt, int s) {
     const int64_t n = bt.n, nn = n * n;
     v.n = bt.n; v.nrhs = bt.nrhs; v.idx = s;
     v.A = bt.A + s * nn;
-    v.LU = bt.LU + s * nn;
-    v.ipiv = bt.ipiv + s * n;
+    v.LU = bt.LU ? bt.LU + s * nn : nullptr;
+    v.ipiv = bt.ipiv ? bt.ipiv + s * n : nullptr;
     v.B = bt.B ? bt.B + s * n * bt.nrhs : nullptr;
     v.X = bt.X ? bt.X + s * n * bt.nrhs : nullptr;
     v.inv = bt.inv ? bt.inv + s * nn : nullptr;
