@@ -303,6 +303,20 @@ int nppb_plan_execute(nppb_plan* plan, const double* dA, const double* dB, doubl
 int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,
                        double* dDet, double* dSign, double* dLogabs, int32_t* dinfo, void* stream,
                        int32_t* chains_out, float* ms_out);
+/* The autotuner's on-disk cache: nppb_plan_autotune first looks its key up
+ * (and on a hit builds the cached configuration and runs it once, untimed,
+ * *ms_out = the cached time), otherwise tunes and appends the result. The
+ * file is $NPPB_AUTOTUNE_CACHE (an empty value disables the cache), else
+ * $XDG_CACHE_HOME/numpp_b200/autotune.txt, else ~/.cache/numpp_b200/autotune.txt;
+ * one line per entry, "<key>\t<chains>\t<ms>" (chains negated with
+ * look-ahead), the last line of a key winning. NPPB_AUTOTUNE_REFRESH=1 tunes
+ * afresh. The key names the device (name, compute capability, SM count; "nodev"
+ * without one), the flags and the batch's histogram over order class
+ * (8, 16, 32, 64, ..., 4096) x right-hand-side class (0, 1, 8, 32, 64, more),
+ * each count bucketed to its power of two. No device work in these three. */
+int nppb_autotune_key(int64_t count, const int32_t* n, const int32_t* nrhs, int flags, char* buf, int64_t len);
+int nppb_autotune_cache_get(const char* key, int32_t* chains, float* ms, int32_t* found);
+int nppb_autotune_cache_put(const char* key, int32_t chains, float ms);
 /* Host buffers: copies in, runs, copies out, synchronises. Inputs in pinned
  * memory take the fast DMA path. */
 int nppb_plan_execute_host(nppb_plan* plan, const double* A, const double* B, double* X,

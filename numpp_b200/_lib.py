@@ -62,6 +62,9 @@ SIGNATURES = {
                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_plan_time_classes": (_int, [_vp] * 10 + [_int, C.POINTER(C.c_float)]),
     "nppb_plan_autotune": (_int, [_vp] * 10 + [C.POINTER(_i32), C.POINTER(C.c_float)]),
+    "nppb_autotune_key": (_int, [C.c_int64, _vp, _vp, C.c_int, C.c_char_p, C.c_int64]),
+    "nppb_autotune_cache_get": (_int, [C.c_char_p, C.POINTER(_i32), C.POINTER(C.c_float), C.POINTER(_i32)]),
+    "nppb_autotune_cache_put": (_int, [C.c_char_p, _i32, C.c_float]),
     "nppb_plan_time_kernels": (_int, [_vp] * 10 + [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nppb_solve_grouped": (_int, [_i64, _vp, _vp, _vp, _vp, _vp, _int] + [_vp] * 8),
     "nppb_d_gemm_batched": (_int, [_i64, _i64, _i64, _i64, _vp, _vp, _vp, _vp]),

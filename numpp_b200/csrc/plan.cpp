@@ -23,6 +23,14 @@
 #include <new>
 #include <string>
 #include <tuple>
+#include <cerrno>
+#include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <map>
+#include <sstream>
+
+#include <sys/stat.h>
 
 #include "../../include/numpp_b200.h"
 
@@ -814,6 +822,150 @@ int build_chunks(nppb_plan& P) {
 
 }  // namespace
 
+namespace {
+
+// ---- the autotuner's on-disk cache ----------------------------------------
+// One line per tuned configuration: "<key>\t<chains>\t<ms>", chains negated
+// when look-ahead is on; the last line for a key wins. The key names the
+// device (name, compute capability, SM count), the plan flags and the batch's
+// histogram over (order class, right-hand-side class), counts bucketed by
+// powers of two, so that batches of the same make share an entry.
+std::mutex g_tune_mu;
+
+std::string tune_cache_path() {
+  if (const char* p = std::getenv("NPPB_AUTOTUNE_CACHE")) return p;  // empty: no disk cache
+  const char* xdg = std::getenv("XDG_CACHE_HOME");
+  if (xdg && *xdg) return std::string(xdg) + "/numpp_b200/autotune.txt";
+  const char* home = std::getenv("HOME");
+  if (home && *home) return std::string(home) + "/.cache/numpp_b200/autotune.txt";
+  return "";
+}
+
+bool make_parent_dirs(const std::string& path) {
+  for (size_t i = 1; i < path.size(); ++i) {
+    if (path[i] != '/') continue;
+    const std::string d = path.substr(0, i);
+    if (mkdir(d.c_str(), 0755) != 0 && errno != EEXIST) return false;
+  }
+  return true;
+}
+
+int order_class(int n) {
+  static const int kBounds[] = {8, 16, 32, 64, 128, 256, 512, 1024, 2048, 4096};
+  for (int b : kBounds)
+    if (n <= b) return b;
+  return 1 << 30;
+}
+int rhs_class(int k) { return k <= 0 ? 0 : k == 1 ? 1 : k <= 8 ? 8 : k <= 32 ? 32 : k <= 64 ? 64 : 65; }
+
+std::string device_signature() {
+  int dev = 0;
+  cudaDeviceProp prop{};
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return "nodev";
+  }
+  std::ostringstream o;
+  for (const char* c = prop.name; *c; ++c) o << (*c == ' ' || *c == '\t' ? '_' : *c);
+  o << "/sm" << prop.major << prop.minor << "/x" << prop.multiProcessorCount;
+  return o.str();
+}
+
+std::string tuning_key(int64_t count, const int32_t* n, const int32_t* nrhs, int flags) {
+  std::map<std::pair<int, int>, int64_t> h;
+  for (int64_t i = 0; i < count; ++i) ++h[{order_class(n[i]), rhs_class(nrhs ? nrhs[i] : 0)}];
+  std::ostringstream o;
+  o << device_signature() << "|f" << flags;
+  for (const auto& [cls, c] : h) {
+    int lg = 0;
+    while ((int64_t{2} << lg) <= c) ++lg;
+    o << "|n" << cls.first << "r" << cls.second << "c" << lg;
+  }
+  return o.str();
+}
+
+bool cache_get(const std::string& key, int* chains, float* ms) {
+  const std::string path = tune_cache_path();
+  if (path.empty()) return false;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  std::ifstream f(path);
+  if (!f) return false;
+  bool found = false;
+  std::string line;
+  while (std::getline(f, line)) {
+    const size_t t1 = line.find('\t');
+    if (t1 == std::string::npos || line.compare(0, t1, key) != 0 || t1 != key.size()) continue;
+    int c = 0;
+    float m = 0.f;
+    if (std::sscanf(line.c_str() + t1 + 1, "%d\t%f", &c, &m) == 2 && c != 0) {
+      *chains = c;
+      *ms = m;
+      found = true;
+    }
+  }
+  return found;
+}
+
+bool cache_put(const std::string& key, int chains, float ms) {
+  const std::string path = tune_cache_path();
+  if (path.empty() || key.find_first_of("\t\n") != std::string::npos) return false;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (!make_parent_dirs(path)) return false;
+  std::ofstream f(path, std::ios::app);
+  if (!f) return false;
+  f << key << '\t' << chains << '\t' << std::setprecision(9) << ms << '\n';
+  return static_cast<bool>(f);
+}
+
+}  // namespace
+
+int nppb_autotune_key(int64_t count, const int32_t* n, const int32_t* nrhs, int flags, char* buf, int64_t len) {
+  return guarded([&]() -> int {
+    if (count < 0 || (count && !n) || !buf || len <= 0) {
+      nppb::set_error("autotune key: bad arguments");
+      return NPPB_E_ARG;
+    }
+    const std::string k = tuning_key(count, n, nrhs, flags);
+    if ((int64_t)k.size() >= len) {
+      nppb::set_error("autotune key: buffer too small");
+      return NPPB_E_RANGE;
+    }
+    std::memcpy(buf, k.c_str(), k.size() + 1);
+    return NPPB_OK;
+  });
+}
+
+int nppb_autotune_cache_get(const char* key, int32_t* chains, float* ms, int32_t* found) {
+  return guarded([&]() -> int {
+    if (!key || !chains || !ms || !found) {
+      nppb::set_error("autotune cache: bad arguments");
+      return NPPB_E_ARG;
+    }
+    int c = 0;
+    float m = 0.f;
+    *found = cache_get(key, &c, &m) ? 1 : 0;
+    if (*found) {
+      *chains = c;
+      *ms = m;
+    }
+    return NPPB_OK;
+  });
+}
+
+int nppb_autotune_cache_put(const char* key, int32_t chains, float ms) {
+  return guarded([&]() -> int {
+    if (!key || chains == 0) {
+      nppb::set_error("autotune cache: bad arguments");
+      return NPPB_E_ARG;
+    }
+    if (!cache_put(key, chains, ms)) {
+      nppb::set_error("autotune cache: not written (no cache path, or the file cannot be written)");
+      return NPPB_E_ARG;
+    }
+    return NPPB_OK;
+  });
+}
+
 int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, double* dX, double* dInv,
                        double* dDet, double* dSign, double* dLogabs, int32_t* dinfo, void* stream,
                        int32_t* chains_out, float* ms_out) {
@@ -840,6 +992,28 @@ int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, doub
     std::unique_ptr<Plan> best;
     float best_ms = 0.f;
     int rc = NPPB_OK;
+    const std::string key = tuning_key(count, plan->n.data(), plan->nrhs.data(), plan->flags);
+    int cached_chains = 0;
+    float cached_ms = 0.f;
+    const char* refresh = std::getenv("NPPB_AUTOTUNE_REFRESH");
+    const bool hit = !(refresh && *refresh && *refresh != '0') && cache_get(key, &cached_chains, &cached_ms);
+    if (hit) {  // the cached configuration, built and run once (the outputs as documented), untimed
+      auto cand = std::make_unique<Plan>();
+      cand->nchains = cached_chains < 0 ? -cached_chains : cached_chains;
+      cand->lookahead_mode = cached_chains < 0 ? 1 : 0;
+      rc = cand->build(count, plan->n.data(), plan->nrhs.data(), plan->a_off.data(), plan->b_off.data(),
+                       plan->inv_off.data(), plan->flags, false, true);
+      if (rc == NPPB_OK) rc = cand->execute(dev_ptrs(*cand, dA, dB, dX, dInv, dDet, dSign, dLogabs, dinfo), st);
+      if (rc == NPPB_OK) {
+        cudaStreamSynchronize(st);
+        plan->pp = std::move(cand);
+        if (chains_out) *chains_out = plan->pp->nchains * (plan->pp->lookahead ? -1 : 1);
+        if (ms_out) *ms_out = cached_ms;
+        return NPPB_OK;
+      }
+      cudaStreamSynchronize(st);
+      rc = NPPB_OK;  // tune afresh
+    }
     static const int kChainCounts[5] = {1, 2, 3, 4, 6};
     for (int cfg = 0; cfg < 10; ++cfg) {
       const int c = kChainCounts[cfg / 2], la = cfg % 2;
@@ -874,6 +1048,7 @@ int nppb_plan_autotune(nppb_plan* plan, const double* dA, const double* dB, doub
     if (rc != NPPB_OK) return rc;
     if (chains_out) *chains_out = plan->pp->nchains * (plan->pp->lookahead ? -1 : 1);
     if (ms_out) *ms_out = best_ms;
+    if (best_ms > 0.f) cache_put(key, plan->pp->nchains * (plan->pp->lookahead ? -1 : 1), best_ms);
     return NPPB_OK;
   });
 }

@@ -86,9 +86,11 @@ def test_plan_device_buffers_torch(lib, oracle):
     plan.close()
 
 
-def test_plan_autotune_keeps_a_working_plan(lib, oracle):
+def test_plan_autotune_keeps_a_working_plan(lib, oracle, tmp_path, monkeypatch):
     """The autotuner times chain counts on the caller's buffers and keeps the
-    fastest; the plan it keeps gives the reference's results."""
+    fastest; the plan it keeps gives the reference's results. A second plan of
+    the same batch takes the choice from the on-disk cache without timing."""
+    monkeypatch.setenv("NPPB_AUTOTUNE_CACHE", str(tmp_path / "autotune.txt"))
     torch = pytest.importorskip("torch")
     sys = workloads.uneven_batch(seed=14, count=300, n_lo=2, n_hi=300)
     plan = Plan(sys, FLAGS)
@@ -108,6 +110,17 @@ def test_plan_autotune_keeps_a_working_plan(lib, oracle):
     check_vs_oracle(sys, dX.cpu().numpy(), dInv.cpu().numpy(), d[0].cpu().numpy(), d[1].cpu().numpy(),
                     d[2].cpu().numpy(), dinfo.cpu().numpy(), oracle)
     plan.close()
+    lines = (tmp_path / "autotune.txt").read_text().splitlines()
+    assert len(lines) == 1
+    plan2 = Plan(sys, FLAGS)
+    dX.zero_()
+    c2, la2, ms2 = plan2.autotune(dA, dB, dX, dInv, d[0], d[1], d[2], dinfo)
+    assert (c2, la2) == (chains, lookahead) and ms2 == pytest.approx(ms, rel=1e-5)
+    assert len((tmp_path / "autotune.txt").read_text().splitlines()) == 1  # a hit appends nothing
+    torch.cuda.synchronize()
+    check_vs_oracle(sys, dX.cpu().numpy(), dInv.cpu().numpy(), d[0].cpu().numpy(), d[1].cpu().numpy(),
+                    d[2].cpu().numpy(), dinfo.cpu().numpy(), oracle)
+    plan2.close()
 
 
 def test_full_uneven_batch_properties(lib):
