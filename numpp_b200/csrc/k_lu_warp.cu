@@ -32,13 +32,13 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarpsPerCta = 2;  // small batches spread over more SMs
-constexpr int kLd = 33;          // row stride of a warp's tile (doubles): conflict-free columns
+constexpr int kLd = 34;          // row stride of a warp's tile (doubles): columns 32, 33 are scratch
 
 template <int NP, int RC>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   __shared__ int s_lane_of_pos[kWarpsPerCta][32];
-  __shared__ double s_rows[kWarpsPerCta][32 * kLd];
+  __shared__ double s_rows[kWarpsPerCta][32 * kLd];  // row r at r * kLd
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = blockIdx.x * kWarpsPerCta + wib;
@@ -52,11 +52,14 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   double* row = R + lane * kLd;  // this lane's row
 
   {
-    // coalesced: lane c reads column c of each row in turn
+    // coalesced: lane c reads column c of every row, all loads in flight before the stores
     const double* src = (flags & kSolveOnly) ? v.LU : v.A;
-#pragma unroll 4
-    for (int r = 0; r < n; ++r)
-      if (live) R[r * kLd + lane] = src[(int64_t)r * n + lane];
+    double t[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) t[r] = (live && r < n) ? src[(int64_t)r * n + lane] : 0.0;
+#pragma unroll
+    for (int r = 0; r < 32; ++r)
+      if (r < n) R[r * kLd + lane] = t[r];
   }
   __syncwarp();
 
@@ -134,18 +137,24 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   }
 
   if ((flags & (kWantDet | kWantSlogdet)) && !(flags & kSolveOnly)) {
-    const double lg = log(fabs(dg));
+    // the pivots and their logs by position (the tile's padding column), folded in
+    // position order by lane 0: the reference's sequence of products and sums
+    double* dgs = R + 32;  // column 32 of the tile: rows 0..n-1 hold the pivot of position r
+    if (live) {
+      dgs[pos * kLd] = dg;
+      dgs[pos * kLd + 1] = log(fabs(dg));  // column 33
+    }
+    __syncwarp();
     double det = (nswap & 1) ? -1.0 : 1.0;
     double sgn = det;
     double logabs = 0.0;
-    if (info == 0) {
+    if (info == 0 && lane == 0) {
       for (int i = 0; i < n; ++i) {
-        const int l = lop[i];
-        const double di = __shfl_sync(kFull, dg, l);
-        const double li = __shfl_sync(kFull, lg, l);
+        const double di = dgs[i * kLd], li = dgs[i * kLd + 1];
         det *= di;
         logabs += li;
-        sgn *= di / fabs(di);
+        // d / |d| is exactly +-1 for finite nonzero d, NaN otherwise
+        sgn = isfinite(di) ? (di < 0.0 ? -sgn : sgn) : NAN;
       }
     }
     if (lane == 0) {
@@ -160,6 +169,7 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   if (info) return;
 
   // ---- substitution: X = U^-1 L^-1 P B, up to RC right-hand-side columns at a time ----
+  const double rdg = live ? 1.0 / row[pos] : 0.0;  // this row's diagonal of U, inverted once
   for (int pass = 0; pass < 2; ++pass) {
     const bool is_inv = pass == 1;
     if (!is_inv && !(flags & kWantSolve)) continue;
@@ -193,14 +203,13 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
           }
         }
       }
-      // back: upper, divide by the diagonal when the row is final
+      // back: upper, multiply by the diagonal's reciprocal when the row is final
 #pragma unroll 1
       for (int k = n - 1; k >= 0; --k) {
         const int l = lop[k];
         if (lane == l) {
-          const double rd = 1.0 / row[k];
 #pragma unroll
-          for (int c = 0; c < RC; ++c) x[c] *= rd;
+          for (int c = 0; c < RC; ++c) x[c] *= rdg;
         }
         const bool above = live && pos < k;
         const double uk = above ? row[k] : 0.0;
