@@ -38,7 +38,7 @@ template <int NP, int RC>
 __global__ void __launch_bounds__(kWarpsPerCta * 32)
 k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
   __shared__ int s_lane_of_pos[kWarpsPerCta][32];
-  __shared__ double s_rows[kWarpsPerCta][32 * kLd];  // row r at r * kLd
+  __shared__ __align__(16) double s_rows[kWarpsPerCta][32 * kLd];  // row r at r * kLd (16-byte aligned rows)
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int w = blockIdx.x * kWarpsPerCta + wib;
@@ -102,8 +102,18 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
       if (live && pos > k) {
         const double f = row[k] / pk;
         row[k] = f;
+        // 16-byte pieces (rows start 16-byte aligned); the piece holding column k
+        // keeps it, columns past n are padding
+        double2* r2 = reinterpret_cast<double2*>(row);
+        const double2* p2 = reinterpret_cast<const double2*>(prow);
 #pragma unroll 4
-        for (int j = k + 1; j < n; ++j) row[j] = fma(-f, prow[j], row[j]);
+        for (int q = (k + 1) >> 1; q < (n + 1) >> 1; ++q) {
+          const double2 pv = p2[q];
+          double2 rv = r2[q];
+          if (2 * q > k) rv.x = fma(-f, pv.x, rv.x);
+          rv.y = fma(-f, pv.y, rv.y);
+          r2[q] = rv;
+        }
       }
       __syncwarp();
     }
@@ -234,7 +244,11 @@ k_lu_warp(Batch bt, const int32_t* __restrict__ order, int nsys) {
 template <int NP>
 cudaError_t launch_np(const Batch& bt, const int32_t* order, int nsys, cudaStream_t st) {
   const int grid = (nsys + kWarpsPerCta - 1) / kWarpsPerCta;
-  k_lu_warp<NP, 8><<<grid, kWarpsPerCta * 32, 0, st>>>(bt, order, nsys);
+  // one right-hand-side column and no inverse (a uniform batch says so): the one-column substitution
+  if (!bt.desc && bt.nrhs <= 1 && !(bt.flags & kWantInv))
+    k_lu_warp<NP, 1><<<grid, kWarpsPerCta * 32, 0, st>>>(bt, order, nsys);
+  else
+    k_lu_warp<NP, 8><<<grid, kWarpsPerCta * 32, 0, st>>>(bt, order, nsys);
   return cudaGetLastError();
 }
 
