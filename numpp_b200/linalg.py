@@ -496,3 +496,49 @@ def lstsq(a, b, rcond=-1.0, backend=None):
     x = X[0, :, 0] if bvec else X[0]
     resid = res[0] if has[0] else np.zeros(0)
     return x.astype(out, copy=False), resid, int(rank[0]), S[0]
+
+
+def _main(argv=None):
+    """Time the small uniform batch on the device: 256 systems of order 32,
+    A = N(0,1) + 32 I from PCG64 (seed 2025), one right-hand side, solve + det
+    in one call of nppb_d_linalg_batched (CUDA events over back-to-back calls)."""
+    import argparse
+
+    import torch
+
+    from . import workloads
+    p = argparse.ArgumentParser(prog="python -m numpp_b200.linalg")
+    p.add_argument("--small", action="store_true", help="the 256 x 32 x 32 solve + det batch")
+    p.add_argument("--reps", type=int, default=200)
+    a = p.parse_args(argv)
+    if not a.small:
+        p.error("nothing to time: pass --small")
+    L = _lib.load()
+    P = _lib.ptr
+    dev = torch.device("cuda:0")
+    A, B = workloads.uniform_batch(seed=2025)
+    dA, dB = torch.from_numpy(A).to(dev), torch.from_numpy(B).to(dev)
+    dX = torch.zeros_like(dB)
+    det = torch.zeros(256, dtype=torch.float64, device=dev)
+    info = torch.zeros(256, dtype=torch.int32, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+
+    def run():
+        _check(L.nppb_d_linalg_batched(256, 32, 1, _lib.WANT_SOLVE | _lib.WANT_DET, P(dA), P(dB), P(dX), None,
+                                       P(det), None, None, None, None, P(info), st))
+
+    for _ in range(10):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.reps):
+        run()
+    e1.record()
+    e1.synchronize()
+    print("256 x 32 x 32 solve + det: %.2f us per call (%d back-to-back calls)" % (e0.elapsed_time(e1) / a.reps * 1e3,
+                                                                                  a.reps), flush=True)
+
+
+if __name__ == "__main__":
+    _main()
