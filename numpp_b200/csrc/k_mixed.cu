@@ -58,13 +58,7 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* bits, doub
 }
 
 // Row pass, one CTA per (system, kMixedRows rows): row scales, ||A||_inf, and
-// the column maxima of diag(r) |A| over this CTA's rows. The rows go in groups
-// of eight: a warp takes a row (its maximum and sum), then after a barrier
-// every thread takes its columns of the group's rows again while they are
-// still in cache, keeping its columns' maxima in registers; they go to the
-// system's maxima once at the end.
-constexpr int kEqGroup = MT / 32;                 // rows per group: one per warp
-constexpr int kEqCols = kMixedMaxN / MT;          // columns per thread
+// the column maxima of diag(r) |A| over this CTA's rows.
 __global__ void __launch_bounds__(MT)
 k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict__ rs,
              double* __restrict__ cmax, RefineState* __restrict__ st) {
@@ -75,51 +69,31 @@ k_equil_rows(const double* __restrict__ A, int n, int equil, double* __restrict_
   const int rows = min(kMixedRows, n - r0);
   const double* a = A + (int64_t)s * n * n + (int64_t)r0 * n;
   double arow = 0.0;
-  double cm[kEqCols];
-#pragma unroll
-  for (int t = 0; t < kEqCols; ++t) cm[t] = 0.0;
-  for (int g0 = 0; g0 < rows; g0 += kEqGroup) {
-    const int i = g0 + warp;
-    if (i < rows) {
-      const double* ai = a + (int64_t)i * n;
-      double m = 0.0, sum = 0.0;
+  for (int i = warp; i < rows; i += MT / 32) {
+    double m = 0.0, sum = 0.0;
 #pragma unroll 8
-      for (int j = lane; j < n; j += 32) {
-        const double v = fabs(ai[j]);
-        m = fmax(m, v);
-        sum += v;
-      }
-      m = warp_max(m);
-      sum = warp_sum(sum);
-      const double r = equil ? pow2_scale(m) : 1.0;
-      if (lane == 0) {
-        rsc[i] = r;
-        rs[(int64_t)s * n + r0 + i] = r;
-      }
-      arow = fmax(arow, sum);
+    for (int j = lane; j < n; j += 32) {
+      const double v = fabs(a[(int64_t)i * n + j]);
+      m = fmax(m, v);
+      sum += v;
     }
-    if (!equil) continue;
-    __syncthreads();  // the group's row scales
-    const int gr = min(kEqGroup, rows - g0);
-#pragma unroll
-    for (int t = 0; t < kEqCols; ++t) {
-      const int j = tid + MT * t;
-      if (j < n) {
-        double m = cm[t];
-#pragma unroll
-        for (int q = 0; q < kEqGroup; ++q)
-          if (q < gr) m = fmax(m, rsc[g0 + q] * fabs(a[(int64_t)(g0 + q) * n + j]));
-        cm[t] = m;
-      }
+    m = warp_max(m);
+    sum = warp_sum(sum);
+    const double r = equil ? pow2_scale(m) : 1.0;
+    if (lane == 0) {
+      rsc[i] = r;
+      rs[(int64_t)s * n + r0 + i] = r;
     }
+    arow = fmax(arow, sum);
   }
-  const double anorm = block_max(arow, red);
+  const double anorm = block_max(arow, red);  // includes the barrier publishing rsc
   if (tid == 0) atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&st[s].anorm), anorm);
   if (!equil) return;
-#pragma unroll
-  for (int t = 0; t < kEqCols; ++t) {
-    const int j = tid + MT * t;
-    if (j < n) atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), cm[t]);
+  for (int j = tid; j < n; j += MT) {
+    double m = 0.0;
+#pragma unroll 8
+    for (int i = 0; i < rows; ++i) m = fmax(m, rsc[i] * fabs(a[(int64_t)i * n + j]));
+    atomic_max_nonneg(reinterpret_cast<unsigned long long*>(&cmax[(int64_t)s * n + j]), m);
   }
 }
 
