@@ -195,7 +195,7 @@ struct DiagAux {
   float lcol[32][32];    // the panel's L11 columns below the diagonal (shifted to index 0)
   int fail;  // 1 + first position whose pivot failed, INT_MAX if none
 };
-constexpr size_t kDiagSmem = sizeof(float) * ((kMxWin + kMxNB) * DLD) + sizeof(DiagAux);
+constexpr size_t kDiagSmem = sizeof(float) * (kMxWin * DLD) + sizeof(DiagAux);
 
 // Inverse of one 32 x 32 diagonal block of the packed factors at (o, o), one
 // warp, lane = column: unit lower (L) by substitution down, upper (U) up.
@@ -368,12 +368,10 @@ __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t
 }
 
 __global__ void __launch_bounds__(DT, 1)
-k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv, float* __restrict__ UinvT,
-          int32_t* __restrict__ perm, int32_t* __restrict__ info, int N, int k) {
+k_mx_diag(float* __restrict__ M, int32_t* __restrict__ perm, int32_t* __restrict__ info, int N, int k) {
   extern __shared__ __align__(16) float dsm[];
-  float* W0 = dsm;                    // [256][DLD] the window by physical row; later L^-1 and the factors
-  float* Ui = W0 + kMxWin * DLD;      // [128][DLD] U^-1 (first the factors in position order)
-  DiagAux& ax = *reinterpret_cast<DiagAux*>(Ui + kMxNB * DLD);
+  float* W0 = dsm;                    // [256][DLD] the window by physical row
+  DiagAux& ax = *reinterpret_cast<DiagAux*>(W0 + kMxWin * DLD);
   const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int R = min(kMxWin, N - K);  // window rows: this block's and the next block's
   constexpr unsigned FULL = 0xffffffffu;
@@ -473,21 +471,39 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   // (their panel values are now their multipliers, L21 = A21 U11^-1)
   int32_t* pw = perm + ((int64_t)s * (N / kMxNB) + k) * kMxWin;
   if (tid < R) pw[tid] = tid < kMxNB ? ax.phys_of[tid] : ax.act[tid - kMxNB];
+#pragma unroll 4
   for (int idx = tid; idx < R * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
     const int ph = r < kMxNB ? ax.phys_of[r] : ax.act[r - kMxNB];
-    const float4 v = *reinterpret_cast<const float4*>(W0 + ph * DLD + c);
-    *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = v;
-    if (r < kMxNB) *reinterpret_cast<float4*>(Ui + r * DLD + c) = v;  // the factors, position order
+    *reinterpret_cast<float4*>(Mb + (int64_t)r * N + c) = *reinterpret_cast<const float4*>(W0 + ph * DLD + c);
   }
-  __syncthreads();
-  float* LU = W0 + kMxNB * DLD;
-  float* Li = W0;
+  if (tid == 0 && ax.fail != INT_MAX && info[s] == 0) info[s] = K + ax.fail;
+}
+
+// The diagonal block's inverses from its packed factors (written by k_mx_diag
+// into M, position order): L^-1, U^-1 and U^-T. A kernel of its own so that it
+// runs beside the window permute (which does not need them). The eight 32 x 32
+// diagonal blocks of L and U inverted by one warp each (lane = column,
+// substitution down / up the block), then two levels of block products,
+// [L00 0; L10 L11]^-1 = [L00^-1 0; -L11^-1 L10 L00^-1 L11^-1] and
+// [U00 U01; 0 U11]^-1 = [U00^-1 -U00^-1 U01 U11^-1; 0 U11^-1], as 32^3 and
+// 64^3 shared-memory GEMMs (temporaries in the quadrants the results leave
+// zero, and at the last level in the factors' diagonal quadrants).
+constexpr size_t kInvSmem = sizeof(float) * 3 * kMxNB * DLD;
+__global__ void __launch_bounds__(DT, 1)
+k_mx_diag_inv(const float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ Uinv,
+              float* __restrict__ UinvT, int N, int k) {
+  extern __shared__ __align__(16) float ism[];
+  float* LU = ism;                  // [128][DLD] the packed factors (position order)
+  float* Li = LU + kMxNB * DLD;     // [128][DLD] L^-1
+  float* Ui = Li + kMxNB * DLD;     // [128][DLD] U^-1
+  const int s = blockIdx.x, K = k * kMxNB, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const float* Mb = M + (int64_t)s * N * N + (int64_t)K * N + K;
+#pragma unroll 4
   for (int idx = tid; idx < kMxNB * 32; idx += DT) {
     const int r = idx >> 5, c = (idx & 31) * 4;
-    *reinterpret_cast<float4*>(LU + r * DLD + c) = *reinterpret_cast<const float4*>(Ui + r * DLD + c);
+    *reinterpret_cast<float4*>(LU + r * DLD + c) = *reinterpret_cast<const float4*>(Mb + (int64_t)r * N + c);
   }
-  __syncthreads();
   for (int idx = tid; idx < kMxNB * DLD; idx += DT) {
     Li[idx] = 0.f;
     Ui[idx] = 0.f;
@@ -533,11 +549,10 @@ k_mx_diag(float* __restrict__ M, float* __restrict__ Linv, float* __restrict__ U
   float* UTb = UinvT + (int64_t)s * N * kMxNB + (int64_t)K * kMxNB;
   for (int idx = tid; idx < kMxNB * kMxNB; idx += DT) {
     const int r = idx >> 7, c = idx & 127;
-    Lb[idx] = c <= r ? Li[r * DLD + c] : 0.f;        // L^-1[r][c] (rows already in position order)
+    Lb[idx] = c <= r ? Li[r * DLD + c] : 0.f;        // L^-1[r][c]
     Ub[idx] = c >= r ? Ui[r * DLD + c] : 0.f;        // U^-1[r][c]
     UTb[idx] = r >= c ? Ui[c * DLD + r] : 0.f;       // U^-T[r][c]
   }
-  if (tid == 0 && ax.fail != INT_MAX && info[s] == 0) info[s] = K + ax.fail;
 }
 
 // ---------------------------------------------------------------------------
@@ -1281,6 +1296,8 @@ cudaError_t mx_prepare() {
     e = cudaFuncSetAttribute(k_mx_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDiagSmem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPermSmem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_mx_diag_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem);
   const int csm = (int)(sizeof(float) * ((size_t)4096 * 8 + 3 * kMxNB * 8));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<1, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
@@ -1325,7 +1342,8 @@ namespace {
 struct MxStreams {
   cudaStream_t panel = nullptr;  // the next block's diagonal factor and triangular solves, highest priority
   cudaStream_t side = nullptr;   // the bulk of the trailing update
-  cudaEvent_t ev[4] = {};
+  cudaStream_t inv = nullptr;    // the diagonal block's inverses, beside the window permute
+  cudaEvent_t ev[6] = {};
 };
 
 MxStreams* mx_streams() {
@@ -1333,7 +1351,7 @@ MxStreams* mx_streams() {
     std::vector<MxStreams> per_dev;
     ~Holder() {
       for (auto& m : per_dev) {
-        for (cudaStream_t t : {m.panel, m.side})
+        for (cudaStream_t t : {m.panel, m.side, m.inv})
           if (t) cudaStreamDestroy(t);
         for (cudaEvent_t e : m.ev)
           if (e) cudaEventDestroy(e);
@@ -1349,6 +1367,7 @@ MxStreams* mx_streams() {
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
     bool ok = cudaStreamCreateWithPriority(&m.panel, cudaStreamNonBlocking, greatest) == cudaSuccess &&
+              cudaStreamCreateWithPriority(&m.inv, cudaStreamNonBlocking, greatest) == cudaSuccess &&
               cudaStreamCreateWithFlags(&m.side, cudaStreamNonBlocking) == cudaSuccess;
     for (cudaEvent_t& e : m.ev) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
@@ -1389,11 +1408,23 @@ cudaError_t mx_factor(const MxBufs& b, cudaStream_t s) {
   for (int k = 0; k < nb; ++k) {
     const int K = k * kMxNB, tiles = nb - k - 1;
     // block k's window was last written by block k-1's cross update, earlier on ps
-    k_mx_diag<<<count, DT, kDiagSmem, ps>>>(b.M, b.Linv, b.Uinv, b.UinvT, b.perm, b.info, N, k);
+    k_mx_diag<<<count, DT, kDiagSmem, ps>>>(b.M, b.perm, b.info, N, k);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // the inverses beside the permute (they read the diagonal tile, which the permute leaves alone)
+    cudaStream_t is = ms ? ms->inv : ps;
+    if (ms) {
+      if ((e = cudaEventRecord(ms->ev[4], ps)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(is, ms->ev[4], 0)) != cudaSuccess) return e;
+    }
+    k_mx_diag_inv<<<count, DT, kInvSmem, is>>>(b.M, b.Linv, b.Uinv, b.UinvT, N, k);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_mx_permute<<<dim3((unsigned)(N / PC), (unsigned)count), 256, kPermSmem, ps>>>(b.M, b.T, b.perm, N, k, count,
                                                                                    buf);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (ms) {
+      if ((e = cudaEventRecord(ms->ev[5], is)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(ps, ms->ev[5], 0)) != cudaSuccess) return e;
+    }
     if (tiles == 0) break;
     // one launch for the two triangular solves (independent of each other):
     // L21 = A21 U11^-1 below the window (the window's rows got theirs from the
