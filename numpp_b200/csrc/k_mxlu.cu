@@ -979,7 +979,6 @@ k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const flo
 // double-buffered: a CTA reaches step k's barrier only after finishing step
 // k-1's updates, so step k+1's owner may overwrite step k-1's buffer after it.
 constexpr int TS = 512;  // threads per CTA: 16 warps
-bool g_trsv16 = false;   // 16-CTA clusters allowed for the substitutions (set by mx_prepare)
 constexpr size_t kTrsv64Smem = 160 * 1024;  // shared-memory cap of the FP64-vector substitution
 
 // tmp[i][w] = sum_m D[i][m] y[m][w] for the block's 128 rows, 16 warps
@@ -1304,17 +1303,6 @@ cudaError_t mx_prepare() {
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<2, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<4, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv_c<8, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, csm);
-  // 16-CTA clusters for the substitutions of small batches, where the device allows them
-  if (e == cudaSuccess) {
-    bool ok16 = true;
-    for (const void* f : {(const void*)k_mx_trsv_c<1, float>, (const void*)k_mx_trsv_c<2, float>,
-                          (const void*)k_mx_trsv_c<4, float>, (const void*)k_mx_trsv_c<8, float>,
-                          (const void*)k_mx_trsv_c<1, double>, (const void*)k_mx_trsv_c<2, double>,
-                          (const void*)k_mx_trsv_c<4, double>})
-      ok16 = ok16 && cudaFuncSetAttribute(f, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess;
-    if (!ok16) cudaGetLastError();
-    g_trsv16 = ok16;
-  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_trsv_c<1, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
   if (e == cudaSuccess)
@@ -1514,17 +1502,15 @@ cudaError_t mx_rhs_in(const float* R, float* Y, int nrhs, const RefineState* st,
 }
 
 // Cluster size of the triangular solves: enough CTAs per system to cover the
-// GPU's SMs when the batch is small (the launch within one wave), at most 16
-// (8 is the portable cluster size; 16 is opted into for the substitution
-// kernels by mx_prepare) and no more than the blocks.
+// GPU's SMs when the batch is small, at most 8 (the portable cluster size) and
+// no more than the blocks.
 int trsv_cluster(int count, int chunks, int nb) {
   int sms = 148;
   int dev = 0;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaGetLastError();
-  const int cmax = g_trsv16 ? 16 : 8;
   int c = 1;
-  while (c < cmax && 2 * c <= nb && (int64_t)count * chunks * 2 * c <= sms) c *= 2;
+  while (c < 8 && 2 * c <= nb && (int64_t)count * chunks * 2 * c <= sms) c *= 2;
   return c;
 }
 
