@@ -297,6 +297,50 @@ def small_uniform(torch, dev, L, _lib, workloads):
             "e2e_path": "nppb_solve_det_batched (host buffers, pageable)"}
 
 
+def gemm_reference_gpu_baseline(torch, dev, L, _lib):
+    """Row a10 head-to-head on this B200: the reference's own GPU GEMM (NumPP's
+    src/backend/cuda_backend.cu, compiled unmodified for sm_100a: its GpuVTable
+    gemm slot, host buffers, 16 x 16 SIMT tiles) against nppb_gemm (host
+    buffers, FP64 DMMA) on the same FP64 operands, both through their
+    host-buffer calls (copies included); and nppb_d_gemm on device-resident
+    operands (CUDA events). A baseline, like cpu_baseline."""
+    from oracle.oracle import load_refcuda
+    R = load_refcuda()
+    if R is None or R.ref_cuda_available() != 1:
+        return {"unavailable": "oracle/_ref/refcuda (the reference's CUDA backend) not built or no device"}
+    P = _lib.ptr
+    out = []
+    for n in (1024, 4096):
+        rng = np.random.default_rng(n)
+        A = rng.standard_normal((n, n))
+        B = rng.standard_normal((n, n))
+        C = np.zeros((n, n))
+        flops = 2.0 * n ** 3
+
+        def host_ms(fn, reps):
+            fn()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                fn()
+            return (time.perf_counter() - t0) / reps * 1e3
+
+        reps = 5 if n <= 1024 else 2
+        t_ref = host_ms(lambda: R.ref_cuda_gemm(0, n, n, n, A.ctypes.data, B.ctypes.data, C.ctypes.data), reps)
+        t_ours = host_ms(lambda: L.nppb_gemm(_lib.DT_FLOAT64, n, n, n, A.ctypes.data, B.ctypes.data,
+                                             C.ctypes.data), reps)
+        dA, dB = torch.from_numpy(A).to(dev), torch.from_numpy(B).to(dev)
+        dC = torch.zeros_like(dA)
+        st = torch.cuda.current_stream().cuda_stream
+        t_dev = _event_ms(torch, lambda: L.nppb_d_gemm(_lib.DT_FLOAT64, n, n, n, P(dA), P(dB), P(dC), st))
+        out.append({"m_n_k": n, "reference_host_ms": t_ref, "reference_tflops": flops / t_ref * 1e-9,
+                    "nppb_host_ms": t_ours, "nppb_host_tflops": flops / t_ours * 1e-9,
+                    "nppb_device_ms": t_dev, "nppb_device_tflops": flops / t_dev * 1e-9,
+                    "host_speedup": t_ref / t_ours})
+        del dA, dB, dC
+    return {"workload": "C = A B, FP64 row-major, A and B N(0,1)", "rows": out,
+            "reference": "NumPP src/backend/cuda_backend.cu gemm_impl / k_gemm_tiled, compiled for sm_100a"}
+
+
 def serving_run(torch, dev, sustained_seconds, rates=((500, 5.0), (2000, None), (5000, 5.0))):
     """C5: Poisson arrivals at each rate against the serving loop (the rate
     with window None runs for `sustained_seconds`, the others for their
@@ -634,6 +678,7 @@ def run_b200(args):
         torch.cuda.empty_cache()
         # a side measurement that fails is reported, not fatal to the headline line
         for key, fn in (("small_batch", lambda: small_uniform(torch, dev, L, _lib, workloads)),
+                        ("gemm_reference_gpu_baseline", lambda: gemm_reference_gpu_baseline(torch, dev, L, _lib)),
                         ("mixed_vs_fp64", lambda: mixed_vs_fp64(torch, dev, L, _lib)),
                         ("serving", lambda: serving_run(torch, dev, args.serve_seconds))):
             try:

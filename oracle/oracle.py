@@ -13,6 +13,19 @@ _REF_SO = os.path.join(_HERE, "_ref", "libnumpp_ref.so")
 # NumPP's portable sources with the B200 front end and GPU vtable compiled in
 # (the drop-in; oracle/Makefile target `dropin`)
 DROPIN_SO = os.path.join(_HERE, "_ref", "dropin", "libnumpp_dropin.so")
+# the reference's own CUDA backend (its GpuVTable gemm), for the a10 head-to-head
+REFCUDA_SO = os.path.join(_HERE, "_ref", "refcuda", "libnumpp_refcuda.so")
+
+
+def load_refcuda():
+    """The reference's CUDA backend behind its C shim, or None when not built."""
+    if not os.path.exists(REFCUDA_SO):
+        return None
+    L = C.CDLL(REFCUDA_SO)
+    L.ref_cuda_available.restype = C.c_int
+    L.ref_cuda_gemm.restype = C.c_int
+    L.ref_cuda_gemm.argtypes = [C.c_int, C.c_int64, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+    return L
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -34,7 +47,7 @@ def build_oracle(ref_src: str | None = None) -> None:
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
     src = ref_src or os.environ.get("NUMPP_REF_SRC")
     if src and os.path.isdir(src):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref", "dropin", f"REF={src}"], check=True)
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "dropin", "refcuda", f"REF={src}"], check=True)
 
 
 class Oracle:
