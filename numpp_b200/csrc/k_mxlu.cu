@@ -24,8 +24,7 @@
 //                  stored diagonal-block inverses: a cluster of 1..8 CTAs per
 //                  system and right-hand-side chunk, each holding its blocks'
 //                  right-hand sides in shared memory, block solutions passed
-//                  through distributed shared memory (k_mx_trsv: the
-//                  single-CTA form).
+//                  through distributed shared memory.
 //  k_mx_rhs_in / k_mx_apply   U^T applied to a right-hand side, V and the
 //                  column scales applied to a solution (FP64 accumulation).
 // Every wait on an mbarrier is bounded (about a second of SM clock): past it the
@@ -844,130 +843,7 @@ k_mx_gemm(const __grid_constant__ CUtensorMap mA1, const __grid_constant__ CUten
 }
 
 // ---------------------------------------------------------------------------
-// Triangular solves with the block factors: one CTA per (system, chunk of W
-// right-hand sides); the chunk sits in shared memory (N x W floats).
-
-constexpr int ST = 1024;  // threads: 32 warps
-
-// tmp[i][w] = sum_m D[i][m] y[m][w], i < 128 (D row-major 128 x 128)
-template <int W>
-__device__ __forceinline__ void block_apply(const float* __restrict__ D, const float* ys, float* tmp, int warp,
-                                            int lane) {
-  float yv[4][W];
-#pragma unroll
-  for (int e = 0; e < 4; ++e)
-#pragma unroll
-    for (int w = 0; w < W; ++w) yv[e][w] = ys[(4 * lane + e) * W + w];
-#pragma unroll
-  for (int rr = 0; rr < 4; ++rr) {
-    const int i = warp + 32 * rr;
-    const float4 d = *reinterpret_cast<const float4*>(D + i * kMxNB + 4 * lane);
-    float sum[W];
-#pragma unroll
-    for (int w = 0; w < W; ++w) sum[w] = d.x * yv[0][w] + d.y * yv[1][w] + d.z * yv[2][w] + d.w * yv[3][w];
-#pragma unroll
-    for (int o = 16; o; o >>= 1)
-#pragma unroll
-      for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
-    if (lane == 0)
-#pragma unroll
-      for (int w = 0; w < W; ++w) tmp[i * W + w] = sum[w];
-  }
-}
-
-// ys[i] -= M[i][K:K+128] . ys[K:K+128] for rows r0 <= i < r1 (warp per row, RU rows in flight)
-template <int W>
-__device__ __forceinline__ void panel_apply(const float* __restrict__ Ms, int N, int K, int r0, int r1, float* ys,
-                                            int warp, int lane) {
-  constexpr int RU = W <= 2 ? 8 : (W == 4 ? 4 : 2);
-  float yv[4][W];
-#pragma unroll
-  for (int e = 0; e < 4; ++e)
-#pragma unroll
-    for (int w = 0; w < W; ++w) yv[e][w] = ys[(K + 4 * lane + e) * W + w];
-  for (int i0 = r0 + warp; i0 < r1; i0 += 32 * RU) {
-    float4 m[RU];
-#pragma unroll
-    for (int u = 0; u < RU; ++u) {
-      const int i = i0 + 32 * u;
-      m[u] = i < r1 ? __ldcs(reinterpret_cast<const float4*>(Ms + (int64_t)i * N + K + 4 * lane))
-                    : make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-#pragma unroll
-    for (int u = 0; u < RU; ++u) {
-      const int i = i0 + 32 * u;
-      float sum[W];
-#pragma unroll
-      for (int w = 0; w < W; ++w)
-        sum[w] = m[u].x * yv[0][w] + m[u].y * yv[1][w] + m[u].z * yv[2][w] + m[u].w * yv[3][w];
-#pragma unroll
-      for (int o = 16; o; o >>= 1)
-#pragma unroll
-        for (int w = 0; w < W; ++w) sum[w] += __shfl_xor_sync(0xffffffffu, sum[w], o);
-      if (lane == 0 && i < r1)
-#pragma unroll
-        for (int w = 0; w < W; ++w) ys[i * W + w] -= sum[w];
-    }
-  }
-}
-
-// Bring rows [r0, r1) x columns [c0, c0 + 128) of M (4 lines of 128 bytes a
-// row) and a 128 x 128 block inverse into L2 ahead of the block step that
-// reads them: those loads do not depend on the solution being computed, so
-// the next step finds them in L2 instead of waiting on HBM.
-__device__ __forceinline__ void prefetch_step(const float* Ms, int N, int c0, int r0, int r1, const float* D,
-                                              int tid) {
-  const int lines = (r1 > r0 ? r1 - r0 : 0) * 4;
-  for (int idx = tid; idx < lines; idx += ST)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(Ms + (int64_t)(r0 + (idx >> 2)) * N + c0 + 32 * (idx & 3)));
-  for (int idx = tid; idx < kMxNB * kMxNB / 32; idx += ST) asm volatile("prefetch.global.L2 [%0];" ::"l"(D + 32 * idx));
-}
-
-template <int W>
-__global__ void __launch_bounds__(ST, 1)
-k_mx_trsv(const float* __restrict__ M, const float* __restrict__ Linv, const float* __restrict__ Uinv,
-          float* __restrict__ Y, int N, int nrhs, const RefineState* __restrict__ st, int only_active) {
-  extern __shared__ float ys[];  // [N][W], then tmp [128][W]
-  float* tmp = ys + (int64_t)N * W;
-  const int s = blockIdx.x, c0 = blockIdx.y * W;
-  if (only_active && st[s].status != kRefineActive) return;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const float* Ms = M + (int64_t)s * N * N;
-  float* Ys = Y + (int64_t)s * N * nrhs;
-  for (int idx = tid; idx < N * W; idx += ST) {
-    const int i = idx / W, w = idx % W;
-    ys[idx] = c0 + w < nrhs ? Ys[(int64_t)i * nrhs + c0 + w] : 0.f;
-  }
-  __syncthreads();
-  const int nb = N / kMxNB;
-  const float* Ls = Linv + (int64_t)s * N * kMxNB;
-  const float* Us = Uinv + (int64_t)s * N * kMxNB;
-  for (int k = 0; k < nb; ++k) {  // L y = P c, block by block
-    const int K = k * kMxNB;
-    if (k + 1 < nb) prefetch_step(Ms, N, K + kMxNB, K + 2 * kMxNB, N, Ls + (int64_t)(K + kMxNB) * kMxNB, tid);
-    else prefetch_step(Ms, N, K, 0, K, Us + (int64_t)K * kMxNB, tid);  // the back substitution's first step
-    block_apply<W>(Ls + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
-    __syncthreads();
-    for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];
-    __syncthreads();
-    panel_apply<W>(Ms, N, K, K + kMxNB, N, ys, warp, lane);
-    __syncthreads();
-  }
-  for (int k = nb - 1; k >= 0; --k) {  // U x = y
-    const int K = k * kMxNB;
-    if (k > 0) prefetch_step(Ms, N, K - kMxNB, 0, K - kMxNB, Us + (int64_t)(K - kMxNB) * kMxNB, tid);
-    block_apply<W>(Us + (int64_t)K * kMxNB, ys + K * W, tmp, warp, lane);
-    __syncthreads();
-    for (int idx = tid; idx < kMxNB * W; idx += ST) ys[K * W + idx] = tmp[idx];
-    __syncthreads();
-    panel_apply<W>(Ms, N, K, 0, K, ys, warp, lane);
-    __syncthreads();
-  }
-  for (int idx = tid; idx < N * W; idx += ST) {
-    const int i = idx / W, w = idx % W;
-    if (c0 + w < nrhs) Ys[(int64_t)i * nrhs + c0 + w] = ys[idx];
-  }
-}
+// Triangular solves with the block factors.
 
 // Cluster form of the triangular solves: C CTAs per (system, chunk of W
 // right-hand sides), C = 1, 2, 4 or 8. CTA r owns the 128-row blocks b with
@@ -1309,11 +1185,6 @@ cudaError_t mx_prepare() {
     e = cudaFuncSetAttribute(k_mx_trsv_c<2, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_mx_trsv_c<4, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsv64Smem);
-  const int tsm = (int)(sizeof(float) * ((size_t)4096 * 8 + kMxNB * 8));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mx_trsv<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm);
   return e;
 }
 
