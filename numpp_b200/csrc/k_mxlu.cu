@@ -9,7 +9,7 @@
 //  k_mx_diag       LU of the 256 x 128 window panel (the diagonal block's
 //                  rows and the next block's) with partial pivoting (one CTA,
 //                  the window in shared memory, 32-column panels with the
-//                  rows in registers), then L^-1, U^-1 and U^-T of the block by
+//                  rows in registers, two per thread), then L^-1, U^-1 and U^-T of the block by
 //                  blocked inversion in shared memory, and the window's order.
 //  k_mx_permute    that order applied to the rest of the window's rows; the
 //                  new panel row transposed (A12^T).
@@ -286,64 +286,76 @@ __device__ __forceinline__ float rcp_approx(float x) {
   return y;
 }
 
-// Panel of the LU (columns c0 .. c0+31) on the eight warps, thread t =
-// physical row t of the window (R rows), in a rolled loop over the steps (the
-// code stays small). At step j a row's 32 registers hold its values in
-// columns c0 + j .. c0 + j + 31 (shifted left by one every step while the row
-// is not chosen, so register indices are static). Step j: each warp's largest
-// key (magnitude with its 8 low mantissa bits dropped, plus one) << 8 |
-// (255 - row) over the rows not yet chosen by one warp reduction; lane 0
-// publishes it and the warp's winner its values (predicated stores); one
-// barrier; the overall winner (the largest |a[j]| up to a relative 2^-15, the
-// lowest row among those) takes position c0 + j, and every row not yet chosen
-// stores l = a[j] / pivot and updates its values right of j. Keys and rows sit
-// in two alternating buffers, so one barrier per step suffices.
+// Panel of the LU (columns c0 .. c0+31) on warps 0-3: thread t owns the
+// physical rows t and t + 128 of the window (R rows), in a rolled loop over
+// the steps (the code stays small). At step j a row's 32 registers hold its
+// values in columns c0 + j .. c0 + j + 31 (shifted left by one every step
+// while the row is not chosen, so register indices are static). Step j: each
+// warp's largest key (magnitude with its 8 low mantissa bits dropped, plus
+// one) << 8 | (255 - row) over its rows not yet chosen by one warp reduction;
+// lane 0 publishes it and the owner of the warp's winner that row's values
+// (predicated stores); one barrier over the four warps; the overall winner
+// (the largest |a[j]| up to a relative 2^-15, the lowest row among those)
+// takes position c0 + j, and every row not yet chosen stores l = a[j] / pivot
+// and updates its values right of j. Keys and rows sit in two alternating
+// buffers, so one barrier per step suffices.
 __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t, int R) {
   constexpr unsigned FULL = 0xffffffffu;
   const int w = t >> 5, lane = t & 31;
-  const bool was = t >= R || ax.pos_of[t] >= 0;  // rows past the window never compete
-  bool done = was;
-  int jd = 0;         // step at which this row was chosen
-  int bad = INT_MAX;  // 1 + position of this row if its pivot failed
-  float v[32];
-  {
-    const float4* src = reinterpret_cast<const float4*>(LU + t * DLD + c0);
+  bool was[2], done[2];
+  int jd[2] = {0, 0};  // step at which each row was chosen
+  int bad = INT_MAX;   // 1 + position of a row of this thread whose pivot failed
+  float v[2][32];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int r = t + 128 * h;
+    was[h] = r >= R || ax.pos_of[r] >= 0;  // rows past the window never compete
+    done[h] = was[h];
+    const float4* src = reinterpret_cast<const float4*>(LU + r * DLD + c0);
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
       const float4 x = src[q];
-      v[4 * q] = x.x;
-      v[4 * q + 1] = x.y;
-      v[4 * q + 2] = x.z;
-      v[4 * q + 3] = x.w;
+      v[h][4 * q] = x.x;
+      v[h][4 * q + 1] = x.y;
+      v[h][4 * q + 2] = x.z;
+      v[h][4 * q + 3] = x.w;
     }
   }
 #pragma unroll 1
   for (int j = 0; j < 32; ++j) {
     const int b = j & 1;
-    const uint32_t key =
-        done ? 0u : ((((__float_as_uint(fabsf(v[0])) >> 8) + 1u) << 8) | (uint32_t)(255 - t));
+    uint32_t key = 0u;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const uint32_t kh =
+          done[h] ? 0u : ((((__float_as_uint(fabsf(v[h][0])) >> 8) + 1u) << 8) | (uint32_t)(255 - (t + 128 * h)));
+      key = max(key, kh);
+    }
     const uint32_t wkey = __reduce_max_sync(FULL, key);
+    const int wrow = 255 - (int)(wkey & 255u);
     // predicated stores, not a divergent branch (a one-lane branch around
     // these stores costs several times their latency)
     st_shared_u32_if(lane == 0, smem_addr(&ax.keys[b][w]), wkey);
-    st_shared_row_if(wkey != 0u && t == 255 - (int)(wkey & 255u), smem_addr(ax.crow[b][w]), v);
-    asm volatile("bar.sync 1, 256;\n" ::: "memory");
-    const uint4 k0 = *reinterpret_cast<const uint4*>(ax.keys[b]);
-    const uint4 k1 = *reinterpret_cast<const uint4*>(ax.keys[b] + 4);
-    const uint32_t best = max(max(max(k0.x, k0.y), max(k0.z, k0.w)), max(max(k1.x, k1.y), max(k1.z, k1.w)));
+    st_shared_row_if(wkey != 0u && wrow == t, smem_addr(ax.crow[b][w]), v[0]);
+    st_shared_row_if(wkey != 0u && wrow == t + 128, smem_addr(ax.crow[b][w]), v[1]);
+    asm volatile("bar.sync 1, 128;\n" ::: "memory");
+    const uint4 kk = *reinterpret_cast<const uint4*>(ax.keys[b]);
+    const uint32_t best = max(max(kk.x, kk.y), max(kk.z, kk.w));
     const int prow = 255 - (int)(best & 255u);
-    const float* pr = ax.crow[b][prow >> 5];
+    const float* pr = ax.crow[b][(prow & 127) >> 5];
     // the winner's bookkeeping without a branch
-    const bool win = t == prow;
-    st_shared_u32_if(win, smem_addr(&ax.pos_of[t]), (uint32_t)(c0 + j));
-    st_shared_u32_if(win, smem_addr(&ax.phys_of[c0 + j]), (uint32_t)t);
-    // the approximate reciprocal below flushes subnormals: such a pivot fails too
-    if (win && !(fabsf(v[0]) >= FLT_MIN && isfinite(v[0]))) bad = min(bad, c0 + j + 1);
-    jd = win ? j : jd;
-    done = done || win;
-    if (!done) {
-      const float l = v[0] * rcp_approx(pr[0]);
-      LU[t * DLD + c0 + j] = l;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const bool win = t + 128 * h == prow;
+      st_shared_u32_if(win, smem_addr(&ax.pos_of[t + 128 * h]), (uint32_t)(c0 + j));
+      st_shared_u32_if(win, smem_addr(&ax.phys_of[c0 + j]), (uint32_t)(t + 128 * h));
+      // the approximate reciprocal below flushes subnormals: such a pivot fails too
+      if (win && !(fabsf(v[h][0]) >= FLT_MIN && isfinite(v[h][0]))) bad = min(bad, c0 + j + 1);
+      jd[h] = win ? j : jd[h];
+      done[h] = done[h] || win;
+    }
+    if (!(done[0] && done[1])) {
+      const float rp = rcp_approx(pr[0]);
       float u[32];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -354,15 +366,25 @@ __device__ __forceinline__ void diag_panel(float* LU, DiagAux& ax, int c0, int t
         u[4 * q + 3] = x.w;
       }
 #pragma unroll
-      for (int c = 0; c < 31; ++c) v[c] = fmaf(-l, u[c + 1], v[c + 1]);
-      v[31] = 0.f;
+      for (int h = 0; h < 2; ++h) {
+        if (!done[h]) {
+          const float l = v[h][0] * rp;
+          LU[(t + 128 * h) * DLD + c0 + j] = l;
+#pragma unroll
+          for (int c = 0; c < 31; ++c) v[h][c] = fmaf(-l, u[c + 1], v[h][c + 1]);
+          v[h][31] = 0.f;
+        }
+      }
     }
   }
   if (bad != INT_MAX) atomicMin(&ax.fail, bad);
-  if (done && !was) {  // the row's U values, columns c0 + jd .. c0 + 31
 #pragma unroll
-    for (int c = 0; c < 32; ++c)
-      if (c < 32 - jd) LU[t * DLD + c0 + jd + c] = v[c];
+  for (int h = 0; h < 2; ++h) {
+    if (done[h] && !was[h]) {  // the row's U values, columns c0 + jd .. c0 + 31
+#pragma unroll
+      for (int c = 0; c < 32; ++c)
+        if (c < 32 - jd[h]) LU[(t + 128 * h) * DLD + c0 + jd[h] + c] = v[h][c];
+    }
   }
 }
 
@@ -386,7 +408,7 @@ k_mx_diag(float* __restrict__ M, int32_t* __restrict__ perm, int32_t* __restrict
 #pragma unroll 1
   for (int p = 0; p < 4; ++p) {
     const int c0 = 32 * p;
-    diag_panel(W0, ax, c0, tid, R);
+    if (warp < 4) diag_panel(W0, ax, c0, tid, R);
     __syncthreads();
     const int W = kMxNB - c0 - 32;  // trailing columns of the block
     const int Rn = R - c0 - 32;     // rows not yet chosen
